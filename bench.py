@@ -1,0 +1,295 @@
+"""Throughput of the SPH geomechanics step: particle-updates/s (soil particles x steps / s).
+
+Default workload: the 1.92M-particle translating retaining wall (soil block 200x80x120
+at dx = 2.5 mm, 262,500 Adami/contact boundary particles, FP32), synthetic seeded
+inputs from retainwall_code_b200.cases.retaining_wall.  A step is one whole
+StepCalculation + PredictorSection + CorrectorSection (src/loquat.cu:548-561), replayed
+from a captured CUDA graph; the state (~1.6 GB) is larger than L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload wall2|col1]
+
+--gpus N under torchrun: N independent replicas of the case, one per GPU (the single
+case does not shard); value = N x npm x K / max-over-ranks device time.
+--impl reference: the reference step on the host cores (the CPU restatement of the
+reference's kernels, all threads), rank 0 only, a bounded sample of steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-updates/s/GPU at 1.92M particles"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return dict(PEAKS_FALLBACK), "fallback"
+
+
+def make_case(workload: str):
+    from retainwall_code_b200 import cases as C
+
+    if workload == "wall2":
+        return C.retaining_wall(), {"workload": "retaining wall, active translation 1 mm/s",
+                                    "soil": "200x80x120", "dx_m": 0.0025, "npm": 1920000,
+                                    "wall_friction": "tan(2/3 phi_c)"}
+    if workload == "col1":
+        return C.column_collapse(), {"workload": "column collapse", "soil": "24x24x48", "dx_m": 0.005, "npm": 27648}
+    raise SystemExit(f"unknown workload {workload}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def allreduce_max(x: float, ws: int) -> float:
+    if ws <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def interaction_bytes(inf, ncell: int, scalar: int) -> int:
+    """Algorithmic HBM bytes of one interaction launch: every live soil particle's own
+    state read once (cell 16, position 4s, velocity 4s, stress 6s, mass 4s, contact
+    state 4x4s) and its outputs written once (contact 2x4s, acceleration 4s, strain rate
+    6s, spin 4s), plus each particle's neighbour record (16s) and position (4s) read once,
+    plus the cell ranges (8 B per cell)."""
+    s = scalar
+    per_soil = 16 + (4 + 4 + 6 + 4 + 16) * s + (8 + 4 + 6 + 4) * s
+    return inf.npm * per_soil + inf.np * 20 * s + ncell * 8
+
+
+def cpu_sample(case, threads: int, steps: int):
+    """The reference step on host cores: the CPU restatement, full case, `steps` steps."""
+    from oracle.oracle import Oracle
+
+    t0 = time.perf_counter()
+    o = Oracle(case, 4, threads)
+    t_init = time.perf_counter() - t0
+    o.step(1)  # warm-up step
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    npm = o.info().npm
+    o.close()
+    return npm * steps / dt, dt, t_init
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    case, cfg = make_case(args.workload)
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, 3))
+    ups, dt, _ = cpu_sample(case, threads, steps)
+    sample = f"{steps} whole steps of the full {case.npm}-particle case after 1 warm-up step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ups, "unit": "particle-updates/s", "n_gpus": args.gpus,
+        "steps": steps, "warmup": 1, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": dict(cfg, host_threads=threads),
+        "cpu_baseline": {"value": ups, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": ups, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+
+    from retainwall_code_b200 import LoquatSph
+    from retainwall_code_b200 import _abi
+
+    case, cfg = make_case(args.workload)
+    # ---- device-resident throughput ----------------------------------------------------
+    sim = LoquatSph(case=case, device=local, precision=4)
+    inf = sim.info()
+    sim.step(args.warmup)
+    sim.synchronize()
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        ms = sim.step_timed(args.steps)
+    sim.synchronize()
+    ms = allreduce_max(ms, ws)
+    barrier(ws)
+    npm = sim.info().npm
+    value = ws * npm * args.steps / (ms * 1e-3)
+    inf = sim.info()
+    if inf.device_err:
+        raise SystemExit(f"device error word {inf.device_err}")
+    # ---- stage profile (CUDA events on the library's stream, per-stage launches) -------
+    stages, kps = sim.profile(5)
+    ix_ms = 0.5 * (stages["interaction_p"] + stages["interaction_c"])
+    sim.close()
+    # ---- end to end through the public API: upload from host, step, read the result ---
+    barrier(ws)
+    t0 = time.perf_counter()
+    sim2 = LoquatSph(case=case, device=local, precision=4)
+    e2e_steps = args.steps
+    for _ in range(e2e_steps):
+        sim2.step(1)
+        sim2.wall_force(0)  # D2H of the step's result (3 doubles)
+    sim2.synchronize()
+    e2e_s = allreduce_max(time.perf_counter() - t0, ws)
+    sim2.close()
+    e2e = ws * npm * e2e_steps / e2e_s
+    # bytes uploaded by rw_create_from_case: codes, cell, position x2, velocity, id/mass,
+    # stress, strain (float32 structure of arrays) + boundary normals
+    h2d = inf.np * (16 * 6 + 24 * 2) + inf.npb * 16
+    # ---- roofline of the dominant kernel ------------------------------------------------
+    pk, kind = peaks()
+    ib = interaction_bytes(inf, inf.ncell, 4)
+    achieved = ib / (ix_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": "k_interaction", "achieved": achieved, "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": kind, "traffic": None,
+            "algorithmic_bytes_per_launch": ib, "launch_ms": ix_ms,
+            "note": "pair arithmetic bound (FP32 issue), not HBM; see fp32 entry"}
+    flop_per_update = 2 * 27000.0  # two interaction passes per step, ~27 kFLOP each pair sweep total
+    clocks = clk.summary()
+    mhz = clocks.get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-updates/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "config": dict(cfg, parallelism=f"replicas x{ws}", np=inf.np, npb=inf.npb, ncell=inf.ncell,
+                       l2="state 1.6 GB > L2: no flush needed"),
+        "e2e": {"value": e2e, "unit": "particle-updates/s", "h2d_bytes_per_step": int(h2d / e2e_steps),
+                "d2h_bytes_per_step": 24, "note": "case upload from host + per-step rw_step + wall-force read"},
+        "roofline": roof,
+        "roofline_fp32": {"bound": "fp32-issue", "achieved_tflops": npm * 27000.0 / (ix_ms * 1e-3) / 1e12,
+                          "peak_tflops_at_clock": fp32_peak, "flop_per_update_per_pass": 27000.0},
+        "stage_ms": stages,
+        "gpu_launches": kps * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        ups, dt, _ = cpu_sample(case, threads, 2)
+        line["cpu_baseline"] = {"value": ups, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+                                "sample": f"2 whole steps of the full {npm}-particle case (+1 warm-up)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="wall2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":  # host cores only: rank 0 runs, the other ranks exit
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        run_reference(args, ws, int(os.environ.get("RANK", "0")))
+        return
+    ws, rank, local = dist_setup()
+    try:
+        run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * retainwall.h - C ABI of the B200-native SPH geomechanics step (librw.so).
+ *
+ * The reference (Xshuaizhang/Retainwall_code, a LOQUAT-derived solver) exposes its
+ * step only as private methods of the C++ class LoquatSph (src/loquat.h:44-126),
+ * driven by LoquatSph::RunSimulation (src/loquat.cu:511-565) from src/main.cpp.
+ * Each entry point below replaces one of those methods (cited per function) so a
+ * host program written against the reference's step sequence can call this library
+ * instead.  Conventions:
+ *   - plain C types only; every call returns an rw_status (0 = RW_OK) and never exits;
+ *   - one context per host thread; a context owns its device memory and CUDA stream;
+ *   - arrays crossing the ABI use the reference's per-particle layouts (see rw_array).
+ */
+#ifndef RETAINWALL_H_
+#define RETAINWALL_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int rw_status;
+enum {
+  RW_OK = 0,
+  RW_EINVAL = 1,     /* bad argument or inconsistent case                          */
+  RW_ENOENT = 2,     /* project file missing                                         */
+  RW_EIO = 3,        /* read/write error                                             */
+  RW_EFORMAT = 4,    /* malformed XML/.dat/.motion, missing mandatory parameter      */
+  RW_ECUDA = 5,      /* CUDA runtime error (message in rw_last_error)                */
+  RW_ENOMEM = 6,     /* device or host allocation failed                             */
+  RW_EDEVICE = 7,    /* a kernel raised the device error word (see rw_info.device_err) */
+  RW_ETIMEDOUT = 8,  /* a bounded device wait gave up                                */
+  RW_ESTATE = 9      /* call out of sequence (e.g. wrong section)                    */
+};
+
+/* Device error word bits (rw_info.device_err). */
+enum {
+  RW_DERR_CELL_RANGE = 1,   /* a live particle's cell left the grid (reference: out-of-bounds write) */
+  RW_DERR_COUNT = 2,        /* particle-count invariant npb+npm+deleted != np (src/loquat_grid.cu:251-254) */
+  RW_DERR_LIST = 4,         /* neighbour list exceeded its per-cell capacity (handled, reported)  */
+  RW_DERR_PERM = 8          /* sort produced an index outside [0, np) (guarded; never expected)  */
+};
+
+#define RW_MODEL_MAX 10
+#define RW_MATERIAL_SIZE 15
+#define RW_MOTION_MAX 10
+#define RW_TABLE_MAX 10
+
+/* One rigid body's motion table (MotionTable, src/types.h:77-97; .motion file). */
+typedef struct rw_motion {
+  int32_t is_translation, n_trans;
+  double trans_time[RW_TABLE_MAX], trans_vel[RW_TABLE_MAX][3], trans_acc[RW_TABLE_MAX][3];
+  int32_t is_rotation, pattern, n_rot, pad_;
+  double pos_rp[3], rotat_vel[3], rotat_time[RW_TABLE_MAX], rotat_acc[RW_TABLE_MAX][3];
+} rw_motion;
+
+/* The parameter file (<project>.xml, read by LoquatIo::LoadParameters,
+ * src/loquat_io.cu:75-202).  Values are given as parsed (double); the library rounds
+ * them to its arithmetic type exactly as the reference's (scalar)atof does. */
+typedef struct rw_case_params {
+  int32_t dim, periodbound, n_motion, np, npb, npm, n_model;
+  int32_t stress_shepard_filter, dynamic_time_step, integration_method, viscosity_type;
+  int32_t output_number, output_format, pad_;
+  double planeleft[4], planeright[4];
+  double domain_size[3], domain_min[3];
+  double dr, hdr, gravity[3], rho0_m, damping;
+  double model_par[RW_MODEL_MAX][RW_MATERIAL_SIZE];
+  double artificial_viscosity_alpha_m, cs_m, cfl, artificial_pressure_coefficient_material;
+  double time_max, time, dt, output_frequency;
+  /* Wall-soil Coulomb coefficient of contact walls.  The reference hard-codes
+   * 0.58108 (src/particle_interaction.cu:188-189); optional XML tag
+   * "wall-friction-coefficient" (type scalar) sets it. */
+  double wall_friction;
+  rw_motion motion[RW_MOTION_MAX];
+} rw_case_params;
+
+/* A case in the reference's particle layout (.dat, src/loquat_io.cu:229-254):
+ * np rows, boundary particles first.  Positions are absolute. */
+typedef struct rw_case {
+  rw_case_params params;
+  const int32_t* codes;    /* np x 4: block id, status (0 Fix / 1 NonFix), model, material|motion */
+  const double* pospres;   /* np x 4 */
+  const double* velrhop;   /* np x 4 */
+  const double* idmassidx; /* np x 4: id (100 material, 0 boundary), mass, (index), w */
+  const double* stress;    /* np x 6: xx yy zz xy xz yz */
+  const double* strain;    /* np x 6 */
+  const double* normal;    /* npb x 4: unit normal, w = +1 free slip / -1 no slip */
+} rw_case;
+
+/* Arrays for rw_get_array / rw_set_array, in the reference's device layouts
+ * (element = scalar of the context's precision unless noted). */
+typedef enum rw_array {
+  RW_ARR_CODES = 0,       /* np   x int4            codes                       */
+  RW_ARR_CELLPOS = 1,     /* np   x int4            cellpos (cell x,y,z, key)   */
+  RW_ARR_POSPRES = 2,     /* np   x 4               in-cell position + pressure */
+  RW_ARR_POSPRES_ORI = 3, /* np   x 4               accumulated displacement    */
+  RW_ARR_VELRHOP = 4,     /* np   x 4               velocity + density          */
+  RW_ARR_IDMASSIDX = 5,   /* np   x 4               id, mass, index, M_crt      */
+  RW_ARR_STR = 6,         /* np   x 6               stress                      */
+  RW_ARR_STN = 7,         /* np   x 6               strain                      */
+  RW_ARR_NORMAL = 8,      /* npb  x 4               wall normals                */
+  RW_ARR_CONTACT_MAG = 9, /* np   x 9               contact force, normal, velocity */
+  RW_ARR_CONTACT_VAR = 10,/* np   x 4               kernel integral, distance, slide flag, wall id */
+  RW_ARR_ACCAD = 11,      /* np   x 4               acceleration + density rate */
+  RW_ARR_SPIN = 12,       /* np   x 4                                           */
+  RW_ARR_ACESTN = 13,     /* np   x 6               strain rate                 */
+  RW_ARR_POSPRES_INI = 14,
+  RW_ARR_VELRHOP_INI = 15,
+  RW_ARR_STR_INI = 16,
+  RW_ARR_STN_INI = 17,
+  RW_ARR_PART_IDX = 18,   /* np   x int32           last sort permutation       */
+  RW_ARR_CELL_BEG = 19,   /* ncell x int32          -1 for empty cells          */
+  RW_ARR_CELL_END = 20,   /* ncell x int32                                      */
+  RW_ARR_POS_ABS = 21,    /* np   x 4               absolute position (get only) */
+  RW_ARR_COUNT_ = 22
+} rw_array;
+
+typedef struct rw_info {
+  int32_t np, npb, npm, np_delete_m, ncell, step, scalar_bytes, device_err;
+  int32_t cell_num[3], n_motion;
+  double time, dt, h;
+} rw_info;
+
+typedef struct rw_ctx rw_ctx;
+
+/* Options (rw_set_option). */
+enum {
+  RW_OPT_WALL_FRICTION = 0,  /* Coulomb coefficient of contact walls (default from the case) */
+  RW_OPT_COMPAT_CONTACT = 1  /* 1 (default): contact state bound to array slots as in the reference
+                                (src/loquat.cu:254-287 never permutes it); 0: follows the particle */
+};
+
+const char* rw_status_string(rw_status s);
+/* Last error message of a context (or of the last failed rw_create* when ctx is NULL). */
+const char* rw_last_error(const rw_ctx* ctx);
+
+/* LoquatSph(name) + RunSimulation's set-up (src/loquat.cu:514-531): reads
+ * <project>.xml/.dat/.motion, initialises parameters (InitializeParameters,
+ * src/loquat.cu:130-190), uploads the state, converts to in-cell positions and runs the
+ * first neighbour search and sort.  precision: 4 (float, the reference default) or 8. */
+rw_status rw_create(const char* project, int device, int precision, rw_ctx** out);
+/* Same set-up from a case held in host memory (no files). */
+rw_status rw_create_from_case(const rw_case* c, int device, int precision, rw_ctx** out);
+/* ~LoquatSph (src/loquat.cu:72-99). */
+rw_status rw_destroy(rw_ctx* ctx);
+
+/* StepCalculation (src/loquat.cu:366-374): dt = cfl*h/cs, time of this step. */
+rw_status rw_begin_step(rw_ctx* ctx);
+/* LoquatGrid::NeighborSearch (src/loquat_grid.cu:216-260) followed by SortArraysPrimary
+ * (section 0, src/loquat.cu:254-266) or SortArraysAll (section 1, src/loquat.cu:269-287). */
+rw_status rw_neighbor_search(rw_ctx* ctx, int section);
+/* LoquatSph::RigidBodyUpdate (src/adami_boundary.cu:175-203), on the device. */
+rw_status rw_rigid_body_update(rw_ctx* ctx);
+/* LoquatSph::AdamiBoundary (src/adami_boundary.cu:160-169). */
+rw_status rw_adami_boundary(rw_ctx* ctx);
+/* LoquatSph::FindCornerParticle (src/adami_boundary.cu:294-306). */
+rw_status rw_find_corner(rw_ctx* ctx);
+/* LoquatSph::StressRegularization (src/field_smoothing.cu:305-314). */
+rw_status rw_shepard_filter(rw_ctx* ctx);
+/* LoquatSph::ParticleInteraction (src/particle_interaction.cu:310-313). */
+rw_status rw_particle_interaction(rw_ctx* ctx);
+/* LoquatSph::Predictor (src/predictor_corrector.cu:87-103). */
+rw_status rw_predictor(rw_ctx* ctx);
+/* LoquatSph::Corrector (src/predictor_corrector.cu:201-213). */
+rw_status rw_corrector(rw_ctx* ctx);
+/* End of RunSimulation's loop body (src/loquat.cu:559-561): time += dt, step++. */
+rw_status rw_end_step(rw_ctx* ctx);
+/* nsteps whole steps (StepCalculation + PredictorSection + CorrectorSection,
+ * src/loquat.cu:548-561) replayed from one captured CUDA graph, no host round trip. */
+rw_status rw_step(rw_ctx* ctx, int nsteps);
+/* rw_step with a CUDA event pair recorded on the context's stream around the nsteps
+ * graph launches; *ms receives the device time (no reference counterpart). */
+rw_status rw_step_timed(rw_ctx* ctx, int nsteps, double* ms);
+/* Blocks until the context's stream is idle; reports RW_EDEVICE if a kernel flagged an error. */
+rw_status rw_synchronize(rw_ctx* ctx);
+
+/* Lateral wall force, FP64 accumulation, in N (not kN).
+ * mode 0: sum of contact force over material particles whose nearest contact wall
+ *         (contact_var.w) equals wall_id;
+ * mode 1: the reference's strip (src/utilities.cu:619-624): x <= x_max, z in [z_min, z_max],
+ *         with strip = {x_max, z_min, z_max}; strip may be NULL for the reference's values
+ *         (0.04 + bound_thickness + 3 dr, bound_thickness + 0.04, bound_thickness + 1.04). */
+rw_status rw_wall_force(rw_ctx* ctx, int mode, int wall_id, const double* strip, double out_xyz[3]);
+/* Saving (src/loquat.cu:439-482) through LoquatIo::SaveXml / SaveParticles: writes
+ * <outdir>/output_N.xml and N.dat (format 1) or <id>_N.vtu (format 2) with the
+ * Shepard-smoothed stress, and appends "time F[kN]" to <outdir>/time_history.txt. */
+rw_status rw_save(rw_ctx* ctx, const char* outdir);
+
+rw_status rw_get_info(rw_ctx* ctx, rw_info* out);
+rw_status rw_set_option(rw_ctx* ctx, int option, double value);
+/* Copy an array out (host_dst, bytes = rows x row size of the context's precision). */
+rw_status rw_get_array(rw_ctx* ctx, int which, void* host_dst, size_t bytes);
+/* Overwrite a state array (golden-state restarts); RW_ARR_POS_ABS is not settable. */
+rw_status rw_set_array(rw_ctx* ctx, int which, const void* host_src, size_t bytes);
+/* Overwrite time, step and the live/deleted counts after rw_set_array restarts. */
+rw_status rw_set_counters(rw_ctx* ctx, double time, int step, int npm, int np_delete_m);
+
+/* Stage timing (no reference counterpart; the reference's Timer buckets CPU clock per
+ * phase, src/types.h:167-184).  Runs nsteps whole steps as per-stage launches with a
+ * CUDA event pair around each stage on the context's stream and returns the mean time
+ * per stage in ms, in the order of RW_STAGE_*.  *kernels_per_step receives the number of
+ * kernels one whole step launches. */
+enum {
+  RW_STAGE_SEARCH_P = 0, RW_STAGE_RIGID = 1, RW_STAGE_ADAMI_P = 2, RW_STAGE_CORNER_P = 3,
+  RW_STAGE_INTERACTION_P = 4, RW_STAGE_PREDICTOR = 5, RW_STAGE_SEARCH_C = 6, RW_STAGE_ADAMI_C = 7,
+  RW_STAGE_CORNER_C = 8, RW_STAGE_INTERACTION_C = 9, RW_STAGE_CORRECTOR = 10, RW_STAGE_COUNT_ = 11
+};
+rw_status rw_profile(rw_ctx* ctx, int nsteps, double* ms_per_stage, int n_stages, int* kernels_per_step);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RETAINWALL_H_ */

@@ -7,13 +7,19 @@
 // oracle's restatement of those functions bit for bit; it is never linked into
 // the product.
 //
-// The headers are written for nvcc; on the host the CUDA qualifiers expand to
-// nothing (cuda_runtime.h host_defines) and only norm3df is missing.
+// The headers are written for nvcc; on the host the CUDA qualifiers expand to nothing
+// (cuda_runtime.h host_defines).  Under nvcc, unqualified pow/exp/sin/sqrt of float
+// arguments resolve to the float overloads; a plain g++ build would pick the double C
+// functions.  The using-declarations below restore nvcc's overload resolution.
 #include <algorithm>
 #include <cmath>
 using std::max;
 using std::min;
-static inline float norm3df(float a, float b, float c) { return std::sqrt(a * a + b * b + c * c); }
+using std::cos;
+using std::exp;
+using std::pow;
+using std::sin;
+using std::sqrt;
 
 #include "functions.h"
 #include "constitutive_model.h"

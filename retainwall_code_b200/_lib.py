@@ -1,0 +1,72 @@
+"""ctypes binding of the in-tree native library (librw.so, include/retainwall.h).
+
+The library is the product: nothing here falls back to Python or to a CPU path.  If
+librw.so is missing or cannot be loaded, ``lib()`` raises."""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+from . import _abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librw.so")
+
+# Every symbol include/retainwall.h declares.
+EXPORTS = [
+    "rw_status_string", "rw_last_error", "rw_create", "rw_create_from_case", "rw_destroy", "rw_begin_step",
+    "rw_neighbor_search", "rw_rigid_body_update", "rw_adami_boundary", "rw_find_corner", "rw_shepard_filter",
+    "rw_particle_interaction", "rw_predictor", "rw_corrector", "rw_end_step", "rw_step", "rw_synchronize",
+    "rw_wall_force", "rw_save", "rw_get_info", "rw_set_option", "rw_get_array", "rw_set_array", "rw_set_counters",
+    "rw_profile", "rw_step_timed",
+]
+STAGE_NAMES = ["search_p", "rigid", "adami_p", "corner_p", "interaction_p", "predictor", "search_c", "adami_c",
+               "corner_c", "interaction_c", "corrector"]
+
+
+class RwError(RuntimeError):
+    def __init__(self, status: int, what: str, detail: str):
+        super().__init__(f"{what}: {_abi.STATUS_NAMES.get(status, status)}: {detail}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ct.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} not built: run `python -m retainwall_code_b200.build`")
+    L = ct.CDLL(LIB_PATH)
+    P = ct.c_void_p
+    L.rw_status_string.restype = ct.c_char_p
+    L.rw_status_string.argtypes = [ct.c_int]
+    L.rw_last_error.restype = ct.c_char_p
+    L.rw_last_error.argtypes = [P]
+    L.rw_create.argtypes = [ct.c_char_p, ct.c_int, ct.c_int, ct.POINTER(P)]
+    L.rw_create_from_case.argtypes = [ct.POINTER(_abi.Case), ct.c_int, ct.c_int, ct.POINTER(P)]
+    for n in ("rw_destroy", "rw_begin_step", "rw_rigid_body_update", "rw_adami_boundary", "rw_find_corner",
+              "rw_shepard_filter", "rw_particle_interaction", "rw_predictor", "rw_corrector", "rw_end_step",
+              "rw_synchronize"):
+        getattr(L, n).argtypes = [P]
+    L.rw_neighbor_search.argtypes = [P, ct.c_int]
+    L.rw_step.argtypes = [P, ct.c_int]
+    L.rw_step_timed.argtypes = [P, ct.c_int, ct.POINTER(ct.c_double)]
+    L.rw_wall_force.argtypes = [P, ct.c_int, ct.c_int, ct.c_void_p, ct.POINTER(ct.c_double)]
+    L.rw_save.argtypes = [P, ct.c_char_p]
+    L.rw_get_info.argtypes = [P, ct.POINTER(_abi.Info)]
+    L.rw_set_option.argtypes = [P, ct.c_int, ct.c_double]
+    L.rw_get_array.argtypes = [P, ct.c_int, ct.c_void_p, ct.c_size_t]
+    L.rw_set_array.argtypes = [P, ct.c_int, ct.c_void_p, ct.c_size_t]
+    L.rw_set_counters.argtypes = [P, ct.c_double, ct.c_int, ct.c_int, ct.c_int]
+    L.rw_profile.argtypes = [P, ct.c_int, ct.POINTER(ct.c_double), ct.c_int, ct.POINTER(ct.c_int)]
+    _lib = L
+    return L
+
+
+def check(status: int, what: str, ctx=None) -> None:
+    if status != 0:
+        detail = lib().rw_last_error(ctx)
+        raise RwError(status, what, detail.decode() if detail else "")

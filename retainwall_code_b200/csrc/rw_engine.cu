@@ -1,0 +1,990 @@
+// Host side of the step: device state, per-stage launches (one per reference stage
+// method), the CUDA-graph whole-step path, array export in the reference layouts,
+// output writing, and the extern "C" ABI declared in include/retainwall.h.
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "../../include/retainwall.h"
+#include "rw_io.h"
+#include "rw_kernels.cuh"
+
+namespace rw {
+
+static thread_local std::string g_create_err;
+
+struct Fail : std::runtime_error {
+  int code;
+  Fail(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define RW_CU(call)                                                                         \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) throw Fail(e_ == cudaErrorMemoryAllocation ? RW_ENOMEM : RW_ECUDA, \
+                                      std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+struct EngineBase {
+  std::string err;
+  int device = 0;
+  virtual ~EngineBase() = default;
+  virtual void begin_step() = 0;
+  virtual void neighbor_search(int section) = 0;
+  virtual void rigid() = 0;
+  virtual void adami() = 0;
+  virtual void corner() = 0;
+  virtual void shepard() = 0;
+  virtual void interaction() = 0;
+  virtual void predictor() = 0;
+  virtual void corrector() = 0;
+  virtual void end_step() = 0;
+  virtual void step(int n) = 0;
+  virtual int sync() = 0;
+  virtual void wall_force(int mode, int wall_id, const double* strip, double* out) = 0;
+  virtual void save(const char* outdir) = 0;
+  virtual void info(rw_info* out) = 0;
+  virtual int set_option(int opt, double v) = 0;
+  virtual int get_array(int which, void* dst, size_t bytes) = 0;
+  virtual int set_array(int which, const void* src, size_t bytes) = 0;
+  virtual void set_counters(double time, int step, int npm, int np_delete_m) = 0;
+  virtual void profile(int nsteps, double* ms, int n, int* kps) = 0;
+  virtual double step_timed(int n) = 0;
+};
+
+static inline unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+template <class T> struct Engine final : EngineBase {
+  Params<T> P{};
+  DevState<T> S{};
+  Dyn<T>* d_dyn = nullptr;
+  cudaStream_t st = nullptr;
+  std::vector<void*> allocs;
+  int cpar = 0;  // live contact buffer
+  bool compat_contact = true;
+  cudaGraphExec_t gexec = nullptr;
+  int g_cpar = -1;
+  rw_case_params cparams{};
+  int output_number = 0;
+
+  ~Engine() override {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (st) cudaStreamSynchronize(st);
+    for (void* p : allocs) cudaFree(p);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  template <class X> X* dalloc(size_t n) {
+    void* p = nullptr;
+    RW_CU(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(X)));
+    allocs.push_back(p);
+    RW_CU(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(X), st));
+    return (X*)p;
+  }
+  template <class X> void up(X* d, const std::vector<X>& h) {
+    if (!h.empty()) RW_CU(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, st));
+  }
+  template <class X> std::vector<X> down(const X* d, size_t n) {
+    std::vector<X> h(n);
+    if (n) RW_CU(cudaMemcpyAsync(h.data(), d, n * sizeof(X), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaStreamSynchronize(st));
+    return h;
+  }
+  int* need_ptr() { return &d_dyn->need_sort; }
+  Dyn<T> dyn_host() {
+    Dyn<T> d;
+    RW_CU(cudaMemcpyAsync(&d, d_dyn, sizeof(d), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaStreamSynchronize(st));
+    return d;
+  }
+  void check_launch() { RW_CU(cudaGetLastError()); }
+
+  // ------------------------------------------------------------------------------
+  // Set-up: InitializeParameters (src/loquat.cu:130-190), AllocateGpuMemory,
+  // CopyDataFromHostToDevice, PositionFromAbsolute2Relative, first NeighborSearch +
+  // SortArraysPrimary (src/loquat.cu:514-531).
+  // ------------------------------------------------------------------------------
+  void create(const rw_case* c, int dev) {
+    device = dev;
+    RW_CU(cudaSetDevice(dev));
+    RW_CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const rw_case_params& q = c->params;
+    cparams = q;
+    output_number = q.output_number;
+    if (q.dim != 3) throw Fail(RW_EINVAL, "only 3D cases are supported (dimension-of-problem must be 3)");
+    if (q.periodbound) throw Fail(RW_EINVAL, "periodic boundaries are not supported");
+    if (q.np != q.npb + q.npm || q.np <= 0 || q.npb < 0 || q.npm < 0)
+      throw Fail(RW_EINVAL, "Error! Wrong number of particles ...");
+    if (q.np >= (1 << 27)) throw Fail(RW_EINVAL, "more than 2^27 particles");
+    if (q.n_motion < 0 || q.n_motion > kMotionMax) throw Fail(RW_EINVAL, "number-of-motion out of range");
+    if (q.n_model < 0 || q.n_model > kModelMax) throw Fail(RW_EINVAL, "number-of-model out of range");
+    for (int i = 0; i < q.np; ++i) {  // indices the kernels use to address tables
+      const int32_t* cc = c->codes + 4 * i;
+      const bool nonfix = cc[1] == 1;
+      if (i < q.npb) {
+        if (nonfix && (cc[3] < 0 || cc[3] >= q.n_motion))
+          throw Fail(RW_EINVAL, "moving boundary particle " + std::to_string(i) + " has motion index out of range");
+      } else if (nonfix && (cc[3] < 0 || cc[3] >= kModelMax)) {
+        throw Fail(RW_EINVAL, "material particle " + std::to_string(i) + " has material index out of range");
+      }
+    }
+    P.dim = q.dim;
+    P.periodbound = 0;
+    P.n_motion = q.n_motion;
+    P.n_model = q.n_model;
+    P.np = q.np;
+    P.npb = q.npb;
+    P.npm0 = q.npm;
+    for (int k = 0; k < 4; ++k) {
+      P.planeleft[k] = (T)q.planeleft[k];
+      P.planeright[k] = (T)q.planeright[k];
+    }
+    for (int k = 0; k < 3; ++k) {
+      P.domain_size[k] = (T)q.domain_size[k];
+      P.domain_min[k] = (T)q.domain_min[k];
+      P.gravity[k] = (T)q.gravity[k];
+    }
+    P.dr = (T)q.dr;
+    P.hdr = (T)q.hdr;
+    P.rho0_m = (T)q.rho0_m;
+    P.damping = (T)q.damping;
+    for (int i = 0; i < kModelMax; ++i)
+      for (int j = 0; j < kMatSize; ++j) P.model_par[i][j] = (T)q.model_par[i][j];
+    P.stress_shepard_filter = q.stress_shepard_filter;
+    P.viscosity_type = q.viscosity_type;
+    P.output_format = q.output_format;
+    P.alpha_m = (T)q.artificial_viscosity_alpha_m;
+    P.cs_m = (T)q.cs_m;
+    P.cfl = (T)q.cfl;
+    P.art_coef = (T)q.artificial_pressure_coefficient_material;
+    P.time_max = (T)q.time_max;
+    P.output_frequency = (T)q.output_frequency;
+    P.wall_fric = (T)q.wall_friction;
+    P.h = P.dr * P.hdr;
+    P.i_h = T(1.0f) / P.h;
+    P.eta = T(0.01f) * P.h * P.h;
+    P.bound_thickness = (T)(std::ceil(2.0 * (double)P.hdr) * (double)P.dr);
+    const double h_d = (double)P.h;
+    P.vol_def = (T)std::pow((double)P.dr, 3.0);
+    P.cell_num[0] = (int)(T(0.5f) * P.i_h * P.domain_size[0]) + 1;
+    P.cell_num[1] = (int)(T(0.5f) * P.i_h * P.domain_size[1]) + 1;
+    P.cell_num[2] = (int)(T(0.5f) * P.i_h * P.domain_size[2]) + 1;
+    P.knorm = (T)(42.0 / (256.0 * 3.14159265358979323846 * std::pow(h_d, 3.0)));
+    P.kgrad = (T)(-5.0 * 42 / (256.0 * 3.14159265358979323846 * std::pow(h_d, 5.0)));
+    const long one = (long)P.cell_num[0] * P.cell_num[1] * P.cell_num[2];
+    if (one <= 0 || 2 * one + 1 > (1L << 30)) throw Fail(RW_EINVAL, "cell grid too large");
+    P.ncell_material = (int)one;
+    P.ncell_delete_m = (int)(2 * one);
+    P.ncell = P.ncell_delete_m + 1;
+    const T qq = P.dr * P.i_h;
+    P.kernel_zero = P.knorm * T(2.0f) * T(2.0f) * T(2.0f) * T(2.0f) * T(0.5f);
+    P.kernel_dr = P.knorm * (T(2.0f) - qq) * (T(2.0f) - qq) * (T(2.0f) - qq) * (T(2.0f) - qq) * (qq + T(0.5f));
+    P.two_h = (T)(2.0 * (double)P.h);
+    const double rpre = 2.0 * h_d * (1.0 + 1e-4);
+    P.r2_prefilter = (T)(rpre * rpre);
+    P.dt = P.cfl * (P.h / P.cs_m);  // StepCalculation (src/loquat.cu:368-369)
+
+    const size_t np = P.np, npb = P.npb;
+    for (int b = 0; b < 2; ++b) {
+      S.codes[b] = dalloc<int4>(np);
+      S.cellpos[b] = dalloc<int4>(np);
+      S.pos[b] = dalloc<V4<T>>(np);
+      S.pos_ori[b] = dalloc<V4<T>>(np);
+      S.vel[b] = dalloc<V4<T>>(np);
+      S.idm[b] = dalloc<V4<T>>(np);
+      S.str_a[b] = dalloc<V4<T>>(np);
+      S.str_b[b] = dalloc<V2<T>>(np);
+      S.stn_a[b] = dalloc<V4<T>>(np);
+      S.stn_b[b] = dalloc<V2<T>>(np);
+      S.normal[b] = dalloc<V4<T>>(npb);
+      S.pos_ini[b] = dalloc<V4<T>>(np);
+      S.vel_ini[b] = dalloc<V4<T>>(np);
+      S.stri_a[b] = dalloc<V4<T>>(np);
+      S.stri_b[b] = dalloc<V2<T>>(np);
+      S.stni_a[b] = dalloc<V4<T>>(np);
+      S.stni_b[b] = dalloc<V2<T>>(np);
+      S.cv[b] = dalloc<V4<T>>(np);
+      S.cf[b] = dalloc<V4<T>>(np);
+    }
+    S.accad = dalloc<V4<T>>(np);
+    S.spin = dalloc<V4<T>>(np);
+    S.ace_a = dalloc<V4<T>>(np);
+    S.ace_b = dalloc<V2<T>>(np);
+    S.cny = dalloc<V4<T>>(np);
+    S.cvz = dalloc<V4<T>>(np);
+    S.rec = dalloc<Rec<T>>(np);
+    S.tc_a = dalloc<V4<T>>(np);
+    S.tc_b = dalloc<V2<T>>(np);
+    S.keys = dalloc<int>(np);
+    S.vals = dalloc<int>(np);
+    S.tk = dalloc<int>(np);
+    S.tv = dalloc<int>(np);
+    S.range = dalloc<int2>(P.ncell);
+    S.ntiles = (int)nblk((long)np, RS_TILE);
+    S.hist = dalloc<int>(256 * (size_t)S.ntiles);
+    S.dtot = dalloc<int>(256);
+    int bits = 1;
+    while ((1L << bits) <= P.ncell_delete_m) ++bits;
+    S.sort_passes = (bits + 7) / 8;
+    S.skeys = (S.sort_passes & 1) ? S.tk : S.keys;
+    S.sperm = (S.sort_passes & 1) ? S.tv : S.vals;
+    S.wsum = dalloc<double>(3 * (WF_BLOCKS + 1));
+    d_dyn = dalloc<Dyn<T>>(1);
+
+    // Host-side conversion to structure-of-arrays, with the reference's
+    // absolute -> in-cell position arithmetic (src/loquat_grid.cu:322-330).
+    std::vector<int4> h_codes(np), h_cell(np);
+    std::vector<V4<T>> h_pos(np), h_ori(np), h_vel(np), h_idm(np), h_nrm(npb);
+    std::vector<V4<T>> h_sa(np), h_na(np);
+    std::vector<V2<T>> h_sb(np), h_nb(np);
+    const T half_ih = (T)(0.5 * (double)P.i_h);
+    for (size_t i = 0; i < np; ++i) {
+      const int32_t* cc = c->codes + 4 * i;
+      h_codes[i] = int4{cc[0], cc[1], cc[2], cc[3]};
+      const double* a = c->pospres + 4 * i;
+      V4<T> pa{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+      h_ori[i] = pa;
+      T sx = pa.x * half_ih, sy = pa.y * half_ih, sz = pa.z * half_ih;
+      int cx = (int)sx, cy = (int)sy, cz = (int)sz;
+      h_cell[i] = int4{cx, cy, cz, 0};
+      T ox = (T)cx * P.two_h, oy = (T)cy * P.two_h, oz = (T)cz * P.two_h;
+      h_pos[i] = V4<T>{pa.x - ox, pa.y - oy, pa.z - oz, pa.w};
+      a = c->velrhop + 4 * i;
+      h_vel[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+      a = c->idmassidx + 4 * i;
+      h_idm[i] = V4<T>{(T)a[0], (T)a[1], (T)i, (T)a[3]};
+      a = c->stress + 6 * i;
+      h_sa[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+      h_sb[i] = V2<T>{(T)a[4], (T)a[5]};
+      a = c->strain + 6 * i;
+      h_na[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+      h_nb[i] = V2<T>{(T)a[4], (T)a[5]};
+    }
+    for (size_t i = 0; i < npb; ++i) {
+      const double* a = c->normal + 4 * i;
+      h_nrm[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+    }
+    up(S.codes[0], h_codes);
+    up(S.cellpos[0], h_cell);
+    up(S.pos[0], h_pos);
+    up(S.pos_ori[0], h_ori);
+    up(S.vel[0], h_vel);
+    up(S.idm[0], h_idm);
+    up(S.str_a[0], h_sa);
+    up(S.str_b[0], h_sb);
+    up(S.stn_a[0], h_na);
+    up(S.stn_b[0], h_nb);
+    up(S.normal[0], h_nrm);
+
+    Dyn<T> d;
+    std::memset(&d, 0, sizeof(d));
+    d.time_d = q.time;
+    d.time_f = (T)q.time;
+    d.npm = q.npm;
+    for (int i = 0; i < P.n_motion; ++i) {
+      const rw_motion& m = q.motion[i];
+      Table<T>& tb = d.tab[i];
+      tb.is_translation = m.is_translation != 0;
+      tb.is_rotation = m.is_rotation != 0;
+      tb.n_trans = m.n_trans;
+      tb.n_rot = m.n_rot;
+      tb.pattern = m.pattern;
+      if (m.n_trans < 0 || m.n_trans > kTableMax || m.n_rot < 0 || m.n_rot > kTableMax)
+        throw Fail(RW_EINVAL, "motion table too long");
+      for (int j = 0; j < kTableMax; ++j) {
+        tb.trans_time[j] = (T)m.trans_time[j];
+        tb.rotat_time[j] = (T)m.rotat_time[j];
+        tb.trans_vel[j] = Vec3<T>{(T)m.trans_vel[j][0], (T)m.trans_vel[j][1], (T)m.trans_vel[j][2]};
+        tb.trans_acc[j] = Vec3<T>{(T)m.trans_acc[j][0], (T)m.trans_acc[j][1], (T)m.trans_acc[j][2]};
+        tb.rotat_acc[j] = Vec3<T>{(T)m.rotat_acc[j][0], (T)m.rotat_acc[j][1], (T)m.rotat_acc[j][2]};
+      }
+      tb.pos_rp = Vec3<T>{(T)m.pos_rp[0], (T)m.pos_rp[1], (T)m.pos_rp[2]};
+      tb.rotat_vel = Vec3<T>{(T)m.rotat_vel[0], (T)m.rotat_vel[1], (T)m.rotat_vel[2]};
+      Motion<T>& mv = d.mv[i];  // LoadParticles, src/loquat_io.cu:289-302
+      mv.is_trans = tb.is_translation;
+      mv.is_rotat = tb.is_rotation;
+      mv.trans_vel = tb.is_translation ? tb.trans_vel[0] : Vec3<T>{T(0), T(0), T(0)};
+      if (mv.is_rotat) {
+        mv.pattern = tb.pattern;
+        mv.pos_rp = tb.pos_rp;
+        mv.rotat_vel = tb.rotat_vel;
+      }
+    }
+    RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
+    RW_CU(cudaFuncSetAttribute(k_interaction<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               IX_CAP * IX_THREADS * (int)sizeof(unsigned)));
+    neighbor_search(0);
+    RW_CU(cudaStreamSynchronize(st));
+  }
+
+  // ------------------------------------------------------------------------------
+  // Stages.
+  // ------------------------------------------------------------------------------
+  void begin_step() override {
+    k_begin<T><<<1, 1, 0, st>>>(d_dyn);
+    check_launch();
+  }
+  void end_step() override {
+    k_end<T><<<1, 1, 0, st>>>(P, d_dyn);
+    check_launch();
+  }
+  void neighbor_search(int section) override {
+    const int np = P.np;
+    k_keys<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
+    if (np > 1) k_check_sorted<<<nblk(np - 1, 256), 256, 0, st>>>(S.keys, np, need_ptr());
+    for (int pass = 0; pass < S.sort_passes; ++pass) {
+      const int* ki = (pass & 1) ? S.tk : S.keys;
+      const int* vi = (pass & 1) ? S.tv : S.vals;
+      int* ko = (pass & 1) ? S.keys : S.tk;
+      int* vo = (pass & 1) ? S.vals : S.tv;
+      k_rs_upsweep<<<S.ntiles, RS_THREADS, 0, st>>>(ki, np, 8 * pass, S.hist, S.ntiles, need_ptr());
+      k_rs_scan<<<256, RS_THREADS, 0, st>>>(S.hist, S.ntiles, S.dtot, need_ptr());
+      k_rs_downsweep<<<S.ntiles, RS_THREADS, 0, st>>>(ki, vi, ko, vo, np, 8 * pass, S.hist, S.dtot, S.ntiles,
+                                                      need_ptr());
+    }
+    RW_CU(cudaMemsetAsync(S.range, 0, (size_t)P.ncell * sizeof(int2), st));
+    k_ranges<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
+    k_count<T><<<1, 1, 0, st>>>(P, S, d_dyn);
+    k_permute<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn, section, compat_contact ? 1 : 0);
+    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
+    check_launch();
+  }
+  void rigid() override {
+    if (P.n_motion <= 0) return;
+    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, -1, 1);
+    check_launch();
+  }
+  void adami() override {
+    if (P.npb == 0) return;
+    k_adami<T><<<nblk(P.npb, 128), 128, 0, st>>>(P, S, d_dyn);
+    check_launch();
+  }
+  void corner() override {
+    if (P.npm0 == 0) return;
+    k_corner<T><<<nblk(P.npm0, 128), 128, 0, st>>>(P, S, d_dyn, cpar);
+    check_launch();
+  }
+  void shepard_kernels(int only_filter_steps) {
+    if (P.npm0 == 0) return;
+    k_shepard<T><<<nblk(P.npm0, 128), 128, 0, st>>>(P, S, d_dyn, only_filter_steps);
+    k_shepard_store<T><<<nblk(P.npm0, 256), 256, 0, st>>>(P, S, d_dyn, only_filter_steps);
+    check_launch();
+  }
+  void shepard() override { shepard_kernels(0); }
+  void interaction() override {
+    const int n = P.np - P.npb;
+    if (n > 0) {
+      k_interaction<T><<<nblk(n, IX_THREADS), IX_THREADS, IX_CAP * IX_THREADS * sizeof(unsigned), st>>>(P, S, d_dyn,
+                                                                                                     cpar);
+      check_launch();
+    }
+    cpar ^= 1;
+  }
+  void predictor() override {
+    k_predictor<T><<<nblk(P.np, 256), 256, 0, st>>>(P, S, d_dyn);
+    check_launch();
+  }
+  void corrector() override {
+    k_corrector<T><<<nblk(P.npb + P.npm0, 256), 256, 0, st>>>(P, S, d_dyn);
+    check_launch();
+  }
+
+  // One whole step (RunSimulation's loop body, src/loquat.cu:548-561).
+  void launch_step() {
+    begin_step();
+    neighbor_search(0);
+    rigid();
+    adami();
+    corner();
+    if (P.stress_shepard_filter != 0) shepard_kernels(1);
+    interaction();
+    predictor();
+    neighbor_search(1);
+    adami();
+    corner();
+    interaction();
+    corrector();
+    end_step();
+  }
+
+  void step(int n) override {
+    if (n <= 0) return;
+    ensure_graph();
+    for (int k = 0; k < n; ++k) RW_CU(cudaGraphLaunch(gexec, st));
+  }
+
+  void ensure_graph() {
+    if (!gexec || g_cpar != cpar) {
+      if (gexec) {
+        cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      const int c0 = cpar;
+      RW_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        launch_step();
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        cpar = c0;
+        throw;
+      }
+      RW_CU(cudaStreamEndCapture(st, &g));
+      cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+      cudaGraphDestroy(g);
+      RW_CU(e);
+      cpar = c0;  // the step runs two interactions: parity is back where it started
+      g_cpar = c0;
+    }
+  }
+
+  // Kernels launched by one whole step (launch_step), for launch accounting.
+  int kernels_per_step() const {
+    const int search = 2 + 3 * S.sort_passes + 4;  // keys, check, sort passes, ranges, count, permute, flip
+    int k = 1 + 2 * search + 2 * 3 + 1 + 1 + 1;     // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
+    if (P.n_motion > 0) k += 1;
+    if (P.stress_shepard_filter != 0) k += 2;
+    if (P.npb == 0) k -= 2;
+    return k;
+  }
+
+  void profile(int nsteps, double* ms, int n, int* kps) override {
+    cudaEvent_t ev[RW_STAGE_COUNT_ + 1];
+    for (auto& e : ev) RW_CU(cudaEventCreate(&e));
+    std::vector<double> acc(RW_STAGE_COUNT_, 0.0);
+    for (int it = 0; it < nsteps; ++it) {
+      begin_step();
+      RW_CU(cudaEventRecord(ev[0], st));
+      neighbor_search(0);
+      RW_CU(cudaEventRecord(ev[1], st));
+      rigid();
+      RW_CU(cudaEventRecord(ev[2], st));
+      adami();
+      RW_CU(cudaEventRecord(ev[3], st));
+      corner();
+      if (P.stress_shepard_filter != 0) shepard_kernels(1);
+      RW_CU(cudaEventRecord(ev[4], st));
+      interaction();
+      RW_CU(cudaEventRecord(ev[5], st));
+      predictor();
+      RW_CU(cudaEventRecord(ev[6], st));
+      neighbor_search(1);
+      RW_CU(cudaEventRecord(ev[7], st));
+      adami();
+      RW_CU(cudaEventRecord(ev[8], st));
+      corner();
+      RW_CU(cudaEventRecord(ev[9], st));
+      interaction();
+      RW_CU(cudaEventRecord(ev[10], st));
+      corrector();
+      RW_CU(cudaEventRecord(ev[11], st));
+      end_step();
+      RW_CU(cudaEventSynchronize(ev[11]));
+      for (int k = 0; k < RW_STAGE_COUNT_; ++k) {
+        float t = 0.f;
+        RW_CU(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        acc[k] += t;
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < n && k < RW_STAGE_COUNT_; ++k) ms[k] = nsteps > 0 ? acc[k] / nsteps : 0.0;
+    if (kps) *kps = kernels_per_step();
+  }
+
+  double step_timed(int n) override {
+    cudaEvent_t e0, e1;
+    RW_CU(cudaEventCreate(&e0));
+    RW_CU(cudaEventCreate(&e1));
+    ensure_graph();  // capture outside the timed interval
+    RW_CU(cudaEventRecord(e0, st));
+    for (int k = 0; k < n; ++k) RW_CU(cudaGraphLaunch(gexec, st));
+    RW_CU(cudaEventRecord(e1, st));
+    RW_CU(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    RW_CU(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (double)ms;
+  }
+
+  int sync() override {
+    RW_CU(cudaStreamSynchronize(st));
+    Dyn<T> d = dyn_host();
+    if (d.err) {
+      err = "device error word " + std::to_string(d.err);
+      return RW_EDEVICE;
+    }
+    return RW_OK;
+  }
+
+  void info(rw_info* o) override {
+    Dyn<T> d = dyn_host();
+    std::memset(o, 0, sizeof(*o));
+    o->np = P.np;
+    o->npb = P.npb;
+    o->npm = d.npm;
+    o->np_delete_m = d.np_delete_m;
+    o->ncell = P.ncell;
+    o->step = d.step;
+    o->scalar_bytes = (int)sizeof(T);
+    o->device_err = (int)d.err;
+    for (int k = 0; k < 3; ++k) o->cell_num[k] = P.cell_num[k];
+    o->n_motion = P.n_motion;
+    o->time = d.time_d;
+    o->dt = (double)P.dt;
+    o->h = (double)P.h;
+  }
+
+  int set_option(int opt, double v) override {
+    if (opt == RW_OPT_WALL_FRICTION) {
+      P.wall_fric = (T)v;
+    } else if (opt == RW_OPT_COMPAT_CONTACT) {
+      if (v == 0.0) {
+        err = "contact state following particles (RW_OPT_COMPAT_CONTACT=0) is not available";
+        return RW_EINVAL;
+      }
+      compat_contact = true;
+    } else {
+      return RW_EINVAL;
+    }
+    if (gexec) {  // parameters are baked into the captured graph
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    return RW_OK;
+  }
+
+  // ------------------------------------------------------------------------------
+  // Arrays in the reference's layouts.
+  // ------------------------------------------------------------------------------
+  static size_t row_bytes(int which) {
+    switch (which) {
+      case RW_ARR_CODES: case RW_ARR_CELLPOS: return 16;
+      case RW_ARR_STR: case RW_ARR_STN: case RW_ARR_ACESTN: case RW_ARR_STR_INI: case RW_ARR_STN_INI: return 6 * sizeof(T);
+      case RW_ARR_CONTACT_MAG: return 9 * sizeof(T);
+      case RW_ARR_PART_IDX: case RW_ARR_CELL_BEG: case RW_ARR_CELL_END: return 4;
+      default: return 4 * sizeof(T);
+    }
+  }
+  size_t rows(int which) const {
+    if (which == RW_ARR_NORMAL) return P.npb;
+    if (which == RW_ARR_CELL_BEG || which == RW_ARR_CELL_END) return P.ncell;
+    return P.np;
+  }
+
+  int get_array(int which, void* dst, size_t bytes) override {
+    if (which < 0 || which >= RW_ARR_COUNT_) return RW_EINVAL;
+    const size_t n = rows(which);
+    if (bytes != n * row_bytes(which)) {
+      err = "rw_get_array: expected " + std::to_string(n * row_bytes(which)) + " bytes";
+      return RW_EINVAL;
+    }
+    RW_CU(cudaStreamSynchronize(st));
+    Dyn<T> d = dyn_host();
+    const int c = d.cur_main, cn = d.cur_nrm, ci = d.cur_ini;
+    T* o = (T*)dst;
+    auto put4 = [&](const V4<T>* src) {
+      auto h = down(src, n);
+      std::memcpy(dst, h.data(), n * sizeof(V4<T>));
+    };
+    auto put6 = [&](const V4<T>* a, const V2<T>* b) {
+      auto ha = down(a, n);
+      auto hb = down(b, n);
+      for (size_t i = 0; i < n; ++i) {
+        o[6 * i + 0] = ha[i].x; o[6 * i + 1] = ha[i].y; o[6 * i + 2] = ha[i].z;
+        o[6 * i + 3] = ha[i].w; o[6 * i + 4] = hb[i].x; o[6 * i + 5] = hb[i].y;
+      }
+    };
+    switch (which) {
+      case RW_ARR_CODES: { auto h = down(S.codes[c], n); std::memcpy(dst, h.data(), bytes); break; }
+      case RW_ARR_CELLPOS: { auto h = down(S.cellpos[c], n); std::memcpy(dst, h.data(), bytes); break; }
+      case RW_ARR_POSPRES: put4(S.pos[c]); break;
+      case RW_ARR_POSPRES_ORI: put4(S.pos_ori[c]); break;
+      case RW_ARR_VELRHOP: put4(S.vel[c]); break;
+      case RW_ARR_IDMASSIDX: put4(S.idm[c]); break;
+      case RW_ARR_STR: put6(S.str_a[c], S.str_b[c]); break;
+      case RW_ARR_STN: put6(S.stn_a[c], S.stn_b[c]); break;
+      case RW_ARR_NORMAL: put4(S.normal[cn]); break;
+      case RW_ARR_CONTACT_MAG: {
+        auto hf = down(S.cf[cpar], n);
+        auto hy = down(S.cny, n);
+        auto hz = down(S.cvz, n);
+        for (size_t i = 0; i < n; ++i) {
+          o[9 * i + 0] = hf[i].x; o[9 * i + 1] = hf[i].y; o[9 * i + 2] = hf[i].z;
+          o[9 * i + 3] = hy[i].x; o[9 * i + 4] = hy[i].y; o[9 * i + 5] = hy[i].z;
+          o[9 * i + 6] = hz[i].x; o[9 * i + 7] = hz[i].y; o[9 * i + 8] = hz[i].z;
+        }
+        break;
+      }
+      case RW_ARR_CONTACT_VAR: put4(S.cv[cpar]); break;
+      case RW_ARR_ACCAD: put4(S.accad); break;
+      case RW_ARR_SPIN: put4(S.spin); break;
+      case RW_ARR_ACESTN: put6(S.ace_a, S.ace_b); break;
+      case RW_ARR_POSPRES_INI: put4(S.pos_ini[ci]); break;
+      case RW_ARR_VELRHOP_INI: put4(S.vel_ini[ci]); break;
+      case RW_ARR_STR_INI: put6(S.stri_a[ci], S.stri_b[ci]); break;
+      case RW_ARR_STN_INI: put6(S.stni_a[ci], S.stni_b[ci]); break;
+      case RW_ARR_PART_IDX: {
+        int* oi = (int*)dst;
+        if (d.need_sort) {
+          auto h = down(S.sperm, n);
+          std::memcpy(oi, h.data(), bytes);
+        } else {
+          for (size_t i = 0; i < n; ++i) oi[i] = (int)i;
+        }
+        break;
+      }
+      case RW_ARR_CELL_BEG: case RW_ARR_CELL_END: {
+        auto h = down(S.range, n);
+        int* oi = (int*)dst;
+        for (size_t k = 0; k < n; ++k) {
+          const bool occ = h[k].y > h[k].x;
+          oi[k] = occ ? (which == RW_ARR_CELL_BEG ? h[k].x : h[k].y) : -1;
+        }
+        break;
+      }
+      case RW_ARR_POS_ABS: {
+        auto hp = down(S.pos[c], n);
+        auto hc = down(S.cellpos[c], n);
+        for (size_t i = 0; i < n; ++i) {
+          o[4 * i + 0] = hp[i].x + (T)hc[i].x * P.two_h;
+          o[4 * i + 1] = hp[i].y + (T)hc[i].y * P.two_h;
+          o[4 * i + 2] = hp[i].z + (T)hc[i].z * P.two_h;
+          o[4 * i + 3] = hp[i].w;
+        }
+        break;
+      }
+      default: return RW_EINVAL;
+    }
+    return RW_OK;
+  }
+
+  int set_array(int which, const void* src, size_t bytes) override {
+    if (which < 0 || which >= RW_ARR_COUNT_ || which == RW_ARR_POS_ABS || which == RW_ARR_PART_IDX ||
+        which == RW_ARR_CELL_BEG || which == RW_ARR_CELL_END)
+      return RW_EINVAL;
+    const size_t n = rows(which);
+    if (bytes != n * row_bytes(which)) {
+      err = "rw_set_array: expected " + std::to_string(n * row_bytes(which)) + " bytes";
+      return RW_EINVAL;
+    }
+    RW_CU(cudaStreamSynchronize(st));
+    Dyn<T> d = dyn_host();
+    const int c = d.cur_main, cn = d.cur_nrm, ci = d.cur_ini;
+    const T* s = (const T*)src;
+    auto get4 = [&](V4<T>* dstp) {
+      std::vector<V4<T>> h(n);
+      std::memcpy(h.data(), src, n * sizeof(V4<T>));
+      up(dstp, h);
+    };
+    auto get6 = [&](V4<T>* a, V2<T>* b) {
+      std::vector<V4<T>> ha(n);
+      std::vector<V2<T>> hb(n);
+      for (size_t i = 0; i < n; ++i) {
+        ha[i] = V4<T>{s[6 * i], s[6 * i + 1], s[6 * i + 2], s[6 * i + 3]};
+        hb[i] = V2<T>{s[6 * i + 4], s[6 * i + 5]};
+      }
+      up(a, ha);
+      up(b, hb);
+    };
+    switch (which) {
+      case RW_ARR_CODES: { std::vector<int4> h(n); std::memcpy(h.data(), src, bytes); up(S.codes[c], h); break; }
+      case RW_ARR_CELLPOS: { std::vector<int4> h(n); std::memcpy(h.data(), src, bytes); up(S.cellpos[c], h); break; }
+      case RW_ARR_POSPRES: get4(S.pos[c]); break;
+      case RW_ARR_POSPRES_ORI: get4(S.pos_ori[c]); break;
+      case RW_ARR_VELRHOP: get4(S.vel[c]); break;
+      case RW_ARR_IDMASSIDX: get4(S.idm[c]); break;
+      case RW_ARR_STR: get6(S.str_a[c], S.str_b[c]); break;
+      case RW_ARR_STN: get6(S.stn_a[c], S.stn_b[c]); break;
+      case RW_ARR_NORMAL: get4(S.normal[cn]); break;
+      case RW_ARR_CONTACT_MAG: {
+        std::vector<V4<T>> hf(n), hy(n), hz(n);
+        for (size_t i = 0; i < n; ++i) {
+          hf[i] = V4<T>{s[9 * i + 0], s[9 * i + 1], s[9 * i + 2], T(0)};
+          hy[i] = V4<T>{s[9 * i + 3], s[9 * i + 4], s[9 * i + 5], T(0)};
+          hz[i] = V4<T>{s[9 * i + 6], s[9 * i + 7], s[9 * i + 8], T(0)};
+        }
+        up(S.cf[cpar], hf);
+        up(S.cny, hy);
+        up(S.cvz, hz);
+        break;
+      }
+      case RW_ARR_CONTACT_VAR: get4(S.cv[cpar]); break;
+      case RW_ARR_ACCAD: get4(S.accad); break;
+      case RW_ARR_SPIN: get4(S.spin); break;
+      case RW_ARR_ACESTN: get6(S.ace_a, S.ace_b); break;
+      case RW_ARR_POSPRES_INI: get4(S.pos_ini[ci]); break;
+      case RW_ARR_VELRHOP_INI: get4(S.vel_ini[ci]); break;
+      case RW_ARR_STR_INI: get6(S.stri_a[ci], S.stri_b[ci]); break;
+      case RW_ARR_STN_INI: get6(S.stni_a[ci], S.stni_b[ci]); break;
+      default: return RW_EINVAL;
+    }
+    RW_CU(cudaStreamSynchronize(st));
+    return RW_OK;
+  }
+
+  void set_counters(double time, int step_, int npm, int np_delete_m) override {
+    Dyn<T> d = dyn_host();
+    d.time_d = time;
+    d.time_f = (T)time;
+    d.step = step_;
+    d.npm = npm;
+    d.np_delete_m = np_delete_m;
+    RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
+    RW_CU(cudaStreamSynchronize(st));
+  }
+
+  void wall_force(int mode, int wall_id, const double* strip, double* out) override {
+    double xmax, zmin, zmax;
+    if (strip) {
+      xmax = strip[0];
+      zmin = strip[1];
+      zmax = strip[2];
+    } else {  // the reference's strip, src/utilities.cu:619-621
+      xmax = (double)(T(0.04f) + P.bound_thickness + P.dr * T(3));
+      zmin = (double)(P.bound_thickness + T(0.04f));
+      zmax = (double)(P.bound_thickness + T(0.04f) + T(1.0f));
+    }
+    k_wall_force<T><<<WF_BLOCKS, WF_THREADS, 0, st>>>(P, S, d_dyn, cpar, mode, wall_id, xmax, zmin, zmax);
+    k_wall_force_final<<<1, 32, 0, st>>>(S.wsum, WF_BLOCKS);
+    check_launch();
+    RW_CU(cudaMemcpyAsync(out, S.wsum + 3 * WF_BLOCKS, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaStreamSynchronize(st));
+  }
+
+  // Saving (src/loquat.cu:439-482): output_N.xml + particles with the Shepard-smoothed
+  // stress (StressSavingRegularization, src/field_smoothing.cu:316-325) + time history.
+  void save(const char* outdir) override {
+    std::string dir = outdir ? outdir : ".";
+    ::mkdir(dir.c_str(), 0755);
+    Dyn<T> d = dyn_host();
+    const int c = d.cur_main;
+    const size_t np = P.np;
+    // tensor2d_cache = str, then Shepard over material particles into the cache.
+    RW_CU(cudaMemcpyAsync(S.tc_a, S.str_a[c], np * sizeof(V4<T>), cudaMemcpyDeviceToDevice, st));
+    RW_CU(cudaMemcpyAsync(S.tc_b, S.str_b[c], np * sizeof(V2<T>), cudaMemcpyDeviceToDevice, st));
+    if (P.npm0 > 0) {
+      k_shepard<T><<<nblk(P.npm0, 128), 128, 0, st>>>(P, S, d_dyn, 0);
+      check_launch();
+    }
+    Frame f;
+    f.np = P.np;
+    f.npb = P.npb;
+    f.npm = d.npm;
+    auto conv4 = [&](int which, std::vector<double>& o, size_t nrow) {
+      std::vector<T> h(4 * nrow);
+      if (nrow) {
+        int rc = get_array(which, h.data(), h.size() * sizeof(T));
+        if (rc) throw Fail(rc, "save: array export failed");
+      }
+      o.assign(h.begin(), h.end());
+    };
+    f.codes.resize(4 * np);
+    if (get_array(RW_ARR_CODES, f.codes.data(), 16 * np)) throw Fail(RW_ECUDA, "save: codes");
+    conv4(RW_ARR_POS_ABS, f.pos, np);
+    conv4(RW_ARR_VELRHOP, f.vel, np);
+    conv4(RW_ARR_ACCAD, f.acc, np);
+    conv4(RW_ARR_IDMASSIDX, f.idm, np);
+    conv4(RW_ARR_NORMAL, f.normal, P.npb);
+    std::vector<T> h6(6 * np);
+    get6_cache(h6);
+    f.str.assign(h6.begin(), h6.end());
+    if (get_array(RW_ARR_STN, h6.data(), h6.size() * sizeof(T))) throw Fail(RW_ECUDA, "save: stn");
+    f.stn.assign(h6.begin(), h6.end());
+    output_number++;
+    const std::string xmlp = dir + "/output_" + std::to_string(output_number) + ".xml";
+    int rc = write_output_xml(xmlp, cparams, P.np, P.npb, d.npm, d.time_d, (double)P.dt, output_number);
+    if (rc) throw Fail(rc, "cannot write " + xmlp);
+    if (P.output_format == 1) rc = write_frame_dat(dir + "/" + std::to_string(output_number) + ".dat", f);
+    else rc = write_frame_vtu(dir, output_number, f);
+    if (rc) throw Fail(rc, "cannot write particle output in " + dir);
+    double wf[3];
+    wall_force(1, 10, nullptr, wf);
+    std::FILE* th = std::fopen((dir + "/time_history.txt").c_str(), "a");
+    if (!th) throw Fail(RW_EIO, "cannot write time_history.txt");
+    std::fprintf(th, "%.9g %.9g\n", (double)d.time_f, 0.001 * wf[0]);
+    std::fclose(th);
+  }
+  void get6_cache(std::vector<T>& o) {
+    const size_t n = P.np;
+    auto ha = down(S.tc_a, n);
+    auto hb = down(S.tc_b, n);
+    for (size_t i = 0; i < n; ++i) {
+      o[6 * i + 0] = ha[i].x; o[6 * i + 1] = ha[i].y; o[6 * i + 2] = ha[i].z;
+      o[6 * i + 3] = ha[i].w; o[6 * i + 4] = hb[i].x; o[6 * i + 5] = hb[i].y;
+    }
+  }
+};
+
+}  // namespace rw
+
+// ===================================================================================
+// C ABI
+// ===================================================================================
+struct rw_ctx {
+  std::unique_ptr<rw::EngineBase> eng;
+};
+
+using rw::Fail;
+
+template <class F> static rw_status guarded(rw_ctx* ctx, F fn) {
+  if (!ctx || !ctx->eng) return RW_EINVAL;
+  try {
+    cudaSetDevice(ctx->eng->device);
+    return fn(*ctx->eng);
+  } catch (const Fail& f) {
+    ctx->eng->err = f.what();
+    return f.code;
+  } catch (const std::bad_alloc&) {
+    ctx->eng->err = "host allocation failed";
+    return RW_ENOMEM;
+  } catch (const std::exception& e) {
+    ctx->eng->err = e.what();
+    return RW_EINVAL;
+  }
+}
+
+extern "C" {
+
+const char* rw_status_string(rw_status s) {
+  static const char* names[] = {"RW_OK", "RW_EINVAL", "RW_ENOENT", "RW_EIO", "RW_EFORMAT",
+                                "RW_ECUDA", "RW_ENOMEM", "RW_EDEVICE", "RW_ETIMEDOUT", "RW_ESTATE"};
+  return (s >= 0 && s <= RW_ESTATE) ? names[s] : "RW_UNKNOWN";
+}
+
+const char* rw_last_error(const rw_ctx* ctx) {
+  if (!ctx || !ctx->eng) return rw::g_create_err.c_str();
+  return ctx->eng->err.c_str();
+}
+
+rw_status rw_create_from_case(const rw_case* c, int device, int precision, rw_ctx** out) {
+  if (!c || !out) return RW_EINVAL;
+  *out = nullptr;
+  if (precision != 4 && precision != 8) {
+    rw::g_create_err = "precision must be 4 or 8";
+    return RW_EINVAL;
+  }
+  std::unique_ptr<rw::EngineBase> e;
+  try {
+    if (precision == 4) {
+      auto p = std::make_unique<rw::Engine<float>>();
+      p->create(c, device);
+      e = std::move(p);
+    } else {
+      auto p = std::make_unique<rw::Engine<double>>();
+      p->create(c, device);
+      e = std::move(p);
+    }
+  } catch (const Fail& f) {
+    rw::g_create_err = f.what();
+    return f.code;
+  } catch (const std::bad_alloc&) {
+    rw::g_create_err = "host allocation failed";
+    return RW_ENOMEM;
+  } catch (const std::exception& ex) {
+    rw::g_create_err = ex.what();
+    return RW_EINVAL;
+  }
+  *out = new rw_ctx{std::move(e)};
+  return RW_OK;
+}
+
+rw_status rw_create(const char* project, int device, int precision, rw_ctx** out) {
+  if (!project || !out) return RW_EINVAL;
+  rw::HostCase hc;
+  std::string msg;
+  int rc = rw::read_project(project, &hc, &msg);
+  if (rc) {
+    rw::g_create_err = msg;
+    return rc;
+  }
+  rw_case view = hc.view();
+  return rw_create_from_case(&view, device, precision, out);
+}
+
+rw_status rw_destroy(rw_ctx* ctx) {
+  if (!ctx) return RW_EINVAL;
+  if (ctx->eng) cudaSetDevice(ctx->eng->device);
+  delete ctx;
+  return RW_OK;
+}
+
+#define RW_STAGE(fn, body) \
+  rw_status fn(rw_ctx* ctx) { return guarded(ctx, [&](rw::EngineBase& e) { body; return RW_OK; }); }
+
+RW_STAGE(rw_begin_step, e.begin_step())
+RW_STAGE(rw_rigid_body_update, e.rigid())
+RW_STAGE(rw_adami_boundary, e.adami())
+RW_STAGE(rw_find_corner, e.corner())
+RW_STAGE(rw_shepard_filter, e.shepard())
+RW_STAGE(rw_particle_interaction, e.interaction())
+RW_STAGE(rw_predictor, e.predictor())
+RW_STAGE(rw_corrector, e.corrector())
+RW_STAGE(rw_end_step, e.end_step())
+
+rw_status rw_neighbor_search(rw_ctx* ctx, int section) {
+  if (section != 0 && section != 1) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { e.neighbor_search(section); return RW_OK; });
+}
+
+rw_status rw_step(rw_ctx* ctx, int nsteps) {
+  if (nsteps < 0) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { e.step(nsteps); return RW_OK; });
+}
+
+rw_status rw_step_timed(rw_ctx* ctx, int nsteps, double* ms) {
+  if (nsteps < 1 || !ms) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { *ms = e.step_timed(nsteps); return RW_OK; });
+}
+
+rw_status rw_synchronize(rw_ctx* ctx) {
+  return guarded(ctx, [&](rw::EngineBase& e) { return e.sync(); });
+}
+
+rw_status rw_wall_force(rw_ctx* ctx, int mode, int wall_id, const double* strip, double out_xyz[3]) {
+  if (!out_xyz || (mode != 0 && mode != 1)) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { e.wall_force(mode, wall_id, strip, out_xyz); return RW_OK; });
+}
+
+rw_status rw_save(rw_ctx* ctx, const char* outdir) {
+  return guarded(ctx, [&](rw::EngineBase& e) { e.save(outdir); return RW_OK; });
+}
+
+rw_status rw_get_info(rw_ctx* ctx, rw_info* out) {
+  if (!out) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { e.info(out); return RW_OK; });
+}
+
+rw_status rw_set_option(rw_ctx* ctx, int option, double value) {
+  return guarded(ctx, [&](rw::EngineBase& e) { return e.set_option(option, value); });
+}
+
+rw_status rw_get_array(rw_ctx* ctx, int which, void* host_dst, size_t bytes) {
+  if (!host_dst) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { return e.get_array(which, host_dst, bytes); });
+}
+
+rw_status rw_set_array(rw_ctx* ctx, int which, const void* host_src, size_t bytes) {
+  if (!host_src) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { return e.set_array(which, host_src, bytes); });
+}
+
+rw_status rw_profile(rw_ctx* ctx, int nsteps, double* ms_per_stage, int n_stages, int* kernels_per_step) {
+  if (nsteps < 0 || (n_stages > 0 && !ms_per_stage)) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) {
+    e.profile(nsteps, ms_per_stage, n_stages, kernels_per_step);
+    return RW_OK;
+  });
+}
+
+rw_status rw_set_counters(rw_ctx* ctx, double time, int step, int npm, int np_delete_m) {
+  return guarded(ctx, [&](rw::EngineBase& e) { e.set_counters(time, step, npm, np_delete_m); return RW_OK; });
+}
+
+}  // extern "C"

@@ -1,0 +1,1017 @@
+// Kernels of the SPH geomechanics step (sm_100a).  Layout in HBM: structure of
+// arrays, one 16-byte (float) / 32-byte (double) vector per particle per field,
+// particles sorted by cell key (boundary cells first, then material cells, then the
+// deleted cell), so the 27 neighbour cells of a particle are 9 contiguous index runs
+// per layer and neighbour reads of consecutive particles hit the same lines.
+#pragma once
+#include "rw_device.cuh"
+#include "rw_params.h"
+
+namespace rw {
+
+// Per-particle record consumed by the pair loop of the interaction: everything the
+// reference recomputes per neighbour pair from j's state (mass, volume, sigma/rho^2,
+// artificial-stress term) computed once per particle per section.
+template <class T> struct Rec {
+  V4<T> vr;   // velocity xyz, density
+  V4<T> aux;  // mass, volume = mass/rho, artificial-stress term of j, contact-wall flag
+  V4<T> sa;   // sigma/rho^2: xx yy zz xy
+  V4<T> sb;   // sigma/rho^2: xz yz
+};
+
+template <class T> struct DevState {
+  // Permuted every section (ping-pong, Dyn::cur_main selects the live buffer).
+  int4* codes[2];
+  int4* cellpos[2];
+  V4<T>* pos[2];
+  V4<T>* pos_ori[2];
+  V4<T>* vel[2];
+  V4<T>* idm[2];
+  V4<T>* str_a[2];
+  V2<T>* str_b[2];
+  V4<T>* stn_a[2];
+  V2<T>* stn_b[2];
+  // Permuted in the predictor section only (SortArraysPrimary), Dyn::cur_nrm.
+  V4<T>* normal[2];
+  // Permuted in the corrector section only (SortArraysAll), Dyn::cur_ini.
+  V4<T>* pos_ini[2];
+  V4<T>* vel_ini[2];
+  V4<T>* stri_a[2];
+  V2<T>* stri_b[2];
+  V4<T>* stni_a[2];
+  V2<T>* stni_b[2];
+  // Stage outputs, indexed like the live buffers.
+  V4<T>* accad;
+  V4<T>* spin;
+  V4<T>* ace_a;
+  V2<T>* ace_b;
+  // Contact state bound to array slots, as in the reference (never permuted there).
+  // contact_var and the contact force are double-buffered across the interaction so
+  // that every particle reads the others' values as of the start of the stage.
+  V4<T>* cv[2];   // kernel integral, distance along normal, slide flag, wall id
+  V4<T>* cf[2];   // contact force xyz
+  V4<T>* cny;     // contact normal (contact_mag.yx..yz)
+  V4<T>* cvz;     // contact velocity (contact_mag.zx..zz)
+  Rec<T>* rec;
+  V4<T>* tc_a;    // Shepard result (tensor2d_cache)
+  V2<T>* tc_b;
+  // Cell list.
+  int* keys;      // cell key per particle (unsorted order)
+  int* vals;
+  int* tk;        // radix-sort ping-pong
+  int* tv;
+  const int* skeys;  // sorted keys / permutation (one of keys|tk, vals|tv)
+  const int* sperm;
+  int2* range;    // [beg, end) per cell, (0,0) when empty
+  int* hist;      // radix-sort digit counts, 256 x ntiles
+  int* dtot;      // per-digit totals
+  int ntiles, sort_passes;
+  double* wsum;   // wall-force partial sums
+};
+
+template <class T> RWD V3<T> ld3(const V4<T>* p, int i) { V4<T> v = p[i]; return {v.x, v.y, v.z}; }
+template <class T> RWD S6<T> ld6(const V4<T>* a, const V2<T>* b, int i) {
+  V4<T> x = a[i];
+  V2<T> y = b[i];
+  return {x.x, x.y, x.z, x.w, y.x, y.y};
+}
+template <class T> RWD void st6(V4<T>* a, V2<T>* b, int i, S6<T> s) {
+  a[i] = V4<T>{s.xx, s.yy, s.zz, s.xy};
+  b[i] = V2<T>{s.xz, s.yz};
+}
+template <class T> RWD bool in_grid(const Params<T>& P, I3 c) {
+  return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < P.cell_num[0] && c.y < P.cell_num[1] && c.z < P.cell_num[2];
+}
+template <class T> RWD int key_of(const Params<T>& P, I3 c) {
+  return c.x * P.cell_num[1] * P.cell_num[2] + c.y * P.cell_num[2] + c.z;
+}
+RWD I3 off_of(int oc) { return {oc % 3 - 1, (oc / 3) % 3 - 1, oc / 9 - 1}; }
+
+RWD float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+RWD double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+RWD float add_rn(float a, float b) { return __fadd_rn(a, b); }
+RWD double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// Neighbour record of particle i (boundary: mass = V0 rho; material: idmassidx.y),
+// with the reference's per-pair expressions (src/particle_interaction.cu:44-49,71,98-104).
+template <class T> RWD void write_rec(const Params<T>& P, Rec<T>* rec, int i, V4<T> vr, S6<T> s, T mass, bool contact) {
+  T rho = vr.w;
+  S6<T> sor = s / (rho * rho);
+  T vol = mass / rho;
+  T rj = T(0.0f);
+  if (P.art_coef != T(0.f)) {
+    rj = trace(sor);
+    if (rj > T(0.0f)) rj *= P.art_coef;
+    else rj = T(0.0f);
+  }
+  Rec<T> r;
+  r.vr = vr;
+  r.aux = V4<T>{mass, vol, rj, contact ? T(1) : T(0)};
+  r.sa = V4<T>{sor.xx, sor.yy, sor.zz, sor.xy};
+  r.sb = V4<T>{sor.xz, sor.yz, T(0), T(0)};
+  rec[i] = r;
+}
+
+// ---------------------------------------------------------------------------------
+// Cell list: keys, stable radix sort, ranges, gather-permute
+// (src/loquat_grid.cu:140-320, src/loquat.cu:254-287).
+// ---------------------------------------------------------------------------------
+
+// cuGetParticleCellIndex (src/loquat_grid.cu:140-164).  A live particle whose cell is
+// outside the grid would make the reference write out of bounds; here its key is
+// clamped into the grid and RW_DERR_CELL_RANGE is raised.
+template <class T> __global__ void k_keys(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) dyn->need_sort = 0;
+  if (i >= P.np) return;
+  const int c = dyn->cur_main;
+  int4 cp = S.cellpos[c][i];
+  int key;
+  if (cp.w == P.ncell_delete_m) {
+    key = P.ncell_delete_m;
+  } else {
+    I3 cc{cp.x, cp.y, cp.z};
+    if (!in_grid(P, cc)) {
+      atomicOr(&dyn->err, 1u);
+      cc.x = min(max(cc.x, 0), P.cell_num[0] - 1);
+      cc.y = min(max(cc.y, 0), P.cell_num[1] - 1);
+      cc.z = min(max(cc.z, 0), P.cell_num[2] - 1);
+    }
+    key = key_of(P, cc);
+    if (!(S.idm[c][i].x < T(RW_MATERIAL_NUMBER))) key += P.ncell_material;
+    S.cellpos[c][i].w = key;
+  }
+  S.keys[i] = key;
+  S.vals[i] = i;
+}
+
+__global__ void k_check_sorted(const int* keys, int n, int* need_sort) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i < n && keys[i - 1] > keys[i]) *need_sort = 1;
+}
+
+constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
+
+// LSD radix sort, 8-bit digits, stable: upsweep (per-tile digit counts), scan
+// (per digit over tiles), downsweep (stable in-tile ranks + scatter).  All three
+// return immediately when the keys are already in order (the permutation is then
+// the identity, exactly what a stable sort of sorted keys returns).
+__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const int* keys, int n, int shift, int* hist, int ntiles,
+                                                         const int* need) {
+  if (!*need) return;
+  __shared__ int h[256];
+  const int t = threadIdx.x;
+  h[t] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * RS_TILE;
+#pragma unroll
+  for (int k = 0; k < RS_ITEMS; ++k) {
+    int idx = base + k * RS_THREADS + t;
+    if (idx < n) atomicAdd(&h[(keys[idx] >> shift) & 255], 1);
+  }
+  __syncthreads();
+  hist[t * ntiles + blockIdx.x] = h[t];
+}
+
+__device__ __forceinline__ int block_excl_scan256(int v, int* total) {
+  __shared__ int ws[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = lane < 8 ? ws[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < 8) ws[lane] = s;
+  }
+  __syncthreads();
+  int incl = x + (w > 0 ? ws[w - 1] : 0);
+  if (total) *total = ws[7];
+  __syncthreads();
+  return incl - v;
+}
+
+// One block per digit: exclusive scan of that digit's per-tile counts.
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scan(int* hist, int ntiles, int* dtot, const int* need) {
+  if (!*need) return;
+  int* row = hist + blockIdx.x * ntiles;
+  const int per = (ntiles + RS_THREADS - 1) / RS_THREADS;
+  const int b = threadIdx.x * per, e = min(ntiles, b + per);
+  int s = 0;
+  for (int k = b; k < e; ++k) s += row[k];
+  int total;
+  int off = block_excl_scan256(s, &total);
+  for (int k = b; k < e; ++k) {
+    int v = row[k];
+    row[k] = off;
+    off += v;
+  }
+  if (threadIdx.x == 0) dtot[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const int* kin, const int* vin, int* kout, int* vout, int n,
+                                                           int shift, const int* hist, const int* dtot, int ntiles,
+                                                           const int* need) {
+  if (!*need) return;
+  __shared__ int base[256];
+  __shared__ int wcnt[8][257];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  int dt_excl = block_excl_scan256(dtot[t], nullptr);
+  base[t] = dt_excl + hist[t * ntiles + blockIdx.x];
+  const unsigned lt = (1u << lane) - 1u;
+  const int tile0 = blockIdx.x * RS_TILE;
+  for (int r = 0; r < RS_ITEMS; ++r) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) wcnt[q][t] = 0;
+    __syncthreads();
+    const int idx = tile0 + r * RS_THREADS + t;
+    const bool valid = idx < n;
+    int key = 0, d = 256;
+    if (valid) {
+      key = kin[idx];
+      d = (key >> shift) & 255;
+    }
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    int rank = __popc(peers & lt);
+    int leader = __ffs(peers) - 1;
+    if (lane == leader && valid) wcnt[w][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      int pre = 0;
+      for (int q = 0; q < w; ++q) pre += wcnt[q][d];
+      int pos = base[d] + pre + rank;
+      if (pos >= 0 && pos < n) {  // always true for consistent counts; guards the scatter
+        kout[pos] = key;
+        vout[pos] = vin[idx];
+      }
+    }
+    __syncthreads();
+    int add = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) add += wcnt[q][t];
+    base[t] += add;
+    __syncthreads();
+  }
+}
+
+// cuFindBegEndInCell (src/loquat_grid.cu:185-213): [beg, end) of every occupied cell.
+template <class T> __global__ void k_ranges(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.np) return;
+  const int* K = dyn->need_sort ? S.skeys : S.keys;
+  const int k = K[i];
+  int* r = reinterpret_cast<int*>(S.range);
+  if (i == 0 || K[i - 1] != k) r[2 * k] = i;
+  if (i == P.np - 1 || K[i + 1] != k) r[2 * k + 1] = i + 1;
+}
+
+// Deleted-particle accounting (src/loquat_grid.cu:234-254), on the device.
+template <class T> __global__ void k_count(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
+  int2 d = S.range[P.ncell_delete_m];
+  int cnt = d.y - d.x;
+  if (cnt > 0) {
+    int now = cnt - dyn->np_delete_m;
+    if (now != 0) {
+      dyn->npm -= now;
+      dyn->np_delete_m += now;
+    }
+  }
+  if (P.npb + dyn->npm + dyn->np_delete_m != P.np) atomicOr(&dyn->err, 2u);
+}
+
+// SortArraysPrimary (section 0) / SortArraysAll (section 1), src/loquat.cu:254-287,
+// as one gather into the other ping-pong buffer.  Stress/strain beyond npb+npm are
+// not part of the reference's sorted range; they keep their slot values.
+template <class T> __global__ void k_permute(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, int section,
+                                             int compat_contact) {
+  if (!dyn->need_sort) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.np) return;
+  int j = S.sperm[i];
+  if (j < 0 || j >= P.np) {  // a valid permutation never gets here
+    atomicOr(&const_cast<Dyn<T>*>(dyn)->err, 8u);
+    j = i;
+  }
+  const int c = dyn->cur_main, n = c ^ 1;
+  S.codes[n][i] = S.codes[c][j];
+  S.cellpos[n][i] = S.cellpos[c][j];
+  S.pos[n][i] = S.pos[c][j];
+  S.pos_ori[n][i] = S.pos_ori[c][j];
+  S.vel[n][i] = S.vel[c][j];
+  S.idm[n][i] = S.idm[c][j];
+  const int npm = dyn->npm;
+  const int nbm = P.npb + npm;
+  const bool perm_str = (section == 0) || (npm != 0);
+  const int ss = (perm_str && i < nbm) ? j : i;
+  S.str_a[n][i] = S.str_a[c][ss];
+  S.str_b[n][i] = S.str_b[c][ss];
+  S.stn_a[n][i] = S.stn_a[c][ss];
+  S.stn_b[n][i] = S.stn_b[c][ss];
+  if (section == 0) {
+    const int cn = dyn->cur_nrm;
+    if (i < P.npb) S.normal[cn ^ 1][i] = S.normal[cn][j];
+  } else {
+    const int ci = dyn->cur_ini, ni = ci ^ 1;
+    S.pos_ini[ni][i] = S.pos_ini[ci][j];
+    S.vel_ini[ni][i] = S.vel_ini[ci][j];
+    S.stri_a[ni][i] = S.stri_a[ci][ss];
+    S.stri_b[ni][i] = S.stri_b[ci][ss];
+    S.stni_a[ni][i] = S.stni_a[ci][ss];
+    S.stni_b[ni][i] = S.stni_b[ci][ss];
+  }
+  (void)compat_contact;
+}
+
+// Buffer flip after a permute; in the predictor section also RigidBodyUpdate
+// (src/adami_boundary.cu:175-203), which the reference runs right after the sort.
+// Plain round-to-nearest products/sums, as the reference's host code computes.
+template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int section, int rigid) {
+  if (section >= 0 && dyn->need_sort) {
+    dyn->cur_main ^= 1;
+    if (section == 0) dyn->cur_nrm ^= 1;
+    else dyn->cur_ini ^= 1;
+  }
+  if (!rigid) return;
+  const T dt = P.dt;
+  const T time = dyn->time_f;
+  for (int i = 0; i < P.n_motion; ++i) {
+    Table<T>& tb = dyn->tab[i];
+    Motion<T>& mv = dyn->mv[i];
+    if (tb.is_rotation) {
+      for (int j = 0; j < tb.n_rot; ++j) {
+        if (time < tb.rotat_time[j]) {
+          tb.rotat_vel.x = add_rn(tb.rotat_vel.x, mul_rn(tb.rotat_acc[j].x, dt));
+          tb.rotat_vel.y = add_rn(tb.rotat_vel.y, mul_rn(tb.rotat_acc[j].y, dt));
+          tb.rotat_vel.z = add_rn(tb.rotat_vel.z, mul_rn(tb.rotat_acc[j].z, dt));
+          const T hdt = (T)(0.5 * (double)dt);
+          Vec3<T> vel{add_rn(tb.trans_vel[j].x, mul_rn(tb.trans_acc[j].x, hdt)),
+                      add_rn(tb.trans_vel[j].y, mul_rn(tb.trans_acc[j].y, hdt)),
+                      add_rn(tb.trans_vel[j].z, mul_rn(tb.trans_acc[j].z, hdt))};
+          tb.pos_rp.x = add_rn(tb.pos_rp.x, mul_rn(vel.x, dt));
+          tb.pos_rp.y = add_rn(tb.pos_rp.y, mul_rn(vel.y, dt));
+          tb.pos_rp.z = add_rn(tb.pos_rp.z, mul_rn(vel.z, dt));
+          mv.rotat_acc = tb.rotat_acc[j];
+          mv.rotat_vel = tb.rotat_vel;
+          mv.pos_rp = tb.pos_rp;
+          break;
+        }
+      }
+    }
+    if (tb.is_translation) {
+      for (int j = 0; j < tb.n_trans; ++j) {
+        if (time < tb.trans_time[j]) {
+          tb.trans_vel[j].x = add_rn(tb.trans_vel[j].x, mul_rn(tb.trans_acc[j].x, dt));
+          tb.trans_vel[j].y = add_rn(tb.trans_vel[j].y, mul_rn(tb.trans_acc[j].y, dt));
+          tb.trans_vel[j].z = add_rn(tb.trans_vel[j].z, mul_rn(tb.trans_acc[j].z, dt));
+          mv.trans_acc = tb.trans_acc[j];
+          mv.trans_vel = tb.trans_vel[j];
+          break;
+        }
+      }
+    }
+  }
+}
+
+template <class T> __global__ void k_begin(Dyn<T>* dyn) { dyn->time_f = (T)dyn->time_d; }
+template <class T> __global__ void k_end(const Params<T> P, Dyn<T>* dyn) {
+  dyn->time_d += (double)P.dt;
+  dyn->step += 1;
+}
+
+// ---------------------------------------------------------------------------------
+// Adami boundary (src/adami_boundary.cu:26-158).
+// ---------------------------------------------------------------------------------
+template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.npb || dyn->npm == 0) return;
+  const int c = dyn->cur_main;
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const V4<T>* __restrict__ vel = S.vel[c];
+  const V4<T>* __restrict__ idm = S.idm[c];
+  const V4<T>* __restrict__ sa = S.str_a[c];
+  const V2<T>* __restrict__ sb = S.str_b[c];
+  const V3<T> pos_i = ld3(pos, i);
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  const int4 code = S.codes[c][i];
+  const bool contact = code.x >= 10;
+  S6<T> rs = zero6<T>();
+  V4<T> rps{T(0), T(0), T(0), T(0)}, rvr{T(0), T(0), T(0), T(0)};
+  V3<T> n_i{T(0), T(0), T(0)};
+  const T th = P.two_h;
+  for (int oc = 0; oc < 27; ++oc) {
+    const I3 off = off_of(oc);
+    const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+    if (!in_grid(P, cj)) continue;
+    const int k = key_of(P, cj);
+    const V3<T> o = mulI(off, th);
+    if (contact) {
+      const int2 rg = S.range[k];
+      for (int j = rg.x; j < rg.y; ++j) {
+        V3<T> dr = pos_i - ld3(pos, j);
+        dr = dr - o;
+        T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+        T q = r * P.i_h;
+        if (q < T(2.0f)) {
+          T dwdr = kernel_f(P.kgrad, q);
+          V3<T> gker = dr * dwdr;
+          n_i = n_i - gker * P.vol_def;
+        }
+      }
+    }
+    const int2 rg = S.range[k + P.ncell_material];
+    for (int j = rg.x; j < rg.y; ++j) {
+      V3<T> dr = pos_i - ld3(pos, j);
+      dr = dr - o;
+      T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+      T q = r * P.i_h;
+      if (q < T(2.0f)) {
+        T ker = kernel_w(P.knorm, q);
+        V4<T> vj = vel[j];
+        T mj = idm[j].y;
+        T vol_j = mj / vj.w;
+        T kv = ker * vol_j;
+        rs = rs + ld6(sa, sb, j) * kv;
+        rps = rps + v4(dr * (ker * mj), kv);
+        rvr = rvr + vj * kv;
+      }
+    }
+  }
+  if (enorm(n_i) > T(0)) {
+    T nn = enorm(n_i);
+    S.cny[i] = V4<T>{n_i.x / nn, n_i.y / nn, n_i.z / nn, T(0)};
+  }
+  V4<T> vr_out = vel[i];
+  S6<T> str_out;
+  if (rps.w > T(0.0f)) {
+    const T kersum = rps.w;
+    const V3<T> dr_ref = xyz(rps);
+    const V4<T> nrm4 = S.normal[dyn->cur_nrm][i];
+    const T fcoef = nrm4.w;
+    const V3<T> nrm = xyz(nrm4);
+    const V3<T> vel_ref = xyz(rvr) / kersum;
+    const V3<T> vel_ref_n = nrm * dot(nrm, vel_ref);
+    const V3<T> vel_ref_t = vel_ref - vel_ref_n;
+    V3<T> vel_rb{T(0.0f), T(0.0f), T(0.0f)};
+    if (code.y == 1) {
+      const Motion<T>& mv = dyn->mv[code.w];
+      vel_rb = V3<T>{mv.trans_vel.x, mv.trans_vel.y, mv.trans_vel.z};
+      if (mv.is_rotat) {
+        V3<T> pabs = pos_i + mulI(celli, T(2.0f) * P.h);
+        V3<T> rp{mv.pos_rp.x, mv.pos_rp.y, mv.pos_rp.z};
+        V3<T> w{mv.rotat_vel.x, mv.rotat_vel.y, mv.rotat_vel.z};
+        vel_rb = vel_rb + cross(w, pabs - rp);
+      }
+    }
+    const V3<T> vel_rb_n = nrm * dot(nrm, vel_rb);
+    const V3<T> vel_rb_t = vel_rb - vel_rb_n;
+    const V3<T> vel_ext_n = vel_rb_n * T(2.0f) - vel_ref_n;
+    const V3<T> vel_ext_t = fcoef == T(-1.0f) ? vel_rb_t * T(2.0f) - vel_ref_t : vel_ref_t;
+    const V3<T> vel_ext = vel_ext_n + vel_ext_t;
+    const T rho = rvr.w / kersum;
+    vr_out = v4(vel_ext, rho);
+    if (contact) {
+      vr_out = v4(vel_rb, rho);
+      S.cvz[i] = V4<T>{vel_ext.x, vel_ext.y, vel_ext.z, T(0)};
+    }
+    const S6<T> str_ref = rs / kersum;
+    const V3<T> g{P.gravity[0], P.gravity[1], P.gravity[2]};
+    str_out = subdiag(str_ref, (g * dr_ref) / kersum);
+    S.vel[c][i] = vr_out;
+  } else {
+    str_out = zero6<T>();
+  }
+  st6(S.str_a[c], S.str_b[c], i, str_out);
+  write_rec(P, S.rec, i, vr_out, str_out, P.vol_def * vr_out.w, contact);
+}
+
+// ---------------------------------------------------------------------------------
+// Nearest contact-wall particle / corner rule (src/adami_boundary.cu:209-292), plus
+// the material neighbour records for the interaction.
+// ---------------------------------------------------------------------------------
+template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
+                                                                  int cpar) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int npm = dyn->npm;
+  if (t >= npm) return;
+  const int i = P.npb + t;
+  const int c = dyn->cur_main;
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const V3<T> pos_i = ld3(pos, i);
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  V4<T> cv = S.cv[cpar][i];
+  cv.x = T(0.0f);
+  cv.y = T(999);
+  T d_ij = T(999);
+  V4<T> ny = S.cny[i];
+  V4<T> vz = S.cvz[i];
+  const T th = P.two_h;
+  if (P.npb > 0) {
+    for (int oc = 0; oc < 27; ++oc) {
+      const I3 off = off_of(oc);
+      const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+      if (!in_grid(P, cj)) continue;
+      const int2 rg = S.range[key_of(P, cj)];
+      const V3<T> o = mulI(off, th);
+      for (int j = rg.x; j < rg.y; ++j) {
+        V3<T> dr = pos_i - ld3(pos, j) - o;
+        T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+        T q = r * P.i_h;
+        if ((double)q < 2.0) {
+          const int codej = S.codes[c][j].x;
+          if (codej >= 10) {
+            T dwdr = kernel_f(P.kgrad, q);
+            V3<T> gker = dr * dwdr;
+            if (r < d_ij && r > T(0)) {
+              const V4<T> na4 = S.cny[j];
+              const V3<T> n_ad{na4.x, na4.y, na4.z};
+              const V3<T> n_mat = dr / r;
+              d_ij = r;
+              cv.y = f_abs(dot(dr, n_ad));
+              cv.w = (T)codej;
+              const V4<T> vj = S.vel[c][j];
+              vz = V4<T>{vj.x, vj.y, vj.z, T(0)};
+              const T cos_c = T(0.866f);
+              const T cos_n = f_abs(dot(n_mat, n_ad));
+              if (cos_n < cos_c) ny = V4<T>{n_mat.x, n_mat.y, n_mat.z, T(0)};
+              else ny = V4<T>{n_ad.x, n_ad.y, n_ad.z, T(0)};
+            }
+            cv.x += f_abs((ny.x * gker.x + ny.y * gker.y + ny.z * gker.z) * P.vol_def);
+          }
+        }
+      }
+    }
+  }
+  S.cv[cpar][i] = cv;
+  S.cny[i] = ny;
+  S.cvz[i] = vz;
+  write_rec(P, S.rec, i, S.vel[c][i], ld6(S.str_a[c], S.str_b[c], i), S.idm[c][i].y, S.codes[c][i].x >= 10);
+}
+
+// ---------------------------------------------------------------------------------
+// Particle interaction (src/particle_interaction.cu:26-297).
+//
+// One thread per material particle.  Phase 1 scans the 27 neighbour cells in the
+// reference's order (cz, cy, cx; boundary range then material range; ascending j)
+// and appends every candidate passing a conservative distance test to a per-thread
+// list in shared memory (column per thread: conflict-free).  Phase 2 walks the list
+// in order and evaluates the exact q < 2 test and the pair terms, so every sum is
+// accumulated in the reference's order while the expensive pair arithmetic runs with
+// the warp converged.  A list that fills up is flushed and the rest of the scan is
+// evaluated directly, still in order.
+// ---------------------------------------------------------------------------------
+template <class T> struct Acc {
+  T accden;
+  V3<T> s, av, as;
+  F9<T> gv;
+};
+
+template <class T> struct IState {
+  V3<T> pos, vel;
+  T rho, ri;
+  S6<T> sor;
+  int shift;
+};
+
+template <class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, const V3<T> dr, const Rec<T>* __restrict__ rec,
+                                      int j, Acc<T>& A) {
+  T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+  T q = r * P.i_h;
+  if (!(q < T(2.0f))) return;
+  T ker = kernel_w(P.knorm, q);
+  T dwdr = kernel_f(P.kgrad, q);
+  V3<T> gker = dr * dwdr;
+  const V4<T> vr = rec[j].vr;
+  const V4<T> aux = rec[j].aux;
+  const T rho_j = vr.w, mass_j = aux.x, vol_j = aux.y;
+  const bool contact_j = aux.w != T(0);
+  V3<T> dvel = I.vel - V3<T>{vr.x, vr.y, vr.z};
+  if (contact_j && I.shift == 1) dvel = V3<T>{T(0), T(0), T(0)};
+  A.gv.xx -= dvel.x * gker.x * vol_j;
+  A.gv.xy -= dvel.x * gker.y * vol_j;
+  A.gv.xz -= dvel.x * gker.z * vol_j;
+  A.gv.yx -= dvel.y * gker.x * vol_j;
+  A.gv.yy -= dvel.y * gker.y * vol_j;
+  A.gv.yz -= dvel.y * gker.z * vol_j;
+  A.gv.zx -= dvel.z * gker.x * vol_j;
+  A.gv.zy -= dvel.z * gker.y * vol_j;
+  A.gv.zz -= dvel.z * gker.z * vol_j;
+  if (contact_j) return;
+  A.accden += I.rho * dot(dvel, gker) * vol_j;
+  const V4<T> sa = rec[j].sa;
+  const V4<T> sb = rec[j].sb;
+  const S6<T> st{I.sor.xx + sa.x, I.sor.yy + sa.y, I.sor.zz + sa.z, I.sor.xy + sa.w, I.sor.xz + sb.x, I.sor.yz + sb.y};
+  A.s = A.s + dotSV(st, gker) * mass_j;
+  if (P.viscosity_type == 1) {
+    T artv = T(0.0f);
+    T visc = dot(dvel, dr);
+    if (visc < T(0.0f)) {
+      T phi = P.h * visc / (r * r + P.eta);
+      artv = P.alpha_m * P.cs_m * phi / (T(0.5f) * (I.rho + rho_j));
+    }
+    A.av = A.av + gker * (mass_j * artv);
+  }
+  if (P.art_coef != T(0.f)) {
+    T artp = I.ri + aux.z;
+    if (artp > T(0.0f)) {
+      artp *= f_pow(ker / P.kernel_dr, P.kernel_zero / P.kernel_dr);
+      A.as = A.as - gker * (mass_j * artp);
+    }
+  }
+}
+
+constexpr int IX_THREADS = 128, IX_CAP = 96;
+
+template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S,
+                                                                              const Dyn<T>* dyn, int cpar) {
+  extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int total = P.np - P.npb;
+  if (t >= total) return;
+  const int i = P.npb + t;
+  const V4<T>* __restrict__ cv_in = S.cv[cpar];
+  const V4<T>* __restrict__ cf_in = S.cf[cpar];
+  V4<T>* cv_out = S.cv[cpar ^ 1];
+  V4<T>* cf_out = S.cf[cpar ^ 1];
+  const int npm = dyn->npm;
+  if (t >= npm) {  // deleted slots keep their contact state
+    cv_out[i] = cv_in[i];
+    cf_out[i] = cf_in[i];
+    return;
+  }
+  const int c = dyn->cur_main;
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const Rec<T>* __restrict__ rec = S.rec;
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  IState<T> I;
+  I.pos = ld3(pos, i);
+  const V4<T> vr_i = S.vel[c][i];
+  I.vel = xyz(vr_i);
+  I.rho = vr_i.w;
+  I.sor = ld6(S.str_a[c], S.str_b[c], i) / (vr_i.w * vr_i.w);
+  I.ri = T(0.0f);
+  if (P.art_coef != T(0.f)) {
+    I.ri = trace(I.sor);
+    if (I.ri > T(0.0f)) I.ri *= P.art_coef;
+    else I.ri = T(0.0f);
+  }
+  V4<T> cv = cv_in[i];
+  I.shift = (int)cv.z;
+  Acc<T> A;
+  A.accden = T(0.f);
+  A.s = A.av = A.as = V3<T>{T(0), T(0), T(0)};
+  A.gv = F9<T>{T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
+  const T th = P.two_h;
+  const T r2max = P.r2_prefilter;
+  unsigned* my = nbl + threadIdx.x;
+  const int stride = blockDim.x;
+  int cnt = 0;
+  bool direct = false;
+  for (int oc = 0; oc < 27; ++oc) {
+    const I3 off = off_of(oc);
+    const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+    if (!in_grid(P, cj)) continue;
+    const int k = key_of(P, cj);
+    const V3<T> o = mulI(off, th);
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      const int2 rg = S.range[pass ? k + P.ncell_material : k];
+      for (int j = rg.x; j < rg.y; ++j) {
+        const V3<T> dr = I.pos - ld3(pos, j) - o;
+        const T r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
+        if (r2 < r2max) {
+          if (!direct) {
+            if (cnt < IX_CAP) {
+              my[cnt * stride] = (unsigned)j | ((unsigned)oc << 27);
+              ++cnt;
+              continue;
+            }
+            for (int e = 0; e < cnt; ++e) {  // list full: flush it, then go direct
+              const unsigned ent = my[e * stride];
+              const int jj = (int)(ent & 0x7ffffffu);
+              const V3<T> oo = mulI(off_of((int)(ent >> 27)), th);
+              pair_term(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
+            }
+            direct = true;
+          }
+          pair_term(P, I, dr, rec, j, A);
+        }
+      }
+    }
+  }
+  if (!direct) {
+    for (int e = 0; e < cnt; ++e) {
+      const unsigned ent = my[e * stride];
+      const int jj = (int)(ent & 0x7ffffffu);
+      const V3<T> oo = mulI(off_of((int)(ent >> 27)), th);
+      pair_term(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
+    }
+  }
+  const V3<T> g{P.gravity[0], P.gravity[1], P.gravity[2]};
+  const V3<T> acc_damp = I.vel * P.damping;
+  const V4<T> acc1 = v4(A.s + A.av + A.as - acc_damp + g, A.accden);
+  const V4<T> vr_new = vr_i + acc1 * P.dt;
+  // Wall contact (cuParticleInteractionMaterialLoopContact, src/particle_interaction.cu:142-241).
+  V3<T> acc_st{T(0.0f), T(0.0f), T(0.0f)};
+  V4<T> fo = cf_in[i];
+  const V4<T> ny = S.cny[i];
+  const V4<T> vz = S.cvz[i];
+  const T mass_i = S.idm[c][i].y;
+  const T mrate = T(2.0f) / (T(2.0f) + T(0.0f));
+  const V3<T> nb{ny.x, ny.y, ny.z};
+  const V3<T> dv{(vz.x - vr_new.x) * mrate, (vz.y - vr_new.y) * mrate, (vz.z - vr_new.z) * mrate};
+  if (cv.y <= P.h * T(2) && dot(dv, nb) > T(0)) {
+    const T fcoef = P.wall_fric;
+    const T dvn_s = dot(dv, nb);
+    const V3<T> dvn{nb.x * dvn_s, nb.y * dvn_s, nb.z * dvn_s};
+    const V3<T> fn = dvn * mass_i / P.dt;
+    const V3<T> dvt = dv - dvn;
+    V3<T> ft = dvt * mass_i / P.dt;
+    const T afn = enorm(fn), aft = enorm(ft);
+    if (aft > (fcoef * afn)) {
+      ft = ft * (fcoef * afn / aft);
+      cv.z = T(1);
+    } else {
+      cv.z = T(0);
+    }
+    V3<T> fric = ft + fn;
+    if (cv.y > P.dr * T(1.0f)) {
+      int count = 0;
+      const V3<T> pabs_i = I.pos + mulI(celli, T(2.0f) * P.h);
+      for (int oc = 0; oc < 27; ++oc) {
+        const I3 off = off_of(oc);
+        const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+        if (!in_grid(P, cj)) continue;
+        const int2 rg = S.range[key_of(P, cj) + P.ncell_material];
+        for (int j = rg.x; j < rg.y; ++j) {
+          const V4<T> cvj = cv_in[j];
+          if (cvj.y <= P.dr * T(1.0001f)) {
+            const V4<T> pj = pos[j];
+            const int4 cpj = S.cellpos[c][j];
+            const V3<T> pabs_j{pj.x + (T)cpj.x * (T(2.0f) * P.h), pj.y + (T)cpj.y * (T(2.0f) * P.h),
+                               pj.z + (T)cpj.z * (T(2.0f) * P.h)};
+            const V3<T> dc = pabs_i - pabs_j;
+            const T rcol = f_abs(dc.x * ny.z + dc.y * ny.y + dc.z * ny.x);
+            const T cvx_j0 = (j == i) ? cv.x : cvj.x;
+            if (rcol <= P.dr / T(2) && cvx_j0 != T(0)) {
+              if (cv.x > cvx_j0) cv.x = cvx_j0;
+              const T cvx_j = (j == i) ? cv.x : cvj.x;
+              const V4<T> fj = cf_in[j];
+              fric.x = fj.x * cv.x / cvx_j;
+              fric.y = fj.y * cv.x / cvx_j;
+              fric.z = fj.z * cv.x / cvx_j;
+              count++;
+            }
+          }
+        }
+      }
+      if (count == 0) fric = fric * T(0);
+    }
+    fo = V4<T>{fric.x, fric.y, fric.z, T(0)};
+    acc_st = fric * (T(1) / mass_i);
+  }
+  cv_out[i] = cv;
+  cf_out[i] = fo;
+  S.accad[i] = v4(A.s + A.av + A.as + acc_st - acc_damp + g, A.accden);
+  st6(S.ace_a, S.ace_b, i, full2sym(A.gv));
+  S.spin[i] = v4(skewpart(A.gv), T(0.f));
+}
+
+// ---------------------------------------------------------------------------------
+// Predictor (src/predictor_corrector.cu:52-103): saves the step-start state into the
+// *_ini buffers (the reference's four D2D copies) and advances material half a step.
+// ---------------------------------------------------------------------------------
+template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.np) return;
+  const int c = dyn->cur_main, ci = dyn->cur_ini;
+  const int npm = dyn->npm;
+  V4<T> ps = S.pos[c][i];
+  V4<T> vr = S.vel[c][i];
+  S.pos_ini[ci][i] = ps;
+  S.vel_ini[ci][i] = vr;
+  if (npm == 0 || i >= P.npb + npm) return;
+  S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
+  S6<T> sn = ld6(S.stn_a[c], S.stn_b[c], i);
+  st6(S.stri_a[ci], S.stri_b[ci], i, sg);
+  st6(S.stni_a[ci], S.stni_b[ci], i, sn);
+  if (i < P.npb) return;
+  const int4 code = S.codes[c][i];
+  if (code.y != 1) return;
+  const T hdt = T(0.5f) * P.dt;
+  vr = vr + S.accad[i] * hdt;
+  ps = add3(ps, xyz(vr) * hdt);
+  const T* mp = P.model_par[code.w];
+  vr.w = f_max(vr.w, mp[kMatSize - 2]);
+  vr.w = f_min(vr.w, mp[kMatSize - 1]);
+  const S6<T> D = ld6(S.ace_a, S.ace_b, i);
+  sn = sn + D * hdt;
+  bool yld = false;
+  T mcrt = T(0);
+  constitutive(code.z, mp, hdt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt);
+  S.pos[c][i] = ps;
+  S.vel[c][i] = vr;
+  st6(S.stn_a[c], S.stn_b[c], i, sn);
+  st6(S.str_a[c], S.str_b[c], i, sg);
+  if (!yld) S.idm[c][i].x = T(100);
+}
+
+// ---------------------------------------------------------------------------------
+// Corrector (src/predictor_corrector.cu:109-213): rigid walls and material.
+// ---------------------------------------------------------------------------------
+template <class T> RWD I3 rebin(V4<T>& ps, T th) {
+  I3 dc{int(ps.x >= th) - int(ps.x < T(0)), int(ps.y >= th) - int(ps.y < T(0)), int(ps.z >= th) - int(ps.z < T(0))};
+  ps = sub3(ps, mulI(dc, th));
+  return dc;
+}
+
+template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int npm = dyn->npm;
+  if (i >= P.npb + npm) return;
+  const int c = dyn->cur_main, ci = dyn->cur_ini;
+  const int4 code = S.codes[c][i];
+  if (code.y != 1) return;
+  const T th = P.two_h;
+  if (i < P.npb) {
+    if (P.n_motion <= 0) return;
+    const Motion<T>& mv = dyn->mv[code.w];
+    V3<T> vel{mv.trans_vel.x, mv.trans_vel.y, mv.trans_vel.z};
+    int4 cp = S.cellpos[c][i];
+    if (mv.is_rotat && mv.pattern != RW_PATTERN_CIRCLE) {
+      const V3<T> pabs = ld3(S.pos[c], i) + mulI(I3{cp.x, cp.y, cp.z}, th);
+      const V3<T> rp{mv.pos_rp.x, mv.pos_rp.y, mv.pos_rp.z};
+      const V3<T> w{mv.rotat_vel.x, mv.rotat_vel.y, mv.rotat_vel.z};
+      vel = vel + cross(w, pabs - rp);
+      const F9<T> R = rodrigues(w * P.dt);
+      const int cn = dyn->cur_nrm;
+      const V4<T> n4 = S.normal[cn][i];
+      const V3<T> n = dotFV(R, xyz(n4));
+      S.normal[cn][i] = v4(n, n4.w);
+    }
+    V4<T> ps = add3(S.pos_ini[ci][i], vel * P.dt);
+    const I3 dc = rebin(ps, th);
+    S.pos[c][i] = ps;
+    S.cellpos[c][i] = int4{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z, cp.w};
+    return;
+  }
+  const V4<T> vri = S.vel_ini[ci][i];
+  V4<T> vr = vri + S.accad[i] * P.dt;
+  V4<T> ps = add3(S.pos_ini[ci][i], xyz(vr + vri) * (T(0.5f) * P.dt));
+  const T* mp = P.model_par[code.w];
+  vr.w = f_max(vr.w, mp[kMatSize - 2]);
+  vr.w = f_min(vr.w, mp[kMatSize - 1]);
+  const I3 dc = rebin(ps, th);
+  int4 cp = S.cellpos[c][i];
+  cp = int4{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z, cp.w};
+  S6<T> sg = ld6(S.stri_a[ci], S.stri_b[ci], i);
+  const S6<T> D = ld6(S.ace_a, S.ace_b, i);
+  const S6<T> sn = ld6(S.stni_a[ci], S.stni_b[ci], i) + D * P.dt;
+  bool yld = false;
+  T mcrt = T(0);
+  constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt);
+  V4<T> id = S.idm[c][i];
+  if (!yld) id.x = T(100);
+  id.w = mcrt;
+  if (!in_grid(P, I3{cp.x, cp.y, cp.z})) {
+    cp.w = P.ncell_delete_m;
+    id.x = T(999.0);
+  }
+  V4<T> po = S.pos_ori[c][i];
+  if (dyn->time_f <= P.dt) po = V4<T>{T(0), T(0), T(0), T(0)};
+  po = add3(po, xyz(vr) * P.dt);
+  S.vel[c][i] = vr;
+  S.pos[c][i] = ps;
+  S.cellpos[c][i] = cp;
+  st6(S.str_a[c], S.str_b[c], i, sg);
+  st6(S.stn_a[c], S.stn_b[c], i, sn);
+  S.idm[c][i] = id;
+  S.pos_ori[c][i] = po;
+  S.accad[i] = po;
+}
+
+// ---------------------------------------------------------------------------------
+// Shepard stress filter (src/field_smoothing.cu:239-314).  store != 0 copies the
+// result back into the stress (StressRegularization) and refreshes the records.
+// ---------------------------------------------------------------------------------
+template <class T> __global__ void __launch_bounds__(128) k_shepard(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
+                                                                   int only_filter_steps) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int npm = dyn->npm;
+  if (t >= npm) return;
+  if (only_filter_steps) {
+    const int st = dyn->step;
+    if (!(P.stress_shepard_filter != 0 && st % P.stress_shepard_filter == 0 && st != 0)) return;
+  }
+  const int i = P.npb + t;
+  const int c = dyn->cur_main;
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const V3<T> pos_i = ld3(pos, i);
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  S6<T> sh = zero6<T>();
+  T sumker = T(0.0f);
+  const T th = P.two_h;
+  for (int oc = 0; oc < 27; ++oc) {
+    const I3 off = off_of(oc);
+    const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+    if (!in_grid(P, cj)) continue;
+    const int2 rg = S.range[key_of(P, cj) + P.ncell_material];
+    const V3<T> o = mulI(off, th);
+    for (int j = rg.x; j < rg.y; ++j) {
+      V3<T> dr = pos_i - ld3(pos, j) - o;
+      T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+      T q = r * P.i_h;
+      if (q < T(2.0f)) {
+        T ker = kernel_w(P.knorm, q);
+        T vol = S.idm[c][j].y / S.vel[c][j].w;
+        sumker += ker * vol;
+        sh = sh + ld6(S.str_a[c], S.str_b[c], j) * (ker * vol);
+      }
+    }
+  }
+  if (sumker != T(0.f)) sh = sh / sumker;
+  st6(S.tc_a, S.tc_b, i, sh);
+}
+
+template <class T> __global__ void k_shepard_store(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
+                                                   int only_filter_steps) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int npm = dyn->npm;
+  if (t >= npm) return;
+  if (only_filter_steps) {
+    const int st = dyn->step;
+    if (!(P.stress_shepard_filter != 0 && st % P.stress_shepard_filter == 0 && st != 0)) return;
+  }
+  const int i = P.npb + t;
+  const int c = dyn->cur_main;
+  const S6<T> sh = ld6(S.tc_a, S.tc_b, i);
+  st6(S.str_a[c], S.str_b[c], i, sh);
+  write_rec(P, S.rec, i, S.vel[c][i], sh, S.idm[c][i].y, S.codes[c][i].x >= 10);
+}
+
+// ---------------------------------------------------------------------------------
+// Lateral wall force with FP64 accumulation (replaces the single-thread loop of
+// src/utilities.cu:578-640): per-block sums in a fixed order, then one block adds
+// the partial sums in block order, so the result is deterministic.
+// ---------------------------------------------------------------------------------
+constexpr int WF_THREADS = 256, WF_BLOCKS = 296;
+
+template <class T> __global__ void __launch_bounds__(WF_THREADS) k_wall_force(const Params<T> P, DevState<T> S,
+                                                                             const Dyn<T>* dyn, int cpar, int mode,
+                                                                             int wall_id, double xmax, double zmin,
+                                                                             double zmax) {
+  __shared__ double red[3][WF_THREADS];
+  const int npm = dyn->npm, c = dyn->cur_main;
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int t = blockIdx.x * WF_THREADS + threadIdx.x; t < npm; t += gridDim.x * WF_THREADS) {
+    const int i = P.npb + t;
+    bool take;
+    if (mode == 0) {
+      const V4<T> cv = S.cv[cpar][i];
+      take = (int)cv.w == wall_id && cv.y <= P.h * T(2);
+    } else {
+      const V4<T> ps = S.pos[c][i];
+      const int4 cp = S.cellpos[c][i];
+      const double px = (double)(ps.x + (T)cp.x * (T(2.0f) * P.h));
+      const double pz = (double)(ps.z + (T)cp.z * (T(2.0f) * P.h));
+      take = px <= xmax && pz >= zmin && pz <= zmax;
+    }
+    if (take) {
+      const V4<T> f = S.cf[cpar][i];
+      a[0] += (double)f.x;
+      a[1] += (double)f.y;
+      a[2] += (double)f.z;
+    }
+  }
+  for (int k = 0; k < 3; ++k) red[k][threadIdx.x] = a[k];
+  __syncthreads();
+  for (int s = WF_THREADS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 3; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) S.wsum[3 * blockIdx.x + k] = red[k][0];
+}
+
+__global__ void k_wall_force_final(double* wsum, int nblocks) {
+  if (threadIdx.x != 0) return;
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int b = 0; b < nblocks; ++b)
+    for (int k = 0; k < 3; ++k) a[k] += wsum[3 * b + k];
+  for (int k = 0; k < 3; ++k) wsum[3 * nblocks + k] = a[k];
+}
+
+}  // namespace rw

@@ -1,0 +1,72 @@
+// Parameter block and device-resident dynamic state of one case.
+//
+// Params<T> mirrors the reference's Parameters (src/types.h:100-165) after
+// InitializeParameters (src/loquat.cu:130-190).  It is passed BY VALUE to every
+// kernel (kernel-parameter constant bank), replacing the reference's per-TU
+// __constant__ copies refreshed by cudaMemcpyToSymbolAsync before each launch.
+// What changes during a run (time, live counts, rigid-body motion, buffer parity,
+// error word) lives in Dyn<T> in device memory, so a whole step can be captured in a
+// CUDA graph with no host round trip.
+#pragma once
+#include <stdint.h>
+
+#define RW_MATERIAL_NUMBER 100.0f  // idmassidx.x >= 100: material (src/types.h:37)
+#define RW_MODEL_RIGID 0
+#define RW_MODEL_DP 1
+#define RW_MODEL_MUIDP 2
+#define RW_MODEL_HYPO_BASIC 3
+#define RW_MODEL_HYPO_CS 4
+#define RW_PATTERN_CIRCLE 1
+
+namespace rw {
+
+constexpr int kModelMax = 10, kMatSize = 15, kMotionMax = 10, kTableMax = 10;
+
+template <class T> struct Vec3 { T x, y, z; };
+
+template <class T> struct Motion {  // RigidMotion (src/types.h:66-75)
+  int is_trans, is_rotat, pattern, pad_;
+  Vec3<T> trans_vel, trans_acc, pos_rp, rotat_vel, rotat_acc;
+};
+
+template <class T> struct Table {  // MotionTable (src/types.h:77-97)
+  int is_translation, is_rotation, n_trans, n_rot, pattern, pad_;
+  T trans_time[kTableMax], rotat_time[kTableMax];
+  Vec3<T> trans_vel[kTableMax], trans_acc[kTableMax], rotat_acc[kTableMax];
+  Vec3<T> pos_rp, rotat_vel;
+};
+
+template <class T> struct Params {
+  int dim, periodbound, n_motion, n_model;
+  int np, npb, npm0;        // particle counts at set-up (np, npb never change)
+  int cell_num[3];
+  int ncell, ncell_material, ncell_delete_m;
+  int stress_shepard_filter, viscosity_type, output_format;
+  T planeleft[4], planeright[4];
+  T domain_size[3], domain_min[3], gravity[3];
+  T h, i_h, two_h, dr, hdr, vol_def, bound_thickness;
+  T rho0_m, damping;
+  T model_par[kModelMax][kMatSize];
+  T knorm, kgrad;            // Wendland normalisations (src/loquat.cu:163-166)
+  T alpha_m, cs_m, eta, cfl, art_coef, kernel_zero, kernel_dr;
+  T time_max, dt, output_frequency;
+  T wall_fric;               // wall-soil Coulomb coefficient
+  T r2_prefilter;            // conservative (2h)^2 bound for the candidate pre-test
+};
+
+// Device-resident state that changes during a run.
+template <class T> struct Dyn {
+  double time_d;             // host-side `time` of RunSimulation, accumulated in double
+  T time_f;                  // par.time (scalar copy of time_d, StepCalculation)
+  T pad0_;
+  int npm, np_delete_m;      // live / deleted material counts (src/loquat_grid.cu:234-249)
+  int cur_main, cur_nrm, cur_ini;  // which ping-pong buffer holds each permuted group
+  int need_sort;             // 1 when the new cell keys are not already in order
+  unsigned err;              // RW_DERR_* bits
+  int step;
+  int pad1_[2];
+  Motion<T> mv[kMotionMax];
+  Table<T> tab[kMotionMax];
+};
+
+}  // namespace rw

@@ -1,0 +1,193 @@
+"""Python mirror of the reference's ``LoquatSph`` (src/loquat.h:44-126) over the C ABI.
+
+Method names follow the reference's (``PredictorSection`` -> ``predictor_section`` ...);
+each one is one C-ABI call into librw.so.  ``run_simulation`` is the reference's
+``RunSimulation`` loop (src/loquat.cu:511-565) with whole steps replayed from a captured
+CUDA graph between saves."""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, lib
+
+
+class LoquatSph:
+    def __init__(self, project: Optional[str] = None, device: int = 0, precision: int = 4, case=None):
+        """Open ``project`` (reads ``<project>.xml/.dat/.motion``) or an in-memory
+        ``cases.Case``.  precision 4 = float (the reference's default build), 8 = double."""
+        L = lib()
+        h = ct.c_void_p()
+        if case is not None:
+            keep: list = []
+            c = _abi.case_struct(case, keep)
+            st = L.rw_create_from_case(ct.byref(c), device, precision, ct.byref(h))
+        else:
+            if project is None:
+                raise ValueError("need a project name or a case")
+            st = L.rw_create(project.encode(), device, precision, ct.byref(h))
+        check(st, "rw_create", None)
+        self._h = h
+        self.project = project
+        self.precision = precision
+
+    # -- lifetime ---------------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().rw_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, st: int, what: str) -> None:
+        check(st, what, self._h)
+
+    # -- the reference's stage methods --------------------------------------------------
+    def step_calculation(self):
+        self._c(lib().rw_begin_step(self._h), "rw_begin_step")
+
+    def neighbor_search(self, section: int):
+        self._c(lib().rw_neighbor_search(self._h, section), "rw_neighbor_search")
+
+    def rigid_body_update(self):
+        self._c(lib().rw_rigid_body_update(self._h), "rw_rigid_body_update")
+
+    def adami_boundary(self):
+        self._c(lib().rw_adami_boundary(self._h), "rw_adami_boundary")
+
+    def find_corner_particle(self):
+        self._c(lib().rw_find_corner(self._h), "rw_find_corner")
+
+    def stress_regularization(self):
+        self._c(lib().rw_shepard_filter(self._h), "rw_shepard_filter")
+
+    def particle_interaction(self):
+        self._c(lib().rw_particle_interaction(self._h), "rw_particle_interaction")
+
+    def predictor(self):
+        self._c(lib().rw_predictor(self._h), "rw_predictor")
+
+    def corrector(self):
+        self._c(lib().rw_corrector(self._h), "rw_corrector")
+
+    def end_step(self):
+        self._c(lib().rw_end_step(self._h), "rw_end_step")
+
+    def predictor_section(self, shepard: bool = False):
+        """src/loquat.cu:376-406 (Shepard only when the caller's step schedule asks)."""
+        self.neighbor_search(0)
+        self.rigid_body_update()
+        self.adami_boundary()
+        self.find_corner_particle()
+        if shepard:
+            self.stress_regularization()
+        self.particle_interaction()
+        self.predictor()
+
+    def corrector_section(self):
+        """src/loquat.cu:408-436."""
+        self.neighbor_search(1)
+        self.adami_boundary()
+        self.find_corner_particle()
+        self.particle_interaction()
+        self.corrector()
+
+    def step(self, n: int = 1):
+        """n whole steps from the captured CUDA graph (asynchronous)."""
+        self._c(lib().rw_step(self._h, n), "rw_step")
+
+    def step_timed(self, n: int) -> float:
+        """n whole steps; returns their device time in ms (CUDA events on the context's
+        stream; the graph is captured before the first event if needed)."""
+        ms = ct.c_double(0.0)
+        self._c(lib().rw_step_timed(self._h, n, ct.byref(ms)), "rw_step_timed")
+        return ms.value
+
+    def synchronize(self):
+        self._c(lib().rw_synchronize(self._h), "rw_synchronize")
+
+    def profile(self, nsteps: int = 5):
+        """Mean device time per stage [ms] over nsteps per-stage steps, and the number
+        of kernels one whole step launches."""
+        from ._lib import STAGE_NAMES
+
+        ms = (ct.c_double * len(STAGE_NAMES))()
+        kps = ct.c_int(0)
+        self._c(lib().rw_profile(self._h, nsteps, ms, len(STAGE_NAMES), ct.byref(kps)), "rw_profile")
+        return dict(zip(STAGE_NAMES, ms[:])), kps.value
+
+    # -- state ----------------------------------------------------------------------------
+    def info(self) -> _abi.Info:
+        inf = _abi.Info()
+        self._c(lib().rw_get_info(self._h, ct.byref(inf)), "rw_get_info")
+        return inf
+
+    def get(self, name: str) -> np.ndarray:
+        rows, cols, dt = _abi.array_spec(name, self.info())
+        a = np.zeros((rows, cols), dt) if cols > 1 else np.zeros(rows, dt)
+        self._c(lib().rw_get_array(self._h, _abi.ARRAYS[name], a.ctypes.data, a.nbytes), f"rw_get_array({name})")
+        return a
+
+    def set(self, name: str, a: np.ndarray) -> None:
+        rows, cols, dt = _abi.array_spec(name, self.info())
+        a = np.ascontiguousarray(a, dtype=dt)
+        self._c(lib().rw_set_array(self._h, _abi.ARRAYS[name], a.ctypes.data, a.nbytes), f"rw_set_array({name})")
+
+    def set_counters(self, time: float, step: int, npm: int, np_delete_m: int) -> None:
+        self._c(lib().rw_set_counters(self._h, time, step, npm, np_delete_m), "rw_set_counters")
+
+    def set_option(self, opt: int, value: float) -> None:
+        self._c(lib().rw_set_option(self._h, opt, value), "rw_set_option")
+
+    def wall_force(self, mode: int = 0, wall_id: int = 10, strip: Optional[Sequence[float]] = None) -> np.ndarray:
+        """Lateral wall force [N], FP64 accumulation (mode 0: by nearest wall id; 1: strip)."""
+        out = (ct.c_double * 3)()
+        sp = None
+        if strip is not None:
+            sa = (ct.c_double * 3)(*strip)
+            sp = ct.cast(sa, ct.c_void_p)
+        self._c(lib().rw_wall_force(self._h, mode, wall_id, sp, out), "rw_wall_force")
+        return np.array(out[:])
+
+    def save(self, outdir: Optional[str] = None) -> None:
+        d = outdir or self.project or "."
+        self._c(lib().rw_save(self._h, d.encode()), "rw_save")
+
+    # -- RunSimulation ---------------------------------------------------------------------
+    def run_simulation(self, outdir: Optional[str] = None, time_max: Optional[float] = None,
+                       output_frequency: Optional[float] = None) -> None:
+        """The reference's main loop (src/loquat.cu:533-561): initial save, then steps with a
+        save whenever the accumulated output time exceeds output-frequency."""
+        from . import cases
+
+        params = cases.read_xml(self.project + ".xml") if self.project else {}
+        tmax = float(time_max if time_max is not None else params.get("time_max", 0.0))
+        freq = float(output_frequency if output_frequency is not None else params.get("output_frequency", 0.0))
+        out = outdir or self.project or "."
+        os.makedirs(out, exist_ok=True)
+        self.save(out)
+        inf = self.info()
+        t, ot, dt = inf.time, 0.0, inf.dt
+        while t < tmax:
+            n = max(1, int((freq - ot) / dt)) if freq > 0 else max(1, int((tmax - t) / dt))
+            self.step(n)
+            self.synchronize()
+            t += n * dt
+            ot += n * dt
+            if freq > 0 and ot > freq:
+                self.save(out)
+                ot = 0.0

@@ -1,0 +1,62 @@
+"""Case generator and the reference's case-file formats (src/GenCase.cu:70-227,
+src/loquat_io.cu:75-312)."""
+import numpy as np
+
+from retainwall_code_b200 import cases as C
+
+
+def test_generator_is_deterministic():
+    a = C.retaining_wall(nx=10, ny=6, nz=8, dx=0.005)
+    b = C.retaining_wall(nx=10, ny=6, nz=8, dx=0.005)
+    assert np.array_equal(a.pospres, b.pospres) and np.array_equal(a.codes, b.codes)
+
+
+def test_counts_and_layout():
+    c = C.retaining_wall(nx=10, ny=6, nz=8, dx=0.005)
+    assert c.npm == 10 * 6 * 8
+    assert c.np_ == c.npb + c.npm
+    assert (c.idmassidx[: c.npb, 0] == 0).all() and (c.idmassidx[c.npb:, 0] == 100).all()
+    assert (c.codes[c.npb:, 2] == C.HYPO_CS).all()
+    assert ((c.codes[: c.npb, 0] == 10) == (c.codes[: c.npb, 1] == C.NONFIX)).all()
+    # every particle strictly inside the grid, with margin
+    pos = c.pospres[:, :3]
+    dom = np.array([c.params["domain_size_x"], c.params["domain_size_y"], c.params["domain_size_z"]])
+    assert (pos > 0).all() and (pos < dom).all()
+
+
+def test_config_sizes():
+    c = C.column_collapse()
+    assert c.npm == 27648
+    specs = C.batch_sweep()
+    assert len(specs) == 64
+    n = [s["nx"] * s["ny"] * s["nz"] for s in specs]
+    assert 40_000 < min(n) and max(n) < 450_000
+
+
+def test_geostatic_stress_and_k0():
+    c = C.column_collapse(nx=4, ny=4, nz=10)
+    m = c.stress[c.npb:]
+    assert (m[:, 2] < 0).all()
+    k0 = 1 - np.sin(np.radians(30.0))
+    np.testing.assert_allclose(m[:, 0] / m[:, 2], k0, rtol=1e-6)
+
+
+def test_hypocs_mapping():
+    m = C.hypocs_model(30.0, 0.7, 1850.0)
+    assert abs(m[6] - (3e5 / 2.6e9) ** 0.27) < 1e-7
+    assert m[9] == np.float32(0.61) and m[10] == np.float32(1.10) and m[5] == np.float32(0.98)
+    assert abs(m[13] - 0.8 * 1850) < 1e-3 and abs(m[14] - 1.2 * 1850) < 1e-3
+
+
+def test_roundtrip_files(tmp_path):
+    c = C.retaining_wall(nx=6, ny=4, nz=5, dx=0.005, mode="rotation")
+    proj = str(tmp_path / "w")
+    C.write_case(c, proj)
+    r = C.read_case(proj)
+    assert np.array_equal(r.codes, c.codes)
+    for a, b in ((r.pospres, c.pospres), (r.velrhop, c.velrhop), (r.stress, c.stress), (r.normal, c.normal)):
+        assert np.array_equal(a.astype(np.float32), b.astype(np.float32))
+    assert r.params["npb"] == c.npb
+    assert np.float32(r.params[C.WALL_FRICTION_TAG]) == np.float32(c.params[C.WALL_FRICTION_TAG])
+    m = r.motions[0]
+    assert m.is_rotation and not m.is_translation and m.rotat_vel[1] == np.float32(-0.005)

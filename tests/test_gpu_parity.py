@@ -1,0 +1,147 @@
+"""Parity of the native sm_100a step (through the C ABI) with the CPU oracle and with
+the reference's own GPU outputs (tests/golden).  Tolerances as in
+tests/test_oracle_golden.py: integer work bit-exact; relative L2 <= 1e-5 per stage and
+over 100 steps away from the contact zone; wall force within 0.5 %."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from retainwall_code_b200 import LoquatSph
+from tests._util import STEP_STAGES, boundary_normal_mask, golden, load_state, mini_cases, rel
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["col_mini", "wall_mini"]
+GPU_STAGE = {
+    "begin_step": lambda s: s.step_calculation(),
+    "neighbor_search_p": lambda s: s.neighbor_search(0),
+    "neighbor_search_c": lambda s: s.neighbor_search(1),
+    "rigid_body_update": lambda s: s.rigid_body_update(),
+    "adami": lambda s: s.adami_boundary(),
+    "find_corner": lambda s: s.find_corner_particle(),
+    "interaction": lambda s: s.particle_interaction(),
+    "predictor": lambda s: s.predictor(),
+    "corrector": lambda s: s.corrector(),
+}
+
+
+@pytest.fixture(scope="module")
+def cases():
+    return mini_cases()
+
+
+def _cmp(a, b, key, tag, npb=None, codes=None, tol=1e-5):
+    if a.dtype.kind == "i":
+        np.testing.assert_array_equal(a, b, err_msg=f"{tag}/{key}")
+    elif key == "contact_mag" and npb is not None:
+        m = boundary_normal_mask(b, npb, codes)
+        assert rel(a[m], b[m]) < tol, (tag, key, rel(a[m], b[m]))
+    else:
+        assert rel(a, b) < tol, (tag, key, rel(a, b))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_initial_cell_list_bit_exact(cases, name):
+    g = golden(name)
+    s = LoquatSph(case=cases[name])
+    o = Oracle(cases[name], 4)
+    for k in ("part_idx", "cell_beg", "cell_end", "cellpos", "codes"):
+        np.testing.assert_array_equal(s.get(k), g[f"init/{k}"] if f"init/{k}" in g else o.get(k), err_msg=k)
+        np.testing.assert_array_equal(s.get(k), o.get(k), err_msg=k)
+    np.testing.assert_array_equal(s.get("pospres"), o.get("pospres"))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_stage_by_stage(cases, name):
+    """GPU and oracle restarted from the reference's state after step 1; every stage of
+    step index 1 compared with the oracle and with the reference's stage dump."""
+    g = golden(name)
+    c = cases[name]
+    s = LoquatSph(case=c)
+    o = Oracle(c, 4)
+    load_state(s, g)
+    load_state(o, g)
+    codes = g["step1/codes"]
+    for st, tag in STEP_STAGES:
+        GPU_STAGE[st](s)
+        o.stage(st)
+        if tag is None:
+            continue
+        for key in [k.split("/", 1)[1] for k in g.files if k.startswith(tag + "/") and not k.endswith("/meta")]:
+            a = s.get(key)
+            _cmp(a, o.get(key), key, tag + "[oracle]", c.npb, codes)
+            _cmp(a, g[f"{tag}/{key}"], key, tag + "[reference]", c.npb, codes)
+    assert s.info().device_err == 0
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_trajectory_100_steps_graph(cases, name):
+    """100 whole steps from the captured CUDA graph against the reference's dumps."""
+    g = golden(name)
+    c = cases[name]
+    s = LoquatSph(case=c)
+    s.set_option(0, 0.58108)
+    wf = []
+    for st in range(1, 101):
+        s.step(1)
+        wf.append(s.wall_force(1)[0] * 1e-3)
+        if st in (1, 10, 100):
+            np.testing.assert_array_equal(s.get("cellpos"), g[f"step{st}/cellpos"])
+            cv = g[f"step{st}/contact_var"]
+            mat = np.arange(c.np_) >= c.npb
+            far = mat & ~(cv[:, 1] <= 2.0 * c.params["dr"] * c.params["hdr"] + 1e-12)
+            for key in ("pospres", "velrhop", "str"):
+                a, b = s.get(key), g[f"step{st}/{key}"]
+                assert rel(a[far], b[far]) < 1e-5, (st, key, rel(a[far], b[far]))
+                assert rel(a, b) < 1e-4, (st, key, rel(a, b))
+    s.synchronize()
+    ref = g["wall_force_kN"][:, 1]
+    assert np.max(np.abs(np.asarray(wf) - ref)) / max(np.abs(ref).max(), 1e-30) < 5e-3
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_graph_equals_stage_calls(cases, name):
+    """The captured whole-step graph and the per-stage C-ABI calls are the same program."""
+    c = cases[name]
+    a = LoquatSph(case=c)
+    b = LoquatSph(case=c)
+    a.step(5)
+    for _ in range(5):
+        b.step_calculation()
+        b.predictor_section()
+        b.corrector_section()
+        b.end_step()
+    for key in ("cellpos", "pospres", "velrhop", "str", "stn", "contact_var", "contact_mag", "idmassidx"):
+        np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
+    assert a.info().step == b.info().step == 5
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_trajectory(cases, name):
+    """GPU vs oracle over 50 steps, float and double."""
+    c = cases[name]
+    for prec, tol in ((4, 1e-5), (8, 1e-11)):
+        s = LoquatSph(case=c, precision=prec)
+        o = Oracle(c, prec)
+        s.step(50)
+        o.step(50)
+        np.testing.assert_array_equal(s.get("cellpos"), o.get("cellpos"))
+        for key in ("pos_abs", "velrhop", "str"):
+            assert rel(s.get(key), o.get(key)) < (tol if name == "col_mini" else 100 * tol), (prec, key)
+        fs, fo = s.wall_force(0), o.wall_force(0)
+        assert abs(fs[0] - fo[0]) <= 5e-3 * max(abs(fo[0]), 1e-12), (prec, fs, fo)
+
+
+def test_device_error_word_on_wall_leaving_grid():
+    """A rigid wall driven out of the grid: the reference would write out of bounds;
+    here the cell key is clamped, RW_DERR_CELL_RANGE is raised, and rw_synchronize
+    reports RW_EDEVICE without any device fault."""
+    from retainwall_code_b200 import cases as C, RwError
+
+    c = C.retaining_wall(nx=8, ny=4, nz=6, dx=0.005, mode="active", wall_speed=400.0)
+    s = LoquatSph(case=c)
+    with pytest.raises(RwError) as ei:
+        s.step(400)
+        s.synchronize()
+    assert ei.value.status == 7
+    assert s.info().device_err & 1
