@@ -47,6 +47,9 @@ def make_case(workload: str):
         return C.retaining_wall(), {"workload": "retaining wall, active translation 1 mm/s",
                                     "soil": "200x80x120", "dx_m": 0.0025, "npm": 1920000,
                                     "wall_friction": "tan(2/3 phi_c)"}
+    if workload == "wall2_half":  # half-length block, for profiler captures
+        return C.retaining_wall(nx=100), {"workload": "retaining wall (half length)", "soil": "100x80x120",
+                                          "dx_m": 0.0025, "npm": 960000}
     if workload == "col1":
         return C.column_collapse(), {"workload": "column collapse", "soil": "24x24x48", "dx_m": 0.005, "npm": 27648}
     raise SystemExit(f"unknown workload {workload}")
@@ -211,6 +214,11 @@ def run_ours(args, ws, rank, local):
     inf = sim.info()
     if inf.device_err:
         raise SystemExit(f"device error word {inf.device_err}")
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": ws * npm * args.steps / (ms * 1e-3),
+                              "ms_per_step": ms / args.steps, "steps": args.steps, "partial": True}), flush=True)
+        return
     # ---- stage profile (CUDA events on the library's stream, per-stage launches) -------
     stages, kps = sim.profile(5)
     ix_ms = 0.5 * (stages["interaction_p"] + stages["interaction_c"])
@@ -274,6 +282,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="wall2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and stage-profile passes")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":  # host cores only: rank 0 runs, the other ranks exit
