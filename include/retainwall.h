@@ -209,6 +209,23 @@ enum {
 };
 rw_status rw_profile(rw_ctx* ctx, int nsteps, double* ms_per_stage, int n_stages, int* kernels_per_step);
 
+/* Allocation-free cell-key sort.  No counterpart in the reference (which sorts with
+ * cub::DeviceRadixSort into buffers it cudaMallocs, src/loquat_grid.cu:167-182); for
+ * callers that cannot allocate device memory.  Stable sort of n cell keys (device
+ * array d_keys, values in [0, max_key]) into d_sorted_keys, with d_perm[i] = index of
+ * the key that lands at position i: the permutation NeighborSearch applies.  Uses a
+ * fixed scratch array inside the library (about 8.6 MB, reserved on every GPU that
+ * loads the library until the process exits) instead of allocating: n is limited to
+ * RW_NOALLOC_MAX_KEYS and max_key to 2^24 - 1 (RW_EINVAL beyond).  Runs on `stream`
+ * (a cudaStream_t, NULL = default stream) of the current device.  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the one scratch array: calls whose work
+ * overlaps on the GPU (other streams, other threads) race and must be serialised by
+ * the caller.  d_keys must not alias the outputs. */
+#define RW_NOALLOC_MAX_KEYS (1 << 20)
+rw_status rw_cell_sort_noalloc(const int32_t* d_keys, int32_t n, int32_t max_key, int32_t* d_sorted_keys,
+                               int32_t* d_perm, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

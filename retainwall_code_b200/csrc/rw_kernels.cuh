@@ -145,7 +145,7 @@ template <class T> __global__ void k_keys(const Params<T> P, DevState<T> S, Dyn<
   S.vals[i] = i;
 }
 
-__global__ void k_check_sorted(const int* keys, int n, int* need_sort) {
+static __global__ void k_check_sorted(const int* keys, int n, int* need_sort) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i < n && keys[i - 1] > keys[i]) *need_sort = 1;
 }
@@ -156,7 +156,7 @@ constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
 // (per digit over tiles), downsweep (stable in-tile ranks + scatter).  All three
 // return immediately when the keys are already in order (the permutation is then
 // the identity, exactly what a stable sort of sorted keys returns).
-__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const int* keys, int n, int shift, int* hist, int ntiles,
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const int* keys, int n, int shift, int* hist, int ntiles,
                                                          const int* need) {
   if (!*need) return;
   __shared__ int h[256];
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const int* keys, int 
   hist[t * ntiles + blockIdx.x] = h[t];
 }
 
-__device__ __forceinline__ int block_excl_scan256(int v, int* total) {
+static __device__ __forceinline__ int block_excl_scan256(int v, int* total) {
   __shared__ int ws[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int x = v;
@@ -201,7 +201,7 @@ __device__ __forceinline__ int block_excl_scan256(int v, int* total) {
 }
 
 // One block per digit: exclusive scan of that digit's per-tile counts.
-__global__ void __launch_bounds__(RS_THREADS) k_rs_scan(int* hist, int ntiles, int* dtot, const int* need) {
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_scan(int* hist, int ntiles, int* dtot, const int* need) {
   if (!*need) return;
   int* row = hist + blockIdx.x * ntiles;
   const int per = (ntiles + RS_THREADS - 1) / RS_THREADS;
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scan(int* hist, int ntiles, i
   if (threadIdx.x == 0) dtot[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const int* kin, const int* vin, int* kout, int* vout, int n,
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const int* kin, const int* vin, int* kout, int* vout, int n,
                                                            int shift, const int* hist, const int* dtot, int ntiles,
                                                            const int* need) {
   if (!*need) return;
@@ -1006,7 +1006,7 @@ template <class T> __global__ void __launch_bounds__(WF_THREADS) k_wall_force(co
     for (int k = 0; k < 3; ++k) S.wsum[3 * blockIdx.x + k] = red[k][0];
 }
 
-__global__ void k_wall_force_final(double* wsum, int nblocks) {
+static __global__ void k_wall_force_final(double* wsum, int nblocks) {
   if (threadIdx.x != 0) return;
   double a[3] = {0.0, 0.0, 0.0};
   for (int b = 0; b < nblocks; ++b)
