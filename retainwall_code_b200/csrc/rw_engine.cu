@@ -69,6 +69,8 @@ template <class T> struct Engine final : EngineBase {
   bool compat_contact = true;
   cudaGraphExec_t gexec = nullptr;
   int g_cpar = -1;
+  int ix_kernel = 1;     // 1: chunked interaction with a shared-memory tile; 0: global path
+  int ncol = 0, max_chunks = 0;
   rw_case_params cparams{};
   int output_number = 0;
 
@@ -234,6 +236,13 @@ template <class T> struct Engine final : EngineBase {
     S.skeys = (S.sort_passes & 1) ? S.tk : S.keys;
     S.sperm = (S.sort_passes & 1) ? S.tv : S.vals;
     S.wsum = dalloc<double>(3 * (WF_BLOCKS + 1));
+    ncol = P.cell_num[0] * P.cell_num[1];
+    max_chunks = P.npm0 / IX2_TB + ncol + 1;
+    S.col_beg = dalloc<int>(ncol);
+    S.col_len = dalloc<int>(ncol);
+    S.col_cnt = dalloc<int>(ncol);
+    S.col_off = dalloc<int>(ncol);
+    S.chunks = dalloc<Chunk>(max_chunks);
     d_dyn = dalloc<Dyn<T>>(1);
 
     // Host-side conversion to structure-of-arrays, with the reference's
@@ -318,6 +327,8 @@ template <class T> struct Engine final : EngineBase {
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     RW_CU(cudaFuncSetAttribute(k_interaction<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                IX_CAP * IX_THREADS * (int)sizeof(unsigned)));
+    RW_CU(cudaFuncSetAttribute(k_interaction2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(Ix2Smem<T>)));
     neighbor_search(0);
     RW_CU(cudaStreamSynchronize(st));
   }
@@ -352,6 +363,11 @@ template <class T> struct Engine final : EngineBase {
     k_count<T><<<1, 1, 0, st>>>(P, S, d_dyn);
     k_permute<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn, section, compat_contact ? 1 : 0);
     k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
+    if (ncol > 0) {  // column chunks of the interaction
+      k_col_count<T><<<nblk(ncol, 256), 256, 0, st>>>(P, S);
+      k_col_scan<T><<<1, 1024, 0, st>>>(P, S, d_dyn);
+      k_col_fill<T><<<nblk(ncol, 256), 256, 0, st>>>(P, S);
+    }
     check_launch();
   }
   void rigid() override {
@@ -379,8 +395,13 @@ template <class T> struct Engine final : EngineBase {
   void interaction() override {
     const int n = P.np - P.npb;
     if (n > 0) {
-      k_interaction<T><<<nblk(n, IX_THREADS), IX_THREADS, IX_CAP * IX_THREADS * sizeof(unsigned), st>>>(P, S, d_dyn,
-                                                                                                     cpar);
+      if (ix_kernel == 1) {
+        const unsigned grid = (unsigned)std::max(max_chunks, (int)nblk(n, IX2_TB));
+        k_interaction2<T><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
+      } else {
+        k_interaction<T><<<nblk(n, IX_THREADS), IX_THREADS, IX_CAP * IX_THREADS * sizeof(unsigned), st>>>(P, S, d_dyn,
+                                                                                                       cpar);
+      }
       check_launch();
     }
     cpar ^= 1;
@@ -446,7 +467,7 @@ template <class T> struct Engine final : EngineBase {
 
   // Kernels launched by one whole step (launch_step), for launch accounting.
   int kernels_per_step() const {
-    const int search = 2 + 3 * S.sort_passes + 4;  // keys, check, sort passes, ranges, count, permute, flip
+    const int search = 2 + 3 * S.sort_passes + 4 + (ncol > 0 ? 3 : 0);  // keys, check, sort, ranges, count, permute, flip, chunks
     int k = 1 + 2 * search + 2 * 3 + 1 + 1 + 1;     // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
     if (P.stress_shepard_filter != 0) k += 2;
@@ -544,6 +565,9 @@ template <class T> struct Engine final : EngineBase {
   int set_option(int opt, double v) override {
     if (opt == RW_OPT_WALL_FRICTION) {
       P.wall_fric = (T)v;
+    } else if (opt == RW_OPT_INTERACTION_KERNEL) {
+      if (v != 0.0 && v != 1.0) return RW_EINVAL;
+      ix_kernel = (int)v;
     } else if (opt == RW_OPT_COMPAT_CONTACT) {
       if (v == 0.0) {
         err = "contact state following particles (RW_OPT_COMPAT_CONTACT=0) is not available";

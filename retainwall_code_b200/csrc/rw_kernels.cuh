@@ -67,6 +67,12 @@ template <class T> struct DevState {
   int* dtot;      // per-digit totals
   int ntiles, sort_passes;
   double* wsum;   // wall-force partial sums
+  // Column chunks of the interaction (rebuilt after every sort).
+  int* col_beg;
+  int* col_len;
+  int* col_cnt;
+  int* col_off;
+  struct Chunk* chunks;
 };
 
 template <class T> RWD V3<T> ld3(const V4<T>* p, int i) { V4<T> v = p[i]; return {v.x, v.y, v.z}; }
@@ -583,19 +589,32 @@ template <class T> struct IState {
   int shift;
 };
 
-template <class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, const V3<T> dr, const Rec<T>* __restrict__ rec,
-                                      int j, Acc<T>& A) {
+// The neighbour-side values one pair term needs (a Rec without its padding).
+template <class T> struct NbVals {
+  V4<T> vr, aux, sa, sb;
+};
+template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) {
+  NbVals<T> v;
+  v.vr = rec[j].vr;
+  v.aux = rec[j].aux;
+  v.sa = rec[j].sa;
+  v.sb = rec[j].sb;
+  return v;
+}
+
+// One pair (i, j) of cuParticleInteractionMaterialLoopSolution
+// (src/particle_interaction.cu:29-114), given dr = (pos_i - pos_j) - offset * 2h.
+template <class T> RWD void pair_eval(const Params<T>& P, const IState<T>& I, const V3<T> dr, const NbVals<T>& nb,
+                                      Acc<T>& A) {
   T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
   T q = r * P.i_h;
   if (!(q < T(2.0f))) return;
   T ker = kernel_w(P.knorm, q);
   T dwdr = kernel_f(P.kgrad, q);
   V3<T> gker = dr * dwdr;
-  const V4<T> vr = rec[j].vr;
-  const V4<T> aux = rec[j].aux;
-  const T rho_j = vr.w, mass_j = aux.x, vol_j = aux.y;
-  const bool contact_j = aux.w != T(0);
-  V3<T> dvel = I.vel - V3<T>{vr.x, vr.y, vr.z};
+  const T rho_j = nb.vr.w, mass_j = nb.aux.x, vol_j = nb.aux.y;
+  const bool contact_j = nb.aux.w != T(0);
+  V3<T> dvel = I.vel - V3<T>{nb.vr.x, nb.vr.y, nb.vr.z};
   if (contact_j && I.shift == 1) dvel = V3<T>{T(0), T(0), T(0)};
   A.gv.xx -= dvel.x * gker.x * vol_j;
   A.gv.xy -= dvel.x * gker.y * vol_j;
@@ -608,9 +627,8 @@ template <class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, co
   A.gv.zz -= dvel.z * gker.z * vol_j;
   if (contact_j) return;
   A.accden += I.rho * dot(dvel, gker) * vol_j;
-  const V4<T> sa = rec[j].sa;
-  const V4<T> sb = rec[j].sb;
-  const S6<T> st{I.sor.xx + sa.x, I.sor.yy + sa.y, I.sor.zz + sa.z, I.sor.xy + sa.w, I.sor.xz + sb.x, I.sor.yz + sb.y};
+  const S6<T> st{I.sor.xx + nb.sa.x, I.sor.yy + nb.sa.y, I.sor.zz + nb.sa.z,
+                 I.sor.xy + nb.sa.w, I.sor.xz + nb.sb.x, I.sor.yz + nb.sb.y};
   A.s = A.s + dotSV(st, gker) * mass_j;
   if (P.viscosity_type == 1) {
     T artv = T(0.0f);
@@ -622,7 +640,7 @@ template <class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, co
     A.av = A.av + gker * (mass_j * artv);
   }
   if (P.art_coef != T(0.f)) {
-    T artp = I.ri + aux.z;
+    T artp = I.ri + nb.aux.z;
     if (artp > T(0.0f)) {
       artp *= f_pow(ker / P.kernel_dr, P.kernel_zero / P.kernel_dr);
       A.as = A.as - gker * (mass_j * artp);
@@ -630,32 +648,16 @@ template <class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, co
   }
 }
 
-constexpr int IX_THREADS = 128, IX_CAP = 96;
+template <class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, const V3<T> dr,
+                                      const Rec<T>* __restrict__ rec, int j, Acc<T>& A) {
+  pair_eval(P, I, dr, load_nb(rec, j), A);
+}
 
-template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S,
-                                                                              const Dyn<T>* dyn, int cpar) {
-  extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int total = P.np - P.npb;
-  if (t >= total) return;
-  const int i = P.npb + t;
-  const V4<T>* __restrict__ cv_in = S.cv[cpar];
-  const V4<T>* __restrict__ cf_in = S.cf[cpar];
-  V4<T>* cv_out = S.cv[cpar ^ 1];
-  V4<T>* cf_out = S.cf[cpar ^ 1];
-  const int npm = dyn->npm;
-  if (t >= npm) {  // deleted slots keep their contact state
-    cv_out[i] = cv_in[i];
-    cf_out[i] = cf_in[i];
-    return;
-  }
-  const int c = dyn->cur_main;
-  const V4<T>* __restrict__ pos = S.pos[c];
-  const Rec<T>* __restrict__ rec = S.rec;
-  const int4 cp = S.cellpos[c][i];
-  const I3 celli{cp.x, cp.y, cp.z};
-  IState<T> I;
-  I.pos = ld3(pos, i);
+// Particle i's own state at the start of cuParticleInteractionMaterial
+// (src/particle_interaction.cu:264-277).
+template <class T> RWD void ix_begin(const Params<T>& P, const DevState<T>& S, int c, int i, const V4<T>& cv_i,
+                                     IState<T>& I, Acc<T>& A) {
+  I.pos = ld3(S.pos[c], i);
   const V4<T> vr_i = S.vel[c][i];
   I.vel = xyz(vr_i);
   I.rho = vr_i.w;
@@ -666,16 +668,22 @@ template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(c
     if (I.ri > T(0.0f)) I.ri *= P.art_coef;
     else I.ri = T(0.0f);
   }
-  V4<T> cv = cv_in[i];
-  I.shift = (int)cv.z;
-  Acc<T> A;
+  I.shift = (int)cv_i.z;
   A.accden = T(0.f);
   A.s = A.av = A.as = V3<T>{T(0), T(0), T(0)};
   A.gv = F9<T>{T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
+}
+
+constexpr int IX_THREADS = 128, IX_CAP = 96;
+
+// Pair sums of particle i straight from global memory: phase 1 lists candidates in
+// shared memory (my[k * stride]), phase 2 evaluates them in order.
+template <class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
+                                           const IState<T>& I, unsigned* my, int stride, int cap, Acc<T>& A) {
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const Rec<T>* __restrict__ rec = S.rec;
   const T th = P.two_h;
   const T r2max = P.r2_prefilter;
-  unsigned* my = nbl + threadIdx.x;
-  const int stride = blockDim.x;
   int cnt = 0;
   bool direct = false;
   for (int oc = 0; oc < 27; ++oc) {
@@ -692,7 +700,7 @@ template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(c
         const T r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
         if (r2 < r2max) {
           if (!direct) {
-            if (cnt < IX_CAP) {
+            if (cnt < cap) {
               my[cnt * stride] = (unsigned)j | ((unsigned)oc << 27);
               ++cnt;
               continue;
@@ -718,11 +726,20 @@ template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(c
       pair_term(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
     }
   }
+}
+
+// End of cuParticleInteractionMaterial: provisional velocity, wall contact
+// (cuParticleInteractionMaterialLoopContact, src/particle_interaction.cu:142-241) and
+// the stage outputs (src/particle_interaction.cu:284-295).
+template <class T> RWD void ix_finish(const Params<T>& P, const DevState<T>& S, int c, int cpar, int i, const I3 celli,
+                                      const IState<T>& I, const Acc<T>& A, V4<T> cv) {
+  const V4<T>* __restrict__ cv_in = S.cv[cpar];
+  const V4<T>* __restrict__ cf_in = S.cf[cpar];
   const V3<T> g{P.gravity[0], P.gravity[1], P.gravity[2]};
   const V3<T> acc_damp = I.vel * P.damping;
   const V4<T> acc1 = v4(A.s + A.av + A.as - acc_damp + g, A.accden);
+  const V4<T> vr_i{I.vel.x, I.vel.y, I.vel.z, I.rho};
   const V4<T> vr_new = vr_i + acc1 * P.dt;
-  // Wall contact (cuParticleInteractionMaterialLoopContact, src/particle_interaction.cu:142-241).
   V3<T> acc_st{T(0.0f), T(0.0f), T(0.0f)};
   V4<T> fo = cf_in[i];
   const V4<T> ny = S.cny[i];
@@ -732,6 +749,7 @@ template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(c
   const V3<T> nb{ny.x, ny.y, ny.z};
   const V3<T> dv{(vz.x - vr_new.x) * mrate, (vz.y - vr_new.y) * mrate, (vz.z - vr_new.z) * mrate};
   if (cv.y <= P.h * T(2) && dot(dv, nb) > T(0)) {
+    const V4<T>* __restrict__ pos = S.pos[c];
     const T fcoef = P.wall_fric;
     const T dvn_s = dot(dv, nb);
     const V3<T> dvn{nb.x * dvn_s, nb.y * dvn_s, nb.z * dvn_s};
@@ -781,11 +799,309 @@ template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(c
     fo = V4<T>{fric.x, fric.y, fric.z, T(0)};
     acc_st = fric * (T(1) / mass_i);
   }
-  cv_out[i] = cv;
-  cf_out[i] = fo;
+  S.cv[cpar ^ 1][i] = cv;
+  S.cf[cpar ^ 1][i] = fo;
   S.accad[i] = v4(A.s + A.av + A.as + acc_st - acc_damp + g, A.accden);
   st6(S.ace_a, S.ace_b, i, full2sym(A.gv));
   S.spin[i] = v4(skewpart(A.gv), T(0.f));
+}
+
+// Interaction, one thread per soil particle, neighbours read from global memory.
+// Used for whole launches when the chunked kernel is disabled, and by the chunked
+// kernel for chunks whose neighbour tile does not fit in shared memory.
+template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S,
+                                                                              const Dyn<T>* dyn, int cpar) {
+  extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int total = P.np - P.npb;
+  if (t >= total) return;
+  const int i = P.npb + t;
+  const int npm = dyn->npm;
+  if (t >= npm) {  // deleted slots keep their contact state
+    S.cv[cpar ^ 1][i] = S.cv[cpar][i];
+    S.cf[cpar ^ 1][i] = S.cf[cpar][i];
+    return;
+  }
+  const int c = dyn->cur_main;
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  const V4<T> cv = S.cv[cpar][i];
+  IState<T> I;
+  Acc<T> A;
+  ix_begin(P, S, c, i, cv, I, A);
+  ix_sums_global(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A);
+  ix_finish(P, S, c, cpar, i, celli, I, A, cv);
+}
+
+// ---------------------------------------------------------------------------------
+// Chunked interaction with the neighbour tile staged in shared memory.
+//
+// The soil particles of one cell column (x, y) are contiguous and ordered by z, so a
+// chunk of up to IX2_TB of them needs the 9 columns (x+-1, y+-1) over the z window
+// [z_first - 1, z_last + 1], in both layers: 18 contiguous index runs.  The block
+// copies those runs' positions into shared memory once; every candidate test of
+// phase 1 then reads shared memory.  Lists are filled in warp-synchronous rounds of
+// IX2_CAP entries (a round ends for the whole warp when any lane's list is full) and
+// evaluated in order with the next neighbour record prefetched, so each particle's
+// sums keep the reference's order exactly.  A chunk whose tile does not fit
+// (more than IX2_SMAX particles or IX2_NZW cells in z) runs the global path.
+// ---------------------------------------------------------------------------------
+constexpr int IX2_TB = 128, IX2_SMAX = 2048, IX2_NZW = 30, IX2_CAP = 32;
+
+struct Chunk {
+  int first, n, col, pad;
+};
+
+template <class T> struct Ix2Smem {
+  V4<T> spos[IX2_SMAX];
+  int2 tab[18][IX2_NZW];
+  int delta[18];   // global index = staged index + delta
+  int gbeg[18], glen[18], base[18];
+  unsigned list[IX2_CAP][IX2_TB];
+  int zl, nzw, total, fallback;
+};
+
+// Per-column soil runs and chunk counts (the chunk list is rebuilt after each sort).
+template <class T> __global__ void k_col_count(const Params<T> P, DevState<T> S) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ncol = P.cell_num[0] * P.cell_num[1];
+  if (col >= ncol) return;
+  const int nz = P.cell_num[2];
+  const int base = P.ncell_material + col * nz;
+  int beg = -1, end = -1;
+  for (int z = 0; z < nz; ++z) {
+    const int2 r = S.range[base + z];
+    if (r.y > r.x) {
+      if (beg < 0) beg = r.x;
+      end = r.y;
+    }
+  }
+  const int len = beg < 0 ? 0 : end - beg;
+  S.col_beg[col] = beg < 0 ? 0 : beg;
+  S.col_len[col] = len;
+  S.col_cnt[col] = (len + IX2_TB - 1) / IX2_TB;
+}
+
+template <class T> __global__ void __launch_bounds__(1024) k_col_scan(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
+  __shared__ int ws[32];
+  const int ncol = P.cell_num[0] * P.cell_num[1];
+  const int per = (ncol + 1023) / 1024;
+  const int b = threadIdx.x * per, e = min(ncol, b + per);
+  int s = 0;
+  for (int k = b; k < e; ++k) s += S.col_cnt[k];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int v = ws[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    ws[lane] = v;
+  }
+  __syncthreads();
+  int off = x - s + (w > 0 ? ws[w - 1] : 0);
+  for (int k = b; k < e; ++k) {
+    const int n = S.col_cnt[k];
+    S.col_off[k] = off;
+    off += n;
+  }
+  if (threadIdx.x == 1023) dyn->nchunks = off;
+}
+
+template <class T> __global__ void k_col_fill(const Params<T> P, DevState<T> S) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ncol = P.cell_num[0] * P.cell_num[1];
+  if (col >= ncol) return;
+  const int n = S.col_cnt[col];
+  if (n == 0) return;
+  const int len = S.col_len[col], beg = S.col_beg[col], off = S.col_off[col];
+  for (int k = 0; k < n; ++k) {  // n nearly equal chunks
+    const int a = beg + (int)((long)len * k / n);
+    const int b = beg + (int)((long)len * (k + 1) / n);
+    S.chunks[off + k] = Chunk{a, b - a, col, 0};
+  }
+}
+
+template <class T> __global__ void __launch_bounds__(IX2_TB) k_interaction2(const Params<T> P, DevState<T> S,
+                                                                          const Dyn<T>* dyn, int cpar) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Ix2Smem<T>& sm = *reinterpret_cast<Ix2Smem<T>*>(smraw);
+  const int tid = threadIdx.x;
+  // Deleted slots keep their contact state (the chunk list covers live particles only).
+  {
+    const int npm = dyn->npm;
+    const int ndel = P.np - P.npb - npm;
+    for (int t = blockIdx.x * IX2_TB + tid; t < ndel; t += gridDim.x * IX2_TB) {
+      const int i = P.npb + npm + t;
+      S.cv[cpar ^ 1][i] = S.cv[cpar][i];
+      S.cf[cpar ^ 1][i] = S.cf[cpar][i];
+    }
+  }
+  if ((int)blockIdx.x >= dyn->nchunks) return;
+  const Chunk ch = S.chunks[blockIdx.x];
+  const int c = dyn->cur_main;
+  const int ny = P.cell_num[1], nz = P.cell_num[2];
+  const int x = ch.col / ny, y = ch.col % ny;
+  if (tid == 0) {
+    const int z0 = S.cellpos[c][ch.first].z;
+    const int z1 = S.cellpos[c][ch.first + ch.n - 1].z;
+    const int zl = max(z0 - 1, 0), zh = min(z1 + 1, nz - 1);
+    sm.zl = zl;
+    sm.nzw = zh - zl + 1;
+  }
+  __syncthreads();
+  const int zl = sm.zl, nzw = sm.nzw;
+  const bool fits_z = nzw <= IX2_NZW;
+  if (fits_z) {
+    // Cell table (global ranges for now) of the 18 runs.
+    for (int idx = tid; idx < 18 * nzw; idx += IX2_TB) {
+      const int s = idx / nzw, zi = idx - s * nzw;
+      const int lay = s / 9, c9 = s - lay * 9;
+      const int xx = x + c9 % 3 - 1, yy = y + c9 / 3 - 1;
+      int2 r{0, 0};
+      if (xx >= 0 && yy >= 0 && xx < P.cell_num[0] && yy < ny)
+        r = S.range[(lay ? P.ncell_material : 0) + xx * ny * nz + yy * nz + zl + zi];
+      sm.tab[s][zi] = r;
+    }
+  }
+  __syncthreads();
+  if (tid < 18) {
+    int gb = 0, ge = 0;
+    bool any = false;
+    if (fits_z)
+      for (int zi = 0; zi < nzw; ++zi) {
+        const int2 r = sm.tab[tid][zi];
+        if (r.y > r.x) {
+          if (!any) gb = r.x;
+          ge = r.y;
+          any = true;
+        }
+      }
+    sm.gbeg[tid] = gb;
+    sm.glen[tid] = any ? ge - gb : 0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int tot = 0;
+    for (int s = 0; s < 18; ++s) {
+      sm.base[s] = tot;
+      sm.delta[s] = sm.gbeg[s] - tot;
+      tot += sm.glen[s];
+    }
+    sm.total = tot;
+    sm.fallback = (!fits_z || tot > IX2_SMAX) ? 1 : 0;
+  }
+  __syncthreads();
+  const bool fallback = sm.fallback != 0;
+  if (!fallback) {
+    // Staged coordinates for the table; copy the runs' positions.
+    for (int idx = tid; idx < 18 * nzw; idx += IX2_TB) {
+      const int s = idx / nzw, zi = idx - s * nzw;
+      const int2 r = sm.tab[s][zi];
+      sm.tab[s][zi] = (r.y > r.x) ? int2{r.x - sm.delta[s], r.y - sm.delta[s]} : int2{0, 0};
+    }
+    const V4<T>* __restrict__ pos = S.pos[c];
+    for (int s = 0; s < 18; ++s) {
+      const int n = sm.glen[s], gb = sm.gbeg[s], b = sm.base[s];
+      for (int k = tid; k < n; k += IX2_TB) sm.spos[b + k] = pos[gb + k];
+    }
+  }
+  __syncthreads();
+  if (tid >= ch.n) return;
+  const int i = ch.first + tid;
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  const V4<T> cv = S.cv[cpar][i];
+  IState<T> I;
+  Acc<T> A;
+  ix_begin(P, S, c, i, cv, I, A);
+  if (fallback) {
+    // Too big for the tile: same arithmetic from global memory, list in the round buffer.
+    ix_sums_global(P, S, c, celli, I, &sm.list[0][tid], IX2_TB, IX2_CAP, A);
+    ix_finish(P, S, c, cpar, i, celli, I, A, cv);
+    return;
+  }
+  const Rec<T>* __restrict__ rec = S.rec;
+  const T th = P.two_h;
+  const T r2max = P.r2_prefilter;
+  const int zi_i = cp.z - zl;
+  const unsigned lanes = __activemask();
+  int rr = 0;            // next of the 54 (cell offset, layer) ranges to open
+  int k = 0, kend = 0;   // current staged range
+  unsigned tag = 0;      // layer and offset of the current range, stored with each entry
+  V3<T> pmo{T(0), T(0), T(0)};
+  bool scanning = true;
+  for (;;) {
+    // Fill: candidates of this lane, in the reference's order, until any lane's list
+    // is full or every lane has scanned all 54 ranges.
+    int cnt = 0;
+    for (;;) {
+      const bool full = cnt >= IX2_CAP;
+      if (__any_sync(lanes, full) || !__any_sync(lanes, scanning)) break;
+      if (!scanning) continue;
+      if (k >= kend) {
+        scanning = false;
+        while (rr < 54) {
+          const int oc = rr >> 1, lay = rr & 1;
+          ++rr;
+          const I3 off = off_of(oc);
+          const int zz = zi_i + off.z;
+          if (zz < 0 || zz >= nzw) continue;
+          const int s = lay * 9 + (off.y + 1) * 3 + (off.x + 1);
+          const int2 r = sm.tab[s][zz];
+          if (r.y > r.x) {
+            k = r.x;
+            kend = r.y;
+            tag = ((unsigned)oc << 16) | ((unsigned)lay << 21);
+            const V3<T> o = mulI(off, th);
+            pmo = I.pos - o;
+            scanning = true;
+            break;
+          }
+        }
+        if (!scanning) continue;
+      }
+      const V4<T> pj = sm.spos[k];
+      const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
+      if (dx * dx + dy * dy + dz * dz < r2max) {
+        sm.list[cnt][tid] = (unsigned)k | tag;
+        ++cnt;
+      }
+      ++k;
+    }
+    // Evaluate this round's entries in order, prefetching the next record.
+    if (cnt > 0) {
+      unsigned ent = sm.list[0][tid];
+      int kk = (int)(ent & 0xffffu);
+      int oc = (int)((ent >> 16) & 31u), lay = (int)(ent >> 21);
+      int s = lay * 9 + (off_of(oc).y + 1) * 3 + (off_of(oc).x + 1);
+      NbVals<T> nb = load_nb(rec, kk + sm.delta[s]);
+      for (int e = 0; e < cnt; ++e) {
+        const NbVals<T> cur = nb;
+        const int kc = kk, occ = oc;
+        if (e + 1 < cnt) {
+          ent = sm.list[e + 1][tid];
+          kk = (int)(ent & 0xffffu);
+          oc = (int)((ent >> 16) & 31u);
+          lay = (int)(ent >> 21);
+          s = lay * 9 + (off_of(oc).y + 1) * 3 + (off_of(oc).x + 1);
+          nb = load_nb(rec, kk + sm.delta[s]);
+        }
+        const V3<T> o = mulI(off_of(occ), th);
+        const V4<T> pj = sm.spos[kc];
+        pair_eval(P, I, I.pos - V3<T>{pj.x, pj.y, pj.z} - o, cur, A);
+      }
+    }
+    if (!__any_sync(lanes, scanning)) break;
+  }
+  ix_finish(P, S, c, cpar, i, celli, I, A, cv);
 }
 
 // ---------------------------------------------------------------------------------

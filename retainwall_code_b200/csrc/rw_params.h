@@ -64,7 +64,8 @@ template <class T> struct Dyn {
   int need_sort;             // 1 when the new cell keys are not already in order
   unsigned err;              // RW_DERR_* bits
   int step;
-  int pad1_[2];
+  int nchunks;               // live entries of the interaction chunk list
+  int pad1_;
   Motion<T> mv[kMotionMax];
   Table<T> tab[kMotionMax];
 };
