@@ -73,6 +73,23 @@ RWD double pair_r2(double x, double y, double z) {
 RWD float pair_r(float r2) { return __fsqrt_rn(r2); }
 RWD double pair_r(double r2) { return __dsqrt_rn(r2); }
 
+// Arithmetic policy of the pair loop.  Every product is an explicit round-to-nearest
+// multiply, so the compiler cannot fuse it differently in different kernels:
+// Strict = false fuses multiply-adds (fma) at fixed places; Strict = true rounds every
+// product and sum separately, i.e. exactly the written evaluation order of the
+// reference's expressions (and of the CPU restatement).
+template <bool Strict> struct Fp {
+  static RWD float mul(float a, float b) { return __fmul_rn(a, b); }
+  static RWD double mul(double a, double b) { return __dmul_rn(a, b); }
+  static RWD float mad(float a, float b, float c) { return Strict ? __fadd_rn(__fmul_rn(a, b), c) : __fmaf_rn(a, b, c); }
+  static RWD double mad(double a, double b, double c) { return Strict ? __dadd_rn(__dmul_rn(a, b), c) : __fma_rn(a, b, c); }
+  // c - a*b
+  static RWD float msub(float a, float b, float c) { return Strict ? __fsub_rn(c, __fmul_rn(a, b)) : __fmaf_rn(-a, b, c); }
+  static RWD double msub(double a, double b, double c) { return Strict ? __dsub_rn(c, __dmul_rn(a, b)) : __fma_rn(-a, b, c); }
+  // a.x*b.x + a.y*b.y + a.z*b.z, left to right
+  template <class T> static RWD T dot3(T ax, T ay, T az, T bx, T by, T bz) { return mad(az, bz, mad(ay, by, mul(ax, bx))); }
+};
+
 // Wendland C2 (src/functions.h:142-143): GetKernel is a double expression in the
 // float build (its 2.0 / 0.5 literals), GetGradKernel stays in scalar.
 template <class T> RWD T kernel_w(T par, T q) {

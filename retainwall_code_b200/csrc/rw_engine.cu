@@ -70,6 +70,7 @@ template <class T> struct Engine final : EngineBase {
   cudaGraphExec_t gexec = nullptr;
   int g_cpar = -1;
   int ix_kernel = 1;     // 1: chunked interaction with a shared-memory tile; 0: global path
+  bool strict_fp = false;  // interaction arithmetic: fused multiply-adds (default) or separately rounded
   int ncol = 0, max_chunks = 0;
   rw_case_params cparams{};
   int output_number = 0;
@@ -325,9 +326,13 @@ template <class T> struct Engine final : EngineBase {
       }
     }
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
-    RW_CU(cudaFuncSetAttribute(k_interaction<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RW_CU(cudaFuncSetAttribute(k_interaction<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                IX_CAP * IX_THREADS * (int)sizeof(unsigned)));
-    RW_CU(cudaFuncSetAttribute(k_interaction2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RW_CU(cudaFuncSetAttribute(k_interaction<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               IX_CAP * IX_THREADS * (int)sizeof(unsigned)));
+    RW_CU(cudaFuncSetAttribute(k_interaction2<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(Ix2Smem<T>)));
+    RW_CU(cudaFuncSetAttribute(k_interaction2<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(Ix2Smem<T>)));
     neighbor_search(0);
     RW_CU(cudaStreamSynchronize(st));
@@ -395,12 +400,14 @@ template <class T> struct Engine final : EngineBase {
   void interaction() override {
     const int n = P.np - P.npb;
     if (n > 0) {
+      const size_t sm1 = IX_CAP * IX_THREADS * sizeof(unsigned);
       if (ix_kernel == 1) {
         const unsigned grid = (unsigned)std::max(max_chunks, (int)nblk(n, IX2_TB));
-        k_interaction2<T><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
+        if (strict_fp) k_interaction2<T, true><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
+        else k_interaction2<T, false><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
       } else {
-        k_interaction<T><<<nblk(n, IX_THREADS), IX_THREADS, IX_CAP * IX_THREADS * sizeof(unsigned), st>>>(P, S, d_dyn,
-                                                                                                       cpar);
+        if (strict_fp) k_interaction<T, true><<<nblk(n, IX_THREADS), IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
+        else k_interaction<T, false><<<nblk(n, IX_THREADS), IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
       }
       check_launch();
     }
@@ -565,6 +572,8 @@ template <class T> struct Engine final : EngineBase {
   int set_option(int opt, double v) override {
     if (opt == RW_OPT_WALL_FRICTION) {
       P.wall_fric = (T)v;
+    } else if (opt == RW_OPT_STRICT_FP) {
+      strict_fp = v != 0.0;
     } else if (opt == RW_OPT_INTERACTION_KERNEL) {
       if (v != 0.0 && v != 1.0) return RW_EINVAL;
       ix_kernel = (int)v;

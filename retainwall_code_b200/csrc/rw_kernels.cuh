@@ -604,68 +604,84 @@ template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) 
 
 // One pair (i, j) of cuParticleInteractionMaterialLoopSolution
 // (src/particle_interaction.cu:29-114), given dr = (pos_i - pos_j) - offset * 2h.
-template <class T> RWD void pair_eval(const Params<T>& P, const IState<T>& I, const V3<T> dr, const NbVals<T>& nb,
-                                      Acc<T>& A) {
+template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const IState<T>& I, const V3<T> dr,
+                                                   const NbVals<T>& nb, Acc<T>& A) {
+  using F = Fp<Strict>;
   T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
-  T q = r * P.i_h;
+  T q = F::mul(r, P.i_h);
   if (!(q < T(2.0f))) return;
   T ker = kernel_w(P.knorm, q);
-  T dwdr = kernel_f(P.kgrad, q);
-  V3<T> gker = dr * dwdr;
+  const T t = T(2.0f) - q;
+  T dwdr = F::mul(F::mul(F::mul(P.kgrad, t), t), t);
+  const V3<T> gker{F::mul(dr.x, dwdr), F::mul(dr.y, dwdr), F::mul(dr.z, dwdr)};
   const T rho_j = nb.vr.w, mass_j = nb.aux.x, vol_j = nb.aux.y;
   const bool contact_j = nb.aux.w != T(0);
-  V3<T> dvel = I.vel - V3<T>{nb.vr.x, nb.vr.y, nb.vr.z};
+  V3<T> dvel{I.vel.x - nb.vr.x, I.vel.y - nb.vr.y, I.vel.z - nb.vr.z};
   if (contact_j && I.shift == 1) dvel = V3<T>{T(0), T(0), T(0)};
-  A.gv.xx -= dvel.x * gker.x * vol_j;
-  A.gv.xy -= dvel.x * gker.y * vol_j;
-  A.gv.xz -= dvel.x * gker.z * vol_j;
-  A.gv.yx -= dvel.y * gker.x * vol_j;
-  A.gv.yy -= dvel.y * gker.y * vol_j;
-  A.gv.yz -= dvel.y * gker.z * vol_j;
-  A.gv.zx -= dvel.z * gker.x * vol_j;
-  A.gv.zy -= dvel.z * gker.y * vol_j;
-  A.gv.zz -= dvel.z * gker.z * vol_j;
+  // grad_vel -= (dvel (x) gker) * vol_j
+  A.gv.xx = F::msub(F::mul(dvel.x, gker.x), vol_j, A.gv.xx);
+  A.gv.xy = F::msub(F::mul(dvel.x, gker.y), vol_j, A.gv.xy);
+  A.gv.xz = F::msub(F::mul(dvel.x, gker.z), vol_j, A.gv.xz);
+  A.gv.yx = F::msub(F::mul(dvel.y, gker.x), vol_j, A.gv.yx);
+  A.gv.yy = F::msub(F::mul(dvel.y, gker.y), vol_j, A.gv.yy);
+  A.gv.yz = F::msub(F::mul(dvel.y, gker.z), vol_j, A.gv.yz);
+  A.gv.zx = F::msub(F::mul(dvel.z, gker.x), vol_j, A.gv.zx);
+  A.gv.zy = F::msub(F::mul(dvel.z, gker.y), vol_j, A.gv.zy);
+  A.gv.zz = F::msub(F::mul(dvel.z, gker.z), vol_j, A.gv.zz);
   if (contact_j) return;
-  A.accden += I.rho * dot(dvel, gker) * vol_j;
+  const T dvg = F::dot3(dvel.x, dvel.y, dvel.z, gker.x, gker.y, gker.z);
+  A.accden = F::mad(F::mul(I.rho, dvg), vol_j, A.accden);
   const S6<T> st{I.sor.xx + nb.sa.x, I.sor.yy + nb.sa.y, I.sor.zz + nb.sa.z,
                  I.sor.xy + nb.sa.w, I.sor.xz + nb.sb.x, I.sor.yz + nb.sb.y};
-  A.s = A.s + dotSV(st, gker) * mass_j;
+  const T fx = F::dot3(st.xx, st.xy, st.xz, gker.x, gker.y, gker.z);
+  const T fy = F::dot3(st.xy, st.yy, st.yz, gker.x, gker.y, gker.z);
+  const T fz = F::dot3(st.xz, st.yz, st.zz, gker.x, gker.y, gker.z);
+  A.s.x = F::mad(fx, mass_j, A.s.x);
+  A.s.y = F::mad(fy, mass_j, A.s.y);
+  A.s.z = F::mad(fz, mass_j, A.s.z);
   if (P.viscosity_type == 1) {
     T artv = T(0.0f);
-    T visc = dot(dvel, dr);
+    const T visc = F::dot3(dvel.x, dvel.y, dvel.z, dr.x, dr.y, dr.z);
     if (visc < T(0.0f)) {
-      T phi = P.h * visc / (r * r + P.eta);
-      artv = P.alpha_m * P.cs_m * phi / (T(0.5f) * (I.rho + rho_j));
+      const T phi = F::mul(P.h, visc) / F::mad(r, r, P.eta);
+      artv = F::mul(F::mul(P.alpha_m, P.cs_m), phi) / F::mul(T(0.5f), I.rho + rho_j);
     }
-    A.av = A.av + gker * (mass_j * artv);
+    const T m = F::mul(mass_j, artv);
+    A.av.x = F::mad(gker.x, m, A.av.x);
+    A.av.y = F::mad(gker.y, m, A.av.y);
+    A.av.z = F::mad(gker.z, m, A.av.z);
   }
   if (P.art_coef != T(0.f)) {
     T artp = I.ri + nb.aux.z;
     if (artp > T(0.0f)) {
-      artp *= f_pow(ker / P.kernel_dr, P.kernel_zero / P.kernel_dr);
-      A.as = A.as - gker * (mass_j * artp);
+      artp = F::mul(artp, f_pow(ker / P.kernel_dr, P.kernel_zero / P.kernel_dr));
+      const T m = F::mul(mass_j, artp);
+      A.as.x = F::msub(gker.x, m, A.as.x);
+      A.as.y = F::msub(gker.y, m, A.as.y);
+      A.as.z = F::msub(gker.z, m, A.as.z);
     }
   }
 }
 
-template <class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, const V3<T> dr,
-                                      const Rec<T>* __restrict__ rec, int j, Acc<T>& A) {
-  pair_eval(P, I, dr, load_nb(rec, j), A);
+template <bool Strict, class T> RWD void pair_term(const Params<T>& P, const IState<T>& I, const V3<T> dr,
+                                                   const Rec<T>* __restrict__ rec, int j, Acc<T>& A) {
+  pair_eval<Strict>(P, I, dr, load_nb(rec, j), A);
 }
 
 // Particle i's own state at the start of cuParticleInteractionMaterial
 // (src/particle_interaction.cu:264-277).
-template <class T> RWD void ix_begin(const Params<T>& P, const DevState<T>& S, int c, int i, const V4<T>& cv_i,
-                                     IState<T>& I, Acc<T>& A) {
+template <bool Strict, class T> RWD void ix_begin(const Params<T>& P, const DevState<T>& S, int c, int i,
+                                                  const V4<T>& cv_i, IState<T>& I, Acc<T>& A) {
+  using F = Fp<Strict>;
   I.pos = ld3(S.pos[c], i);
   const V4<T> vr_i = S.vel[c][i];
   I.vel = xyz(vr_i);
   I.rho = vr_i.w;
-  I.sor = ld6(S.str_a[c], S.str_b[c], i) / (vr_i.w * vr_i.w);
+  I.sor = ld6(S.str_a[c], S.str_b[c], i) / F::mul(vr_i.w, vr_i.w);
   I.ri = T(0.0f);
   if (P.art_coef != T(0.f)) {
     I.ri = trace(I.sor);
-    if (I.ri > T(0.0f)) I.ri *= P.art_coef;
+    if (I.ri > T(0.0f)) I.ri = F::mul(I.ri, P.art_coef);
     else I.ri = T(0.0f);
   }
   I.shift = (int)cv_i.z;
@@ -678,7 +694,7 @@ constexpr int IX_THREADS = 128, IX_CAP = 96;
 
 // Pair sums of particle i straight from global memory: phase 1 lists candidates in
 // shared memory (my[k * stride]), phase 2 evaluates them in order.
-template <class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
+template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
                                            const IState<T>& I, unsigned* my, int stride, int cap, Acc<T>& A) {
   const V4<T>* __restrict__ pos = S.pos[c];
   const Rec<T>* __restrict__ rec = S.rec;
@@ -709,11 +725,11 @@ template <class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>
               const unsigned ent = my[e * stride];
               const int jj = (int)(ent & 0x7ffffffu);
               const V3<T> oo = mulI(off_of((int)(ent >> 27)), th);
-              pair_term(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
+              pair_term<Strict>(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
             }
             direct = true;
           }
-          pair_term(P, I, dr, rec, j, A);
+          pair_term<Strict>(P, I, dr, rec, j, A);
         }
       }
     }
@@ -723,7 +739,7 @@ template <class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>
       const unsigned ent = my[e * stride];
       const int jj = (int)(ent & 0x7ffffffu);
       const V3<T> oo = mulI(off_of((int)(ent >> 27)), th);
-      pair_term(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
+      pair_term<Strict>(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
     }
   }
 }
@@ -731,42 +747,50 @@ template <class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>
 // End of cuParticleInteractionMaterial: provisional velocity, wall contact
 // (cuParticleInteractionMaterialLoopContact, src/particle_interaction.cu:142-241) and
 // the stage outputs (src/particle_interaction.cu:284-295).
-template <class T> RWD void ix_finish(const Params<T>& P, const DevState<T>& S, int c, int cpar, int i, const I3 celli,
-                                      const IState<T>& I, const Acc<T>& A, V4<T> cv) {
+template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const DevState<T>& S, int c, int cpar, int i,
+                                                   const I3 celli, const IState<T>& I, const Acc<T>& A, V4<T> cv) {
+  using F = Fp<Strict>;
   const V4<T>* __restrict__ cv_in = S.cv[cpar];
   const V4<T>* __restrict__ cf_in = S.cf[cpar];
   const V3<T> g{P.gravity[0], P.gravity[1], P.gravity[2]};
-  const V3<T> acc_damp = I.vel * P.damping;
-  const V4<T> acc1 = v4(A.s + A.av + A.as - acc_damp + g, A.accden);
-  const V4<T> vr_i{I.vel.x, I.vel.y, I.vel.z, I.rho};
-  const V4<T> vr_new = vr_i + acc1 * P.dt;
+  const V3<T> damp{F::mul(I.vel.x, P.damping), F::mul(I.vel.y, P.damping), F::mul(I.vel.z, P.damping)};
+  const V3<T> acc0{A.s.x + A.av.x + A.as.x - damp.x + g.x, A.s.y + A.av.y + A.as.y - damp.y + g.y,
+                   A.s.z + A.av.z + A.as.z - damp.z + g.z};
+  const V4<T> vr_new{F::mad(acc0.x, P.dt, I.vel.x), F::mad(acc0.y, P.dt, I.vel.y), F::mad(acc0.z, P.dt, I.vel.z),
+                     F::mad(A.accden, P.dt, I.rho)};
   V3<T> acc_st{T(0.0f), T(0.0f), T(0.0f)};
   V4<T> fo = cf_in[i];
   const V4<T> ny = S.cny[i];
   const V4<T> vz = S.cvz[i];
   const T mass_i = S.idm[c][i].y;
   const T mrate = T(2.0f) / (T(2.0f) + T(0.0f));
-  const V3<T> nb{ny.x, ny.y, ny.z};
-  const V3<T> dv{(vz.x - vr_new.x) * mrate, (vz.y - vr_new.y) * mrate, (vz.z - vr_new.z) * mrate};
-  if (cv.y <= P.h * T(2) && dot(dv, nb) > T(0)) {
+  const V3<T> dv{F::mul(vz.x - vr_new.x, mrate), F::mul(vz.y - vr_new.y, mrate), F::mul(vz.z - vr_new.z, mrate)};
+  const T dvn_s = F::dot3(dv.x, dv.y, dv.z, ny.x, ny.y, ny.z);
+  if (cv.y <= F::mul(P.h, T(2)) && dvn_s > T(0)) {
     const V4<T>* __restrict__ pos = S.pos[c];
     const T fcoef = P.wall_fric;
-    const T dvn_s = dot(dv, nb);
-    const V3<T> dvn{nb.x * dvn_s, nb.y * dvn_s, nb.z * dvn_s};
-    const V3<T> fn = dvn * mass_i / P.dt;
-    const V3<T> dvt = dv - dvn;
-    V3<T> ft = dvt * mass_i / P.dt;
-    const T afn = enorm(fn), aft = enorm(ft);
-    if (aft > (fcoef * afn)) {
-      ft = ft * (fcoef * afn / aft);
+    const V3<T> dvn{F::mul(ny.x, dvn_s), F::mul(ny.y, dvn_s), F::mul(ny.z, dvn_s)};
+    const V3<T> fn{F::mul(dvn.x, mass_i) / P.dt, F::mul(dvn.y, mass_i) / P.dt, F::mul(dvn.z, mass_i) / P.dt};
+    const V3<T> dvt{dv.x - dvn.x, dv.y - dvn.y, dv.z - dvn.z};
+    V3<T> ft{F::mul(dvt.x, mass_i) / P.dt, F::mul(dvt.y, mass_i) / P.dt, F::mul(dvt.z, mass_i) / P.dt};
+    const T afn = f_sqrt(F::dot3(fn.x, fn.y, fn.z, fn.x, fn.y, fn.z));
+    const T aft = f_sqrt(F::dot3(ft.x, ft.y, ft.z, ft.x, ft.y, ft.z));
+    const T cap = F::mul(fcoef, afn);
+    if (aft > cap) {
+      const T ratio = cap / aft;
+      ft = V3<T>{F::mul(ft.x, ratio), F::mul(ft.y, ratio), F::mul(ft.z, ratio)};
       cv.z = T(1);
     } else {
       cv.z = T(0);
     }
-    V3<T> fric = ft + fn;
-    if (cv.y > P.dr * T(1.0f)) {
+    V3<T> fric{ft.x + fn.x, ft.y + fn.y, ft.z + fn.z};
+    if (cv.y > F::mul(P.dr, T(1.0f))) {
       int count = 0;
-      const V3<T> pabs_i = I.pos + mulI(celli, T(2.0f) * P.h);
+      const T h2 = F::mul(T(2.0f), P.h);
+      const V3<T> pabs_i{F::mad((T)celli.x, h2, I.pos.x), F::mad((T)celli.y, h2, I.pos.y),
+                         F::mad((T)celli.z, h2, I.pos.z)};
+      const T ylim = F::mul(P.dr, T(1.0001f));
+      const T half_dr = P.dr / T(2);
       for (int oc = 0; oc < 27; ++oc) {
         const I3 off = off_of(oc);
         const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
@@ -774,34 +798,35 @@ template <class T> RWD void ix_finish(const Params<T>& P, const DevState<T>& S, 
         const int2 rg = S.range[key_of(P, cj) + P.ncell_material];
         for (int j = rg.x; j < rg.y; ++j) {
           const V4<T> cvj = cv_in[j];
-          if (cvj.y <= P.dr * T(1.0001f)) {
+          if (cvj.y <= ylim) {
             const V4<T> pj = pos[j];
             const int4 cpj = S.cellpos[c][j];
-            const V3<T> pabs_j{pj.x + (T)cpj.x * (T(2.0f) * P.h), pj.y + (T)cpj.y * (T(2.0f) * P.h),
-                               pj.z + (T)cpj.z * (T(2.0f) * P.h)};
-            const V3<T> dc = pabs_i - pabs_j;
-            const T rcol = f_abs(dc.x * ny.z + dc.y * ny.y + dc.z * ny.x);
+            const V3<T> pabs_j{F::mad((T)cpj.x, h2, pj.x), F::mad((T)cpj.y, h2, pj.y), F::mad((T)cpj.z, h2, pj.z)};
+            const V3<T> dc{pabs_i.x - pabs_j.x, pabs_i.y - pabs_j.y, pabs_i.z - pabs_j.z};
+            const T rcol = f_abs(F::dot3(dc.x, dc.y, dc.z, ny.z, ny.y, ny.x));
             const T cvx_j0 = (j == i) ? cv.x : cvj.x;
-            if (rcol <= P.dr / T(2) && cvx_j0 != T(0)) {
+            if (rcol <= half_dr && cvx_j0 != T(0)) {
               if (cv.x > cvx_j0) cv.x = cvx_j0;
               const T cvx_j = (j == i) ? cv.x : cvj.x;
               const V4<T> fj = cf_in[j];
-              fric.x = fj.x * cv.x / cvx_j;
-              fric.y = fj.y * cv.x / cvx_j;
-              fric.z = fj.z * cv.x / cvx_j;
+              fric.x = F::mul(fj.x, cv.x) / cvx_j;
+              fric.y = F::mul(fj.y, cv.x) / cvx_j;
+              fric.z = F::mul(fj.z, cv.x) / cvx_j;
               count++;
             }
           }
         }
       }
-      if (count == 0) fric = fric * T(0);
+      if (count == 0) fric = V3<T>{F::mul(fric.x, T(0)), F::mul(fric.y, T(0)), F::mul(fric.z, T(0))};
     }
     fo = V4<T>{fric.x, fric.y, fric.z, T(0)};
-    acc_st = fric * (T(1) / mass_i);
+    const T im = T(1) / mass_i;
+    acc_st = V3<T>{F::mul(fric.x, im), F::mul(fric.y, im), F::mul(fric.z, im)};
   }
   S.cv[cpar ^ 1][i] = cv;
   S.cf[cpar ^ 1][i] = fo;
-  S.accad[i] = v4(A.s + A.av + A.as + acc_st - acc_damp + g, A.accden);
+  S.accad[i] = V4<T>{A.s.x + A.av.x + A.as.x + acc_st.x - damp.x + g.x, A.s.y + A.av.y + A.as.y + acc_st.y - damp.y + g.y,
+                     A.s.z + A.av.z + A.as.z + acc_st.z - damp.z + g.z, A.accden};
   st6(S.ace_a, S.ace_b, i, full2sym(A.gv));
   S.spin[i] = v4(skewpart(A.gv), T(0.f));
 }
@@ -809,8 +834,8 @@ template <class T> RWD void ix_finish(const Params<T>& P, const DevState<T>& S, 
 // Interaction, one thread per soil particle, neighbours read from global memory.
 // Used for whole launches when the chunked kernel is disabled, and by the chunked
 // kernel for chunks whose neighbour tile does not fit in shared memory.
-template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S,
-                                                                              const Dyn<T>* dyn, int cpar) {
+template <class T, bool Strict> __global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S,
+                                                                                           const Dyn<T>* dyn, int cpar) {
   extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int total = P.np - P.npb;
@@ -828,9 +853,9 @@ template <class T> __global__ void __launch_bounds__(IX_THREADS) k_interaction(c
   const V4<T> cv = S.cv[cpar][i];
   IState<T> I;
   Acc<T> A;
-  ix_begin(P, S, c, i, cv, I, A);
-  ix_sums_global(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A);
-  ix_finish(P, S, c, cpar, i, celli, I, A, cv);
+  ix_begin<Strict>(P, S, c, i, cv, I, A);
+  ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A);
+  ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
 
 // ---------------------------------------------------------------------------------
@@ -929,8 +954,8 @@ template <class T> __global__ void k_col_fill(const Params<T> P, DevState<T> S) 
   }
 }
 
-template <class T> __global__ void __launch_bounds__(IX2_TB) k_interaction2(const Params<T> P, DevState<T> S,
-                                                                          const Dyn<T>* dyn, int cpar) {
+template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_interaction2(const Params<T> P, DevState<T> S,
+                                                                                       const Dyn<T>* dyn, int cpar) {
   extern __shared__ __align__(16) unsigned char smraw[];
   Ix2Smem<T>& sm = *reinterpret_cast<Ix2Smem<T>*>(smraw);
   const int tid = threadIdx.x;
@@ -1021,11 +1046,11 @@ template <class T> __global__ void __launch_bounds__(IX2_TB) k_interaction2(cons
   const V4<T> cv = S.cv[cpar][i];
   IState<T> I;
   Acc<T> A;
-  ix_begin(P, S, c, i, cv, I, A);
+  ix_begin<Strict>(P, S, c, i, cv, I, A);
   if (fallback) {
     // Too big for the tile: same arithmetic from global memory, list in the round buffer.
-    ix_sums_global(P, S, c, celli, I, &sm.list[0][tid], IX2_TB, IX2_CAP, A);
-    ix_finish(P, S, c, cpar, i, celli, I, A, cv);
+    ix_sums_global<Strict>(P, S, c, celli, I, &sm.list[0][tid], IX2_TB, IX2_CAP, A);
+    ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
     return;
   }
   const Rec<T>* __restrict__ rec = S.rec;
@@ -1096,12 +1121,12 @@ template <class T> __global__ void __launch_bounds__(IX2_TB) k_interaction2(cons
         }
         const V3<T> o = mulI(off_of(occ), th);
         const V4<T> pj = sm.spos[kc];
-        pair_eval(P, I, I.pos - V3<T>{pj.x, pj.y, pj.z} - o, cur, A);
+        pair_eval<Strict>(P, I, I.pos - V3<T>{pj.x, pj.y, pj.z} - o, cur, A);
       }
     }
     if (!__any_sync(lanes, scanning)) break;
   }
-  ix_finish(P, S, c, cpar, i, celli, I, A, cv);
+  ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
 
 // ---------------------------------------------------------------------------------
