@@ -200,6 +200,10 @@ def run_ours(args, ws, rank, local):
     case, cfg = make_case(args.workload)
     # ---- device-resident throughput ----------------------------------------------------
     sim = LoquatSph(case=case, device=local, precision=4)
+    if args.ix_kernel is not None:
+        sim.set_option(_abi.OPT_INTERACTION_KERNEL, args.ix_kernel)
+    if args.strict:
+        sim.set_option(_abi.OPT_STRICT_FP, 1)
     inf = sim.info()
     sim.step(args.warmup)
     sim.synchronize()
@@ -283,6 +287,8 @@ def main():
     ap.add_argument("--workload", default="wall2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and stage-profile passes")
+    ap.add_argument("--ix-kernel", type=int, default=None, help="interaction kernel: 1 chunked (default), 0 global")
+    ap.add_argument("--strict", action="store_true", help="separately rounded interaction arithmetic")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":  # host cores only: rank 0 runs, the other ranks exit

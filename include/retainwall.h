@@ -130,8 +130,9 @@ enum {
   RW_OPT_WALL_FRICTION = 0,  /* Coulomb coefficient of contact walls (default from the case) */
   RW_OPT_COMPAT_CONTACT = 1, /* 1 (default): contact state bound to array slots as in the reference
                                 (src/loquat.cu:254-287 never permutes it); 0: follows the particle */
-  RW_OPT_INTERACTION_KERNEL = 2, /* 1 (default): chunked interaction with the neighbour tile in shared
-                                   memory; 0: neighbours read from global memory.  Same results. */
+  RW_OPT_INTERACTION_KERNEL = 2, /* 0 (default): one thread per particle, neighbours through L1/L2;
+                                   1: column chunks with the neighbour positions staged in shared memory.
+                                   Bit-identical results. */
   RW_OPT_STRICT_FP = 3          /* interaction arithmetic: 0 (default) fused multiply-adds at fixed places;
                                    1 every product and sum rounded separately, the written order of the
                                    reference's expressions (slower; for bit-level comparisons) */

@@ -69,7 +69,7 @@ template <class T> struct Engine final : EngineBase {
   bool compat_contact = true;
   cudaGraphExec_t gexec = nullptr;
   int g_cpar = -1;
-  int ix_kernel = 1;     // 1: chunked interaction with a shared-memory tile; 0: global path
+  int ix_kernel = 0;     // 0: neighbours through L1/L2 (default); 1: chunked, shared-memory position tile
   bool strict_fp = false;  // interaction arithmetic: fused multiply-adds (default) or separately rounded
   int ncol = 0, max_chunks = 0;
   rw_case_params cparams{};

@@ -10,13 +10,13 @@
 namespace rw {
 
 // Per-particle record consumed by the pair loop of the interaction: everything the
-// reference recomputes per neighbour pair from j's state (mass, volume, sigma/rho^2,
-// artificial-stress term) computed once per particle per section.
+// reference recomputes per neighbour pair from j's state (mass, volume, sigma/rho^2),
+// computed once per particle per section.  48 bytes in float: the contact-wall flag
+// travels as the sign of the (always positive) volume.
 template <class T> struct Rec {
-  V4<T> vr;   // velocity xyz, density
-  V4<T> aux;  // mass, volume = mass/rho, artificial-stress term of j, contact-wall flag
-  V4<T> sa;   // sigma/rho^2: xx yy zz xy
-  V4<T> sb;   // sigma/rho^2: xz yz
+  V4<T> vr;  // velocity xyz, density
+  V4<T> a;   // mass, +-volume (negative: contact-wall particle), sigma/rho^2 xx, yy
+  V4<T> b;   // sigma/rho^2 zz, xy, xz, yz
 };
 
 template <class T> struct DevState {
@@ -94,27 +94,22 @@ template <class T> RWD int key_of(const Params<T>& P, I3 c) {
 RWD I3 off_of(int oc) { return {oc % 3 - 1, (oc / 3) % 3 - 1, oc / 9 - 1}; }
 
 RWD float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+RWD float rmul(float a, float b) { return __fmul_rn(a, b); }
+RWD double rmul(double a, double b) { return __dmul_rn(a, b); }
 RWD double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 RWD float add_rn(float a, float b) { return __fadd_rn(a, b); }
 RWD double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
 // Neighbour record of particle i (boundary: mass = V0 rho; material: idmassidx.y),
-// with the reference's per-pair expressions (src/particle_interaction.cu:44-49,71,98-104).
+// with the reference's per-pair expressions (src/particle_interaction.cu:44-49,71).
 template <class T> RWD void write_rec(const Params<T>& P, Rec<T>* rec, int i, V4<T> vr, S6<T> s, T mass, bool contact) {
-  T rho = vr.w;
-  S6<T> sor = s / (rho * rho);
-  T vol = mass / rho;
-  T rj = T(0.0f);
-  if (P.art_coef != T(0.f)) {
-    rj = trace(sor);
-    if (rj > T(0.0f)) rj *= P.art_coef;
-    else rj = T(0.0f);
-  }
+  const T rho = vr.w;
+  const S6<T> sor = s / rmul(rho, rho);
+  const T vol = mass / rho;
   Rec<T> r;
   r.vr = vr;
-  r.aux = V4<T>{mass, vol, rj, contact ? T(1) : T(0)};
-  r.sa = V4<T>{sor.xx, sor.yy, sor.zz, sor.xy};
-  r.sb = V4<T>{sor.xz, sor.yz, T(0), T(0)};
+  r.a = V4<T>{mass, contact ? -vol : vol, sor.xx, sor.yy};
+  r.b = V4<T>{sor.zz, sor.xy, sor.xz, sor.yz};
   rec[i] = r;
 }
 
@@ -589,16 +584,15 @@ template <class T> struct IState {
   int shift;
 };
 
-// The neighbour-side values one pair term needs (a Rec without its padding).
+// The neighbour-side values one pair term needs.
 template <class T> struct NbVals {
-  V4<T> vr, aux, sa, sb;
+  V4<T> vr, a, b;
 };
 template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) {
   NbVals<T> v;
   v.vr = rec[j].vr;
-  v.aux = rec[j].aux;
-  v.sa = rec[j].sa;
-  v.sb = rec[j].sb;
+  v.a = rec[j].a;
+  v.b = rec[j].b;
   return v;
 }
 
@@ -614,8 +608,8 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
   const T t = T(2.0f) - q;
   T dwdr = F::mul(F::mul(F::mul(P.kgrad, t), t), t);
   const V3<T> gker{F::mul(dr.x, dwdr), F::mul(dr.y, dwdr), F::mul(dr.z, dwdr)};
-  const T rho_j = nb.vr.w, mass_j = nb.aux.x, vol_j = nb.aux.y;
-  const bool contact_j = nb.aux.w != T(0);
+  const T rho_j = nb.vr.w, mass_j = nb.a.x, vol_j = f_abs(nb.a.y);
+  const bool contact_j = nb.a.y < T(0);
   V3<T> dvel{I.vel.x - nb.vr.x, I.vel.y - nb.vr.y, I.vel.z - nb.vr.z};
   if (contact_j && I.shift == 1) dvel = V3<T>{T(0), T(0), T(0)};
   // grad_vel -= (dvel (x) gker) * vol_j
@@ -631,8 +625,8 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
   if (contact_j) return;
   const T dvg = F::dot3(dvel.x, dvel.y, dvel.z, gker.x, gker.y, gker.z);
   A.accden = F::mad(F::mul(I.rho, dvg), vol_j, A.accden);
-  const S6<T> st{I.sor.xx + nb.sa.x, I.sor.yy + nb.sa.y, I.sor.zz + nb.sa.z,
-                 I.sor.xy + nb.sa.w, I.sor.xz + nb.sb.x, I.sor.yz + nb.sb.y};
+  const S6<T> st{I.sor.xx + nb.a.z, I.sor.yy + nb.a.w, I.sor.zz + nb.b.x,
+                 I.sor.xy + nb.b.y, I.sor.xz + nb.b.z, I.sor.yz + nb.b.w};
   const T fx = F::dot3(st.xx, st.xy, st.xz, gker.x, gker.y, gker.z);
   const T fy = F::dot3(st.xy, st.yy, st.yz, gker.x, gker.y, gker.z);
   const T fz = F::dot3(st.xz, st.yz, st.zz, gker.x, gker.y, gker.z);
@@ -652,7 +646,10 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
     A.av.z = F::mad(gker.z, m, A.av.z);
   }
   if (P.art_coef != T(0.f)) {
-    T artp = I.ri + nb.aux.z;
+    T rj = nb.a.z + nb.a.w + nb.b.x;  // artificial-stress term of j (src/particle_interaction.cu:102-104)
+    if (rj > T(0.0f)) rj = F::mul(rj, P.art_coef);
+    else rj = T(0.0f);
+    T artp = I.ri + rj;
     if (artp > T(0.0f)) {
       artp = F::mul(artp, f_pow(ker / P.kernel_dr, P.kernel_zero / P.kernel_dr));
       const T m = F::mul(mass_j, artp);
@@ -694,54 +691,68 @@ constexpr int IX_THREADS = 128, IX_CAP = 96;
 
 // Pair sums of particle i straight from global memory: phase 1 lists candidates in
 // shared memory (my[k * stride]), phase 2 evaluates them in order.
-template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
-                                           const IState<T>& I, unsigned* my, int stride, int cap, Acc<T>& A) {
+template <bool Strict, class T> RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c,
+                                                      const IState<T>& I, const unsigned* my, int stride, int cnt,
+                                                      Acc<T>& A) {
   const V4<T>* __restrict__ pos = S.pos[c];
   const Rec<T>* __restrict__ rec = S.rec;
   const T th = P.two_h;
+  if (cnt <= 0) return;
+  unsigned ent = my[0];
+  int jj = (int)(ent & 0x7ffffffu);
+  int oc = (int)(ent >> 27);
+  V4<T> pj = pos[jj];
+  NbVals<T> nb = load_nb(rec, jj);
+  for (int e = 0; e < cnt; ++e) {  // next entry's position and record prefetched
+    const V4<T> pc = pj;
+    const NbVals<T> cur = nb;
+    const int occ = oc;
+    if (e + 1 < cnt) {
+      ent = my[(e + 1) * stride];
+      jj = (int)(ent & 0x7ffffffu);
+      oc = (int)(ent >> 27);
+      pj = pos[jj];
+      nb = load_nb(rec, jj);
+    }
+    const V3<T> o = mulI(off_of(occ), th);
+    pair_eval<Strict>(P, I, I.pos - V3<T>{pc.x, pc.y, pc.z} - o, cur, A);
+  }
+}
+
+// Pair sums of particle i straight from global memory: phase 1 lists candidates in
+// shared memory (my[k * stride]), phase 2 evaluates them in order.  A list that fills
+// up is evaluated and emptied, and the scan resumes (order preserved).
+template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
+                                                        const IState<T>& I, unsigned* my, int stride, int cap, Acc<T>& A) {
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const T th = P.two_h;
   const T r2max = P.r2_prefilter;
   int cnt = 0;
-  bool direct = false;
   for (int oc = 0; oc < 27; ++oc) {
     const I3 off = off_of(oc);
     const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
     if (!in_grid(P, cj)) continue;
     const int k = key_of(P, cj);
-    const V3<T> o = mulI(off, th);
+    const V3<T> pmo = I.pos - mulI(off, th);  // conservative pre-test only
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
       const int2 rg = S.range[pass ? k + P.ncell_material : k];
+#pragma unroll 4
       for (int j = rg.x; j < rg.y; ++j) {
-        const V3<T> dr = I.pos - ld3(pos, j) - o;
-        const T r2 = dr.x * dr.x + dr.y * dr.y + dr.z * dr.z;
-        if (r2 < r2max) {
-          if (!direct) {
-            if (cnt < cap) {
-              my[cnt * stride] = (unsigned)j | ((unsigned)oc << 27);
-              ++cnt;
-              continue;
-            }
-            for (int e = 0; e < cnt; ++e) {  // list full: flush it, then go direct
-              const unsigned ent = my[e * stride];
-              const int jj = (int)(ent & 0x7ffffffu);
-              const V3<T> oo = mulI(off_of((int)(ent >> 27)), th);
-              pair_term<Strict>(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
-            }
-            direct = true;
+        const V4<T> pj = pos[j];
+        const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
+        if (dx * dx + dy * dy + dz * dz < r2max) {
+          if (cnt == cap) {
+            ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
+            cnt = 0;
           }
-          pair_term<Strict>(P, I, dr, rec, j, A);
+          my[cnt * stride] = (unsigned)j | ((unsigned)oc << 27);
+          ++cnt;
         }
       }
     }
   }
-  if (!direct) {
-    for (int e = 0; e < cnt; ++e) {
-      const unsigned ent = my[e * stride];
-      const int jj = (int)(ent & 0x7ffffffu);
-      const V3<T> oo = mulI(off_of((int)(ent >> 27)), th);
-      pair_term<Strict>(P, I, I.pos - ld3(pos, jj) - oo, rec, jj, A);
-    }
-  }
+  ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
 }
 
 // End of cuParticleInteractionMaterial: provisional velocity, wall contact
@@ -871,7 +882,14 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX_THREADS) k_
 // sums keep the reference's order exactly.  A chunk whose tile does not fit
 // (more than IX2_SMAX particles or IX2_NZW cells in z) runs the global path.
 // ---------------------------------------------------------------------------------
-constexpr int IX2_TB = 128, IX2_SMAX = 2048, IX2_NZW = 30, IX2_CAP = 32;
+constexpr int IX2_TB = 128, IX2_SMAX = 2048, IX2_NZW = 30, IX2_CAP = 96;
+
+// Run of a staged index: boundary runs are staged before material runs, so the layer
+// is k >= base of the first material run; the column comes from the cell offset.
+RWD int ix2_seg(int k, int oc, int base9) {
+  const I3 off = off_of(oc);
+  return (k >= base9 ? 9 : 0) + (off.y + 1) * 3 + (off.x + 1);
+}
 
 struct Chunk {
   int first, n, col, pad;
@@ -882,7 +900,7 @@ template <class T> struct Ix2Smem {
   int2 tab[18][IX2_NZW];
   int delta[18];   // global index = staged index + delta
   int gbeg[18], glen[18], base[18];
-  unsigned list[IX2_CAP][IX2_TB];
+  unsigned short list[IX2_CAP][IX2_TB];  // staged index (11 bits) | cell offset << 11
   int zl, nzw, total, fallback;
 };
 
@@ -1049,7 +1067,8 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
   ix_begin<Strict>(P, S, c, i, cv, I, A);
   if (fallback) {
     // Too big for the tile: same arithmetic from global memory, list in the round buffer.
-    ix_sums_global<Strict>(P, S, c, celli, I, &sm.list[0][tid], IX2_TB, IX2_CAP, A);
+    ix_sums_global<Strict>(P, S, c, celli, I, reinterpret_cast<unsigned*>(&sm.list[0][0]) + tid, IX2_TB,
+                           IX2_CAP / 2, A);
     ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
     return;
   }
@@ -1058,74 +1077,53 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
   const T r2max = P.r2_prefilter;
   const int zi_i = cp.z - zl;
   const unsigned lanes = __activemask();
-  int rr = 0;            // next of the 54 (cell offset, layer) ranges to open
-  int k = 0, kend = 0;   // current staged range
-  unsigned tag = 0;      // layer and offset of the current range, stored with each entry
-  V3<T> pmo{T(0), T(0), T(0)};
-  bool scanning = true;
-  for (;;) {
-    // Fill: candidates of this lane, in the reference's order, until any lane's list
-    // is full or every lane has scanned all 54 ranges.
-    int cnt = 0;
-    for (;;) {
-      const bool full = cnt >= IX2_CAP;
-      if (__any_sync(lanes, full) || !__any_sync(lanes, scanning)) break;
-      if (!scanning) continue;
-      if (k >= kend) {
-        scanning = false;
-        while (rr < 54) {
-          const int oc = rr >> 1, lay = rr & 1;
-          ++rr;
-          const I3 off = off_of(oc);
-          const int zz = zi_i + off.z;
-          if (zz < 0 || zz >= nzw) continue;
-          const int s = lay * 9 + (off.y + 1) * 3 + (off.x + 1);
-          const int2 r = sm.tab[s][zz];
-          if (r.y > r.x) {
-            k = r.x;
-            kend = r.y;
-            tag = ((unsigned)oc << 16) | ((unsigned)lay << 21);
-            const V3<T> o = mulI(off, th);
-            pmo = I.pos - o;
-            scanning = true;
-            break;
-          }
-        }
-        if (!scanning) continue;
-      }
-      const V4<T> pj = sm.spos[k];
-      const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
-      if (dx * dx + dy * dy + dz * dz < r2max) {
-        sm.list[cnt][tid] = (unsigned)k | tag;
-        ++cnt;
-      }
-      ++k;
-    }
-    // Evaluate this round's entries in order, prefetching the next record.
+  unsigned short* my = &sm.list[0][tid];
+  int cnt = 0;
+  // Evaluate the listed candidates in order (next neighbour record prefetched).
+  auto flush = [&]() {
     if (cnt > 0) {
-      unsigned ent = sm.list[0][tid];
-      int kk = (int)(ent & 0xffffu);
-      int oc = (int)((ent >> 16) & 31u), lay = (int)(ent >> 21);
-      int s = lay * 9 + (off_of(oc).y + 1) * 3 + (off_of(oc).x + 1);
-      NbVals<T> nb = load_nb(rec, kk + sm.delta[s]);
+      int kk = my[0] & 0x7ff, oc = my[0] >> 11;
+      NbVals<T> nb = load_nb(rec, kk + sm.delta[ix2_seg(kk, oc, sm.base[9])]);
       for (int e = 0; e < cnt; ++e) {
         const NbVals<T> cur = nb;
         const int kc = kk, occ = oc;
         if (e + 1 < cnt) {
-          ent = sm.list[e + 1][tid];
-          kk = (int)(ent & 0xffffu);
-          oc = (int)((ent >> 16) & 31u);
-          lay = (int)(ent >> 21);
-          s = lay * 9 + (off_of(oc).y + 1) * 3 + (off_of(oc).x + 1);
-          nb = load_nb(rec, kk + sm.delta[s]);
+          const unsigned short ent = my[(e + 1) * IX2_TB];
+          kk = ent & 0x7ff;
+          oc = ent >> 11;
+          nb = load_nb(rec, kk + sm.delta[ix2_seg(kk, oc, sm.base[9])]);
         }
         const V3<T> o = mulI(off_of(occ), th);
         const V4<T> pj = sm.spos[kc];
         pair_eval<Strict>(P, I, I.pos - V3<T>{pj.x, pj.y, pj.z} - o, cur, A);
       }
     }
-    if (!__any_sync(lanes, scanning)) break;
+    cnt = 0;
+  };
+  // Phase 1 over the 54 (cell offset, layer) ranges in the reference's order; a range
+  // that could overflow any lane's list first flushes every lane's list.
+  for (int oc = 0; oc < 27; ++oc) {
+    const I3 off = off_of(oc);
+    const int zz = zi_i + off.z;
+    const bool zin = zz >= 0 && zz < nzw;
+    const V3<T> pmo = I.pos - mulI(off, th);
+#pragma unroll 1
+    for (int lay = 0; lay < 2; ++lay) {
+      int2 r{0, 0};
+      if (zin) r = sm.tab[lay * 9 + (off.y + 1) * 3 + (off.x + 1)][zz];
+      if (__any_sync(lanes, cnt + (r.y - r.x) > IX2_CAP)) flush();
+      for (int k = r.x; k < r.y; ++k) {
+        const V4<T> pj = sm.spos[k];
+        const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
+        if (dx * dx + dy * dy + dz * dz < r2max) {
+          if (cnt == IX2_CAP) flush();  // only a cell with more than IX2_CAP particles gets here
+          my[cnt * IX2_TB] = (unsigned short)(k | (oc << 11));
+          ++cnt;
+        }
+      }
+    }
   }
+  flush();
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
 
