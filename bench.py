@@ -28,6 +28,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-updates/s/GPU at 1.92M particles"
+# From the ncu capture of k_interaction on the 0.96M-particle case
+# (profiles/k_interaction_wall2_half.md): DRAM read+write 186.4 + 62.7 MB and 716.1M warp
+# instructions per launch.  Both grow with the particle count, so they are scaled per
+# soil particle to the benchmarked case.
+IX_DRAM_BYTES_PER_SOIL = (186.42e6 + 62.72e6) / 960000
+IX_WARP_INSTR_PER_SOIL = 716.09e6 / 960000
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
@@ -247,13 +253,16 @@ def run_ours(args, ws, rank, local):
     ib = interaction_bytes(inf, inf.ncell, 4)
     achieved = ib / (ix_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": "k_interaction", "achieved": achieved, "peak": pk["hbm_gbs"],
-            "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": kind, "traffic": None,
-            "algorithmic_bytes_per_launch": ib, "launch_ms": ix_ms,
-            "note": "pair arithmetic bound (FP32 issue), not HBM; see fp32 entry"}
-    flop_per_update = 2 * 27000.0  # two interaction passes per step, ~27 kFLOP each pair sweep total
+            "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": kind,
+            "traffic": IX_DRAM_BYTES_PER_SOIL * npm, "algorithmic_bytes_per_launch": ib, "launch_ms": ix_ms,
+            "note": "not HBM-bound: gather latency and pair arithmetic; see the issue entry"}
     clocks = clk.summary()
-    mhz = clocks.get("sm_mhz") or 1965.0
-    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    mhz = clocks.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
+    issue_peak = 148 * 4 * mhz * 1e6  # warp instructions per second
+    issue_ach = IX_WARP_INSTR_PER_SOIL * npm / (ix_ms * 1e-3)
+    issue = {"bound": "instruction issue", "kernel": "k_interaction", "achieved": issue_ach, "peak": issue_peak,
+             "unit": "warp-instructions/s", "frac": issue_ach / issue_peak,
+             "note": "instructions per launch from the ncu capture, scaled per soil particle"}
     line = {
         "metric": METRIC, "value": value, "unit": "particle-updates/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -263,8 +272,7 @@ def run_ours(args, ws, rank, local):
         "e2e": {"value": e2e, "unit": "particle-updates/s", "h2d_bytes_per_step": int(h2d / e2e_steps),
                 "d2h_bytes_per_step": 24, "note": "case upload from host + per-step rw_step + wall-force read"},
         "roofline": roof,
-        "roofline_fp32": {"bound": "fp32-issue", "achieved_tflops": npm * 27000.0 / (ix_ms * 1e-3) / 1e12,
-                          "peak_tflops_at_clock": fp32_peak, "flop_per_update_per_pass": 27000.0},
+        "roofline_issue": issue,
         "stage_ms": stages,
         "gpu_launches": kps * args.steps,
         "clocks": clocks,
@@ -278,6 +286,71 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def invariants(sig):
+    """p = -tr(sigma)/3 and q = sqrt(3/2 s:s) per particle (sigma: n x 6, xx yy zz xy xz yz)."""
+    import numpy as np
+
+    sig = np.asarray(sig, np.float64)
+    p = -(sig[:, 0] + sig[:, 1] + sig[:, 2]) / 3.0
+    s = sig.copy()
+    s[:, :3] += p[:, None]
+    ss = (s[:, 0] ** 2 + s[:, 1] ** 2 + s[:, 2] ** 2 + 2 * (s[:, 3] ** 2 + s[:, 4] ** 2 + s[:, 5] ** 2))
+    return p, np.sqrt(1.5 * ss)
+
+
+def precision_report(args):
+    """Precision form against FP64 runs of the same seed: the column collapse (config 1)
+    for positions and stress invariants, a retaining wall for the wall resultant."""
+    import numpy as np
+
+    from retainwall_code_b200 import LoquatSph, _abi, cases as C
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+    out = {"metric": "precision form error vs FP64", "steps": {}}
+    col = C.column_collapse()
+    wall = C.retaining_wall(nx=48, ny=24, nz=36, dx=0.0025)
+    runs = {}
+    for name, case, steps in (("column_collapse_27648", col, args.precision_steps),
+                              ("retaining_wall_41472", wall, args.precision_steps)):
+        res = {}
+        for mode in ("f64", "f32", "f32_mixed"):
+            sim = LoquatSph(case=case, precision=8 if mode == "f64" else 4)
+            if mode == "f32_mixed":
+                sim.set_option(_abi.OPT_MIXED_PRECISION, 1)
+            x0 = sim.get("pos_abs")[:, :3].astype(np.float64)
+            wf = []
+            chunk = max(1, steps // 20)
+            done = 0
+            while done < steps:
+                n = min(chunk, steps - done)
+                sim.step(n)
+                done += n
+                wf.append(sim.wall_force(0)[0])
+            sim.synchronize()
+            inf = sim.info()
+            mat = slice(inf.npb, inf.npb + inf.npm)
+            res[mode] = dict(x=sim.get("pos_abs")[:, :3].astype(np.float64)[mat], x0=x0[mat],
+                             sig=sim.get("str")[mat], wf=np.array(wf))
+            sim.close()
+        ref = res["f64"]
+        p64, q64 = invariants(ref["sig"])
+        disp = ref["x"] - ref["x0"]
+        entry = {"steps": steps}
+        for mode in ("f32", "f32_mixed"):
+            r = res[mode]
+            p, q = invariants(r["sig"])
+            entry[mode] = {"displacement_rel_l2": rel(r["x"] - r["x0"], disp),
+                           "position_max_abs_m": float(np.abs(r["x"] - ref["x"]).max()),
+                           "p_rel_l2": rel(p, p64), "q_rel_l2": rel(q, q64),
+                           "wall_force_max_rel": float(np.max(np.abs(r["wf"] - ref["wf"])) /
+                                                       max(np.abs(ref["wf"]).max(), 1e-30))}
+        entry["wall_force_f64_N"] = float(ref["wf"][-1])
+        out["steps"][name] = entry
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -289,8 +362,13 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and stage-profile passes")
     ap.add_argument("--ix-kernel", type=int, default=None, help="interaction kernel: 1 chunked (default), 0 global")
     ap.add_argument("--strict", action="store_true", help="separately rounded interaction arithmetic")
+    ap.add_argument("--precision-report", action="store_true", help="precision form vs FP64 (configs 1 and 3)")
+    ap.add_argument("--precision-steps", type=int, default=2000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.precision_report:
+        precision_report(args)
+        return
     if args.impl == "reference":  # host cores only: rank 0 runs, the other ranks exit
         ws = int(os.environ.get("WORLD_SIZE", "1"))
         run_reference(args, ws, int(os.environ.get("RANK", "0")))

@@ -133,9 +133,13 @@ enum {
   RW_OPT_INTERACTION_KERNEL = 2, /* 0 (default): one thread per particle, neighbours through L1/L2;
                                    1: column chunks with the neighbour positions staged in shared memory.
                                    Bit-identical results. */
-  RW_OPT_STRICT_FP = 3          /* interaction arithmetic: 0 (default) fused multiply-adds at fixed places;
+  RW_OPT_STRICT_FP = 3,         /* interaction arithmetic: 0 (default) fused multiply-adds at fixed places;
                                    1 every product and sum rounded separately, the written order of the
                                    reference's expressions (slower; for bit-level comparisons) */
+  RW_OPT_MIXED_PRECISION = 4    /* precision form (float contexts): 1 = compensated (Kahan) position and
+                                   velocity integration and an FP64 strain-rate norm in the hypoplastic
+                                   update; the wall resultant is always accumulated in FP64.  Set before
+                                   stepping. */
 };
 
 const char* rw_status_string(rw_status s);

@@ -10,7 +10,7 @@ RW_OK, RW_EINVAL, RW_ENOENT, RW_EIO, RW_EFORMAT, RW_ECUDA, RW_ENOMEM, RW_EDEVICE
 STATUS_NAMES = {0: "RW_OK", 1: "RW_EINVAL", 2: "RW_ENOENT", 3: "RW_EIO", 4: "RW_EFORMAT", 5: "RW_ECUDA",
                 6: "RW_ENOMEM", 7: "RW_EDEVICE", 8: "RW_ETIMEDOUT", 9: "RW_ESTATE"}
 MODEL_MAX, MATERIAL_SIZE, MOTION_MAX, TABLE_MAX = 10, 15, 10, 10
-OPT_WALL_FRICTION, OPT_COMPAT_CONTACT, OPT_INTERACTION_KERNEL, OPT_STRICT_FP = 0, 1, 2, 3
+OPT_WALL_FRICTION, OPT_COMPAT_CONTACT, OPT_INTERACTION_KERNEL, OPT_STRICT_FP, OPT_MIXED_PRECISION = 0, 1, 2, 3, 4
 
 # rw_array ids and their row shapes (columns, integer?)
 ARRAYS: Dict[str, int] = {

@@ -240,7 +240,7 @@ template <class T> RWD HypoC<T> hypo_coef(T Ei, T Vi, T phi_c, T p_ref) {
 }
 
 // cuMatModHypo (basic), src/constitutive_model.h:136-202.
-template <class T> RWD void mat_hypo_basic(T dt, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp) {
+template <class T> RWD void mat_hypo_basic(T dt, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, bool dnorm = false) {
   T Ei = mp[0], Vi = mp[1], phi_c = mp[2], coh = mp[3], p_ref = mp[4];
   HypoC<T> c = hypo_coef(Ei, Vi, phi_c, p_ref);
   F9<T> sf = sym2full(sigma);
@@ -254,7 +254,7 @@ template <class T> RWD void mat_hypo_basic(T dt, V3<T> om, S6<T> D, S6<T>& sigma
   }
   S6<T> dev = str - ident6<T>() * (T)((double)I1 / 3.0);
   T tr_str = trace(str), tr_D = trace(D), tr_sD = trace2(str, D);
-  T nD = f_sqrt(trace2(D, D));
+  T nD = rate_norm(D, dnorm);
   S6<T> rate = jau + D * (c.C1 * tr_str) + str * (c.C2 * tr_D) + str * (c.C3 * tr_sD / tr_str) + (str + dev) * (c.C4 * nD);
   str = sigma + rate * dt;
   T sph = (T)((double)trace(str) / 3.0);
@@ -273,7 +273,8 @@ template <class T> RWD void mat_hypo_basic(T dt, V3<T> om, S6<T> D, S6<T>& sigma
 }
 
 // cuMatModHypo (critical state, HypoCS), src/constitutive_model.h:209-299.
-template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, T& M_crt) {
+template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, T& M_crt,
+                                        bool dnorm = false) {
   T Ei = mp[0], Vi = mp[1], phi_c = mp[2], coh = mp[3], p_ref = mp[4], void_co = mp[5], lambda = mp[6];
   T xi = mp[7], alpha = mp[8], void_min = mp[9], void_max = mp[10], void_0 = mp[11], rho0 = mp[12];
   HypoC<T> c = hypo_coef(Ei, Vi, phi_c, p_ref);
@@ -288,7 +289,7 @@ template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T
   }
   S6<T> dev = str - ident6<T>() * (T)((double)I1 / 3.0);
   T tr_str = trace(str), tr_D = trace(D), tr_sD = trace2(str, D);
-  T nD = f_sqrt(trace2(D, D));
+  T nD = rate_norm(D, dnorm);
   T p = (T)(-(double)I1 / 3.0);
   T e = (T)((1.0 + (double)void_0) * (double)rho0 / (double)density - 1.0);
   e = f_max(e, void_min);
@@ -322,14 +323,38 @@ template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T
   sigma = dev + ident6<T>() * (sph + coh);
 }
 
+// Strain-rate norm sqrt(D:D).  The precision form evaluates it in double (the
+// survey's "hypoplastic substep norm"); otherwise the reference's scalar sqrt.
+template <class T> RWD T rate_norm(S6<T> D, bool dnorm) {
+  if (!dnorm) return f_sqrt(trace2(D, D));
+  const double d = (double)D.xx * D.xx + (double)D.yy * D.yy + (double)D.zz * D.zz +
+                   2.0 * ((double)D.xy * D.xy + (double)D.xz * D.xz + (double)D.yz * D.yz);
+  return (T)sqrt(d);
+}
+
 // Model dispatch of cuPredictorMaterial / cuCorrectorMaterial
 // (src/predictor_corrector.cu:72-75, :169-172).
 template <class T> RWD void constitutive(int model, const T* mp, T dt, T rho, V3<T> om, S6<T> D, S6<T>& sig,
-                                         bool& yld, T& M_crt) {
+                                         bool& yld, T& M_crt, bool dnorm = false) {
   if (model == RW_MODEL_DP) mat_dp(dt, om, D, sig, mp, yld);
   else if (model == RW_MODEL_MUIDP) mat_muidp(dt, om, D, sig, mp);
-  else if (model == RW_MODEL_HYPO_BASIC) mat_hypo_basic(dt, om, D, sig, mp);
-  else if (model == RW_MODEL_HYPO_CS) mat_hypo_cs(dt, rho, om, D, sig, mp, M_crt);
+  else if (model == RW_MODEL_HYPO_BASIC) mat_hypo_basic(dt, om, D, sig, mp, dnorm);
+  else if (model == RW_MODEL_HYPO_CS) mat_hypo_cs(dt, rho, om, D, sig, mp, M_crt, dnorm);
+}
+
+// Compensated (Kahan) accumulation s += x with running compensation c.  Explicit
+// round-to-nearest operations so the compensation is not optimised away.
+RWD void kahan_add(float& s, float& c, float x) {
+  const float y = __fsub_rn(x, c);
+  const float t = __fadd_rn(s, y);
+  c = __fsub_rn(__fsub_rn(t, s), y);
+  s = t;
+}
+RWD void kahan_add(double& s, double& c, double x) {
+  const double y = __dsub_rn(x, c);
+  const double t = __dadd_rn(s, y);
+  c = __dsub_rn(__dsub_rn(t, s), y);
+  s = t;
 }
 
 }  // namespace rw

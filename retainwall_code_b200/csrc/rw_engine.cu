@@ -213,6 +213,10 @@ template <class T> struct Engine final : EngineBase {
       S.stni_b[b] = dalloc<V2<T>>(np);
       S.cv[b] = dalloc<V4<T>>(np);
       S.cf[b] = dalloc<V4<T>>(np);
+      S.cmp_p[b] = dalloc<V4<T>>(np);
+      S.cmp_v[b] = dalloc<V4<T>>(np);
+      S.cmp_pi[b] = dalloc<V4<T>>(np);
+      S.cmp_vi[b] = dalloc<V4<T>>(np);
     }
     S.accad = dalloc<V4<T>>(np);
     S.spin = dalloc<V4<T>>(np);
@@ -572,6 +576,12 @@ template <class T> struct Engine final : EngineBase {
   int set_option(int opt, double v) override {
     if (opt == RW_OPT_WALL_FRICTION) {
       P.wall_fric = (T)v;
+    } else if (opt == RW_OPT_MIXED_PRECISION) {
+      if (sizeof(T) != 4 && v != 0.0) {
+        err = "the precision form applies to float contexts";
+        return RW_EINVAL;
+      }
+      P.mixed = v != 0.0 ? 1 : 0;
     } else if (opt == RW_OPT_STRICT_FP) {
       strict_fp = v != 0.0;
     } else if (opt == RW_OPT_INTERACTION_KERNEL) {

@@ -40,6 +40,12 @@ template <class T> struct DevState {
   V2<T>* stri_b[2];
   V4<T>* stni_a[2];
   V2<T>* stni_b[2];
+  // Compensation terms of the precision form (position xyz, velocity xyz+rho),
+  // permuted with the particles; *_ini copies saved by the predictor.
+  V4<T>* cmp_p[2];
+  V4<T>* cmp_v[2];
+  V4<T>* cmp_pi[2];
+  V4<T>* cmp_vi[2];
   // Stage outputs, indexed like the live buffers.
   V4<T>* accad;
   V4<T>* spin;
@@ -309,6 +315,10 @@ template <class T> __global__ void k_permute(const Params<T> P, DevState<T> S, c
   S.pos_ori[n][i] = S.pos_ori[c][j];
   S.vel[n][i] = S.vel[c][j];
   S.idm[n][i] = S.idm[c][j];
+  if (P.mixed) {
+    S.cmp_p[n][i] = S.cmp_p[c][j];
+    S.cmp_v[n][i] = S.cmp_v[c][j];
+  }
   const int npm = dyn->npm;
   const int nbm = P.npb + npm;
   const bool perm_str = (section == 0) || (npm != 0);
@@ -328,6 +338,10 @@ template <class T> __global__ void k_permute(const Params<T> P, DevState<T> S, c
     S.stri_b[ni][i] = S.stri_b[ci][ss];
     S.stni_a[ni][i] = S.stni_a[ci][ss];
     S.stni_b[ni][i] = S.stni_b[ci][ss];
+    if (P.mixed) {
+      S.cmp_pi[ni][i] = S.cmp_pi[ci][j];
+      S.cmp_vi[ni][i] = S.cmp_vi[ci][j];
+    }
   }
   (void)compat_contact;
 }
@@ -1140,6 +1154,13 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
   V4<T> vr = S.vel[c][i];
   S.pos_ini[ci][i] = ps;
   S.vel_ini[ci][i] = vr;
+  V4<T> kp{T(0), T(0), T(0), T(0)}, kv{T(0), T(0), T(0), T(0)};
+  if (P.mixed) {
+    kp = S.cmp_p[c][i];
+    kv = S.cmp_v[c][i];
+    S.cmp_pi[ci][i] = kp;
+    S.cmp_vi[ci][i] = kv;
+  }
   if (npm == 0 || i >= P.npb + npm) return;
   S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
   S6<T> sn = ld6(S.stn_a[c], S.stn_b[c], i);
@@ -1149,8 +1170,19 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
   const int4 code = S.codes[c][i];
   if (code.y != 1) return;
   const T hdt = T(0.5f) * P.dt;
-  vr = vr + S.accad[i] * hdt;
-  ps = add3(ps, xyz(vr) * hdt);
+  const V4<T> acc = S.accad[i];
+  if (P.mixed) {  // compensated half step; the compensation itself is not kept
+    kahan_add(vr.x, kv.x, acc.x * hdt);
+    kahan_add(vr.y, kv.y, acc.y * hdt);
+    kahan_add(vr.z, kv.z, acc.z * hdt);
+    kahan_add(vr.w, kv.w, acc.w * hdt);
+    kahan_add(ps.x, kp.x, vr.x * hdt);
+    kahan_add(ps.y, kp.y, vr.y * hdt);
+    kahan_add(ps.z, kp.z, vr.z * hdt);
+  } else {
+    vr = vr + acc * hdt;
+    ps = add3(ps, xyz(vr) * hdt);
+  }
   const T* mp = P.model_par[code.w];
   vr.w = f_max(vr.w, mp[kMatSize - 2]);
   vr.w = f_min(vr.w, mp[kMatSize - 1]);
@@ -1158,7 +1190,7 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
   sn = sn + D * hdt;
   bool yld = false;
   T mcrt = T(0);
-  constitutive(code.z, mp, hdt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt);
+  constitutive(code.z, mp, hdt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
   S.pos[c][i] = ps;
   S.vel[c][i] = vr;
   st6(S.stn_a[c], S.stn_b[c], i, sn);
@@ -1169,6 +1201,12 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
 // ---------------------------------------------------------------------------------
 // Corrector (src/predictor_corrector.cu:109-213): rigid walls and material.
 // ---------------------------------------------------------------------------------
+// Rounding error of s = fl(a + b): exact(a + b) - s (Knuth's TwoSum).
+template <class T> RWD T two_sum_err(T a, T b, T s) {
+  const T bb = add_rn(s, -a);
+  return add_rn(add_rn(a, -add_rn(s, -bb)), add_rn(b, -bb));
+}
+
 template <class T> RWD I3 rebin(V4<T>& ps, T th) {
   I3 dc{int(ps.x >= th) - int(ps.x < T(0)), int(ps.y >= th) - int(ps.y < T(0)), int(ps.z >= th) - int(ps.z < T(0))};
   ps = sub3(ps, mulI(dc, th));
@@ -1206,12 +1244,39 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
     return;
   }
   const V4<T> vri = S.vel_ini[ci][i];
-  V4<T> vr = vri + S.accad[i] * P.dt;
-  V4<T> ps = add3(S.pos_ini[ci][i], xyz(vr + vri) * (T(0.5f) * P.dt));
+  V4<T> vr, ps;
+  V4<T> kp{T(0), T(0), T(0), T(0)}, kv{T(0), T(0), T(0), T(0)};
+  if (P.mixed) {  // compensated full step (position and velocity keep their lost low bits)
+    kp = S.cmp_pi[ci][i];
+    kv = S.cmp_vi[ci][i];
+    const V4<T> acc = S.accad[i];
+    vr = vri;
+    kahan_add(vr.x, kv.x, acc.x * P.dt);
+    kahan_add(vr.y, kv.y, acc.y * P.dt);
+    kahan_add(vr.z, kv.z, acc.z * P.dt);
+    kahan_add(vr.w, kv.w, acc.w * P.dt);
+    ps = S.pos_ini[ci][i];
+    const T hdt = T(0.5f) * P.dt;
+    kahan_add(ps.x, kp.x, (vr.x + vri.x) * hdt);
+    kahan_add(ps.y, kp.y, (vr.y + vri.y) * hdt);
+    kahan_add(ps.z, kp.z, (vr.z + vri.z) * hdt);
+  } else {
+    vr = vri + S.accad[i] * P.dt;
+    ps = add3(S.pos_ini[ci][i], xyz(vr + vri) * (T(0.5f) * P.dt));
+  }
   const T* mp = P.model_par[code.w];
   vr.w = f_max(vr.w, mp[kMatSize - 2]);
   vr.w = f_min(vr.w, mp[kMatSize - 1]);
+  const V4<T> ps0 = ps;
   const I3 dc = rebin(ps, th);
+  if (P.mixed) {  // re-binning adds -+2h: fold its rounding error into the compensation
+    const V3<T> sh = mulI(dc, th);
+    kp.x = add_rn(kp.x, -two_sum_err(ps0.x, -sh.x, ps.x));
+    kp.y = add_rn(kp.y, -two_sum_err(ps0.y, -sh.y, ps.y));
+    kp.z = add_rn(kp.z, -two_sum_err(ps0.z, -sh.z, ps.z));
+    S.cmp_p[c][i] = kp;
+    S.cmp_v[c][i] = kv;
+  }
   int4 cp = S.cellpos[c][i];
   cp = int4{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z, cp.w};
   S6<T> sg = ld6(S.stri_a[ci], S.stri_b[ci], i);
@@ -1219,7 +1284,7 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
   const S6<T> sn = ld6(S.stni_a[ci], S.stni_b[ci], i) + D * P.dt;
   bool yld = false;
   T mcrt = T(0);
-  constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt);
+  constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
   V4<T> id = S.idm[c][i];
   if (!yld) id.x = T(100);
   id.w = mcrt;

@@ -52,6 +52,8 @@ template <class T> struct Params {
   T time_max, dt, output_frequency;
   T wall_fric;               // wall-soil Coulomb coefficient
   T r2_prefilter;            // conservative (2h)^2 bound for the candidate pre-test
+  int mixed;                 // precision form: compensated integration, FP64 strain-rate norm
+  int pad_m;
 };
 
 // Device-resident state that changes during a run.

@@ -209,3 +209,25 @@ def test_interaction_strict_bit_exact_vs_oracle(cases, name, ix_kernel):
     for key in ("accad", "acestn", "spin", "contact_var", "contact_mag"):
         a, b = s.get(key), o.get(key)
         np.testing.assert_array_equal(a, b, err_msg=key)
+
+
+def test_precision_form_runs_close_to_fp64(cases):
+    """Precision form (compensated integration, FP64 strain-rate norm): stays within
+    rounding-level distance of an FP64 run and does not drift further than plain FP32."""
+    from retainwall_code_b200 import _abi
+
+    c = cases["col_mini"]
+    sims = {}
+    for mode in ("f64", "f32", "mixed"):
+        s = LoquatSph(case=c, precision=8 if mode == "f64" else 4)
+        if mode == "mixed":
+            s.set_option(_abi.OPT_MIXED_PRECISION, 1)
+        s.step(200)
+        sims[mode] = s
+    ref = sims["f64"].get("pos_abs").astype(np.float64)
+    err32 = rel(sims["f32"].get("pos_abs"), ref)
+    errmx = rel(sims["mixed"].get("pos_abs"), ref)
+    assert errmx < 1e-6 and err32 < 1e-6
+    assert errmx <= 2.0 * err32 + 1e-9
+    for s in sims.values():
+        assert s.info().device_err == 0
