@@ -219,6 +219,23 @@ enum {
 };
 rw_status rw_profile(rw_ctx* ctx, int nsteps, double* ms_per_stage, int n_stages, int* kernels_per_step);
 
+/* Batched cases (no reference counterpart; the reference runs one case per process).
+ * Contexts on one device are advanced together: each context's whole step becomes an
+ * independent child graph of one parent graph, so one graph launch per step runs every
+ * case and the executor overlaps their kernels.  rw_batch_step is asynchronous unless
+ * ms is non-NULL (then it waits and returns the device time of the nsteps launches);
+ * call rw_batch_synchronize before reading any context.  The contexts must outlive the
+ * batch and must not be stepped individually while it is in use. */
+typedef struct rw_batch rw_batch;
+rw_status rw_batch_create(rw_ctx* const* ctxs, int n, rw_batch** out);
+rw_status rw_batch_step(rw_batch* b, int nsteps, double* ms);
+rw_status rw_batch_synchronize(rw_batch* b);
+rw_status rw_batch_destroy(rw_batch* b);
+/* Autotuner: times each interaction kernel (RW_OPT_INTERACTION_KERNEL 0 and 1) on this
+ * case for `steps` steps (plus one capture step each; the case advances) and keeps the
+ * faster; *chosen receives it. */
+rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen);
+
 /* Allocation-free cell-key sort.  No counterpart in the reference (which sorts with
  * cub::DeviceRadixSort into buffers it cudaMallocs, src/loquat_grid.cu:167-182); for
  * callers that cannot allocate device memory.  Stable sort of n cell keys (device

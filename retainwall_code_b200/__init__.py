@@ -4,5 +4,5 @@
 native library ``librw.so`` (hand-written sm_100a kernels behind the C ABI of
 include/retainwall.h).  ``cases`` builds and reads/writes the reference's case files.
 """
-from .sph import LoquatSph  # noqa: F401
+from .sph import Batch, LoquatSph  # noqa: F401
 from ._lib import RwError  # noqa: F401

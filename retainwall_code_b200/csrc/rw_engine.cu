@@ -55,6 +55,9 @@ struct EngineBase {
   virtual void set_counters(double time, int step, int npm, int np_delete_m) = 0;
   virtual void profile(int nsteps, double* ms, int n, int* kps) = 0;
   virtual double step_timed(int n) = 0;
+  virtual cudaGraph_t step_graph() = 0;
+  virtual cudaStream_t stream() const = 0;
+  virtual int soil_count() = 0;
 };
 
 static inline unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -450,29 +453,35 @@ template <class T> struct Engine final : EngineBase {
     for (int k = 0; k < n; ++k) RW_CU(cudaGraphLaunch(gexec, st));
   }
 
+  // One whole step captured as a graph (not instantiated); the caller owns it.
+  cudaGraph_t capture_step() {
+    cudaGraph_t g = nullptr;
+    const int c0 = cpar;
+    RW_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      launch_step();
+    } catch (...) {
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      cpar = c0;
+      throw;
+    }
+    RW_CU(cudaStreamEndCapture(st, &g));
+    cpar = c0;  // the step runs two interactions: parity is back where it started
+    return g;
+  }
+
   void ensure_graph() {
     if (!gexec || g_cpar != cpar) {
       if (gexec) {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
       }
-      cudaGraph_t g = nullptr;
-      const int c0 = cpar;
-      RW_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      try {
-        launch_step();
-      } catch (...) {
-        cudaStreamEndCapture(st, &g);
-        if (g) cudaGraphDestroy(g);
-        cpar = c0;
-        throw;
-      }
-      RW_CU(cudaStreamEndCapture(st, &g));
+      cudaGraph_t g = capture_step();
       cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
       cudaGraphDestroy(g);
       RW_CU(e);
-      cpar = c0;  // the step runs two interactions: parity is back where it started
-      g_cpar = c0;
+      g_cpar = cpar;
     }
   }
 
@@ -544,6 +553,10 @@ template <class T> struct Engine final : EngineBase {
     cudaEventDestroy(e1);
     return (double)ms;
   }
+
+  cudaGraph_t step_graph() override { return capture_step(); }
+  cudaStream_t stream() const override { return st; }
+  int soil_count() override { return dyn_host().npm; }
 
   int sync() override {
     RW_CU(cudaStreamSynchronize(st));
@@ -865,6 +878,44 @@ template <class T> struct Engine final : EngineBase {
   }
 };
 
+// ===================================================================================
+// Batch: many contexts on one device advanced by one graph launch per step
+// ===================================================================================
+struct Batch {
+  std::vector<EngineBase*> engines;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::string err;
+  ~Batch() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  }
+  // Parent graph with every context's step as an independent child graph: the branches
+  // have no dependencies on each other, so the executor runs them concurrently.
+  void build() {
+    cudaGraph_t parent = nullptr;
+    RW_CU(cudaGraphCreate(&parent, 0));
+    try {
+      for (EngineBase* e : engines) {
+        cudaGraph_t child = e->step_graph();
+        cudaGraphNode_t node;
+        cudaError_t rc = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+        cudaGraphDestroy(child);
+        RW_CU(rc);
+      }
+      RW_CU(cudaGraphInstantiate(&gexec, parent, 0));
+    } catch (...) {
+      cudaGraphDestroy(parent);
+      throw;
+    }
+    cudaGraphDestroy(parent);
+  }
+};
+
 }  // namespace rw
 
 // ===================================================================================
@@ -1022,6 +1073,101 @@ rw_status rw_profile(rw_ctx* ctx, int nsteps, double* ms_per_stage, int n_stages
   if (nsteps < 0 || (n_stages > 0 && !ms_per_stage)) return RW_EINVAL;
   return guarded(ctx, [&](rw::EngineBase& e) {
     e.profile(nsteps, ms_per_stage, n_stages, kernels_per_step);
+    return RW_OK;
+  });
+}
+
+struct rw_batch {
+  rw::Batch b;
+};
+
+rw_status rw_batch_create(rw_ctx* const* ctxs, int n, rw_batch** out) {
+  if (!ctxs || n <= 0 || !out) return RW_EINVAL;
+  *out = nullptr;
+  auto bt = std::make_unique<rw_batch>();
+  try {
+    for (int k = 0; k < n; ++k) {
+      if (!ctxs[k] || !ctxs[k]->eng) return RW_EINVAL;
+      if (k > 0 && ctxs[k]->eng->device != ctxs[0]->eng->device) {
+        rw::g_create_err = "all contexts of a batch must be on one device";
+        return RW_EINVAL;
+      }
+      bt->b.engines.push_back(ctxs[k]->eng.get());
+    }
+    bt->b.device = ctxs[0]->eng->device;
+    RW_CU(cudaSetDevice(bt->b.device));
+    for (auto* e : bt->b.engines) RW_CU(cudaStreamSynchronize(e->stream()));
+    RW_CU(cudaStreamCreateWithFlags(&bt->b.st, cudaStreamNonBlocking));
+    bt->b.build();
+  } catch (const Fail& f) {
+    rw::g_create_err = f.what();
+    return f.code;
+  } catch (const std::exception& e) {
+    rw::g_create_err = e.what();
+    return RW_EINVAL;
+  }
+  *out = bt.release();
+  return RW_OK;
+}
+
+rw_status rw_batch_step(rw_batch* b, int nsteps, double* ms) {
+  if (!b || nsteps < 0) return RW_EINVAL;
+  try {
+    RW_CU(cudaSetDevice(b->b.device));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+      RW_CU(cudaEventCreate(&e0));
+      RW_CU(cudaEventCreate(&e1));
+      RW_CU(cudaEventRecord(e0, b->b.st));
+    }
+    for (int k = 0; k < nsteps; ++k) RW_CU(cudaGraphLaunch(b->b.gexec, b->b.st));
+    if (ms) {
+      RW_CU(cudaEventRecord(e1, b->b.st));
+      RW_CU(cudaEventSynchronize(e1));
+      float t = 0.f;
+      RW_CU(cudaEventElapsedTime(&t, e0, e1));
+      *ms = t;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
+  } catch (const Fail& f) {
+    b->b.err = f.what();
+    return f.code;
+  }
+  return RW_OK;
+}
+
+rw_status rw_batch_synchronize(rw_batch* b) {
+  if (!b) return RW_EINVAL;
+  cudaSetDevice(b->b.device);
+  return cudaStreamSynchronize(b->b.st) == cudaSuccess ? RW_OK : RW_ECUDA;
+}
+
+rw_status rw_batch_destroy(rw_batch* b) {
+  if (!b) return RW_EINVAL;
+  cudaSetDevice(b->b.device);
+  delete b;
+  return RW_OK;
+}
+
+rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen) {
+  if (steps < 1) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) {
+    // Interaction kernel by measurement: each candidate runs one step to capture its
+    // graph and `steps` timed steps; the faster one stays selected.
+    double best = 1e300;
+    int pick = 0;
+    for (int cand = 0; cand < 2; ++cand) {
+      if (e.set_option(RW_OPT_INTERACTION_KERNEL, cand) != RW_OK) continue;
+      e.step(1);
+      const double t = e.step_timed(steps);
+      if (t < best) {
+        best = t;
+        pick = cand;
+      }
+    }
+    e.set_option(RW_OPT_INTERACTION_KERNEL, pick);
+    if (chosen) *chosen = pick;
     return RW_OK;
   });
 }

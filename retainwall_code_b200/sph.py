@@ -130,6 +130,12 @@ class LoquatSph:
         self._c(lib().rw_profile(self._h, nsteps, ms, len(STAGE_NAMES), ct.byref(kps)), "rw_profile")
         return dict(zip(STAGE_NAMES, ms[:])), kps.value
 
+    def autotune(self, steps: int = 2) -> int:
+        """Pick the faster interaction kernel for this case by timing (the case advances)."""
+        ch = ct.c_int(-1)
+        self._c(lib().rw_autotune(self._h, steps, ct.byref(ch)), "rw_autotune")
+        return ch.value
+
     # -- state ----------------------------------------------------------------------------
     def info(self) -> _abi.Info:
         inf = _abi.Info()
@@ -191,3 +197,37 @@ class LoquatSph:
             if freq > 0 and ot > freq:
                 self.save(out)
                 ot = 0.0
+
+
+class Batch:
+    """Several cases on one device advanced by one graph launch per step
+    (rw_batch_*).  The LoquatSph objects must stay alive while the batch is used."""
+
+    def __init__(self, sims):
+        self.sims = list(sims)
+        arr = (ct.c_void_p * len(self.sims))(*[s._h.value for s in self.sims])
+        h = ct.c_void_p()
+        check(lib().rw_batch_create(arr, len(self.sims), ct.byref(h)), "rw_batch_create", None)
+        self._h = h
+
+    def step(self, n: int = 1) -> None:
+        check(lib().rw_batch_step(self._h, n, None), "rw_batch_step", None)
+
+    def step_timed(self, n: int) -> float:
+        ms = ct.c_double(0.0)
+        check(lib().rw_batch_step(self._h, n, ct.byref(ms)), "rw_batch_step", None)
+        return ms.value
+
+    def synchronize(self) -> None:
+        check(lib().rw_batch_synchronize(self._h), "rw_batch_synchronize", None)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().rw_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

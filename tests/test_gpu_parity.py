@@ -231,3 +231,33 @@ def test_precision_form_runs_close_to_fp64(cases):
     assert errmx <= 2.0 * err32 + 1e-9
     for s in sims.values():
         assert s.info().device_err == 0
+
+
+def test_batch_equals_individual_runs():
+    """Cases advanced together by one graph launch per step (rw_batch_*) end in exactly
+    the states they reach when stepped alone."""
+    from retainwall_code_b200 import Batch, cases as C
+
+    specs = C.batch_sweep(n_cases=3, seed=7, n_lo=2000, n_hi=6000)
+    cs = [C.retaining_wall(nx=s["nx"], ny=s["ny"], nz=s["nz"], dx=s["dx"], phi_c=s["phi_c"], e0=s["e0"],
+                           mode=s["mode"], seed=s["seed"]) for s in specs]
+    together = [LoquatSph(case=c) for c in cs]
+    b = Batch(together)
+    b.step(6)
+    b.synchronize()
+    for c, t in zip(cs, together):
+        alone = LoquatSph(case=c)
+        alone.step(6)
+        for key in ("cellpos", "pospres", "velrhop", "str", "contact_mag"):
+            np.testing.assert_array_equal(t.get(key), alone.get(key), err_msg=key)
+        assert t.info().step == 6
+    b.close()
+
+
+def test_autotune_picks_a_kernel():
+    from retainwall_code_b200 import cases as C
+
+    s = LoquatSph(case=C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005))
+    k = s.autotune(2)
+    assert k in (0, 1)
+    assert s.info().step == 6 and s.info().device_err == 0
