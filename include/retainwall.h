@@ -120,7 +120,7 @@ typedef enum rw_array {
 typedef struct rw_info {
   int32_t np, npb, npm, np_delete_m, ncell, step, scalar_bytes, device_err;
   int32_t cell_num[3], n_motion;
-  double time, dt, h;
+  double time, dt, h, dr;
 } rw_info;
 
 typedef struct rw_ctx rw_ctx;
@@ -193,9 +193,17 @@ rw_status rw_synchronize(rw_ctx* ctx);
  *         with strip = {x_max, z_min, z_max}; strip may be NULL for the reference's values
  *         (0.04 + bound_thickness + 3 dr, bound_thickness + 0.04, bound_thickness + 1.04). */
 rw_status rw_wall_force(rw_ctx* ctx, int mode, int wall_id, const double* strip, double out_xyz[3]);
+/* Earth-pressure profile along the wall (GetValuesAlongLine, src/utilities.cu:266-367):
+ * out[4*b] = depth b*dr, out[4*b+1..3] = contact_mag.xx / dr of the last soil particle
+ * (index order, as the reference) in depth bin b of the 1st, 2nd, 3rd dr-thick band from
+ * the wall face x_wall; bins of size dz below z_top; 0 for empty bins.  NaN x_wall, z_top
+ * or dz select the reference's hard-coded values (face 0.04 + bound_thickness - 0.005 t,
+ * top 0.04 + 1.0 + bound_thickness, dz = dr). */
+rw_status rw_wall_profile(rw_ctx* ctx, double x_wall, double z_top, double dz, int nbins, double* out);
 /* Saving (src/loquat.cu:439-482) through LoquatIo::SaveXml / SaveParticles: writes
  * <outdir>/output_N.xml and N.dat (format 1) or <id>_N.vtu (format 2) with the
- * Shepard-smoothed stress, and appends "time F[kN]" to <outdir>/time_history.txt. */
+ * Shepard-smoothed stress, stress_zzN.txt (rw_wall_profile with the reference's
+ * defaults) and appends "time F[kN]" to <outdir>/time_history.txt. */
 rw_status rw_save(rw_ctx* ctx, const char* outdir);
 
 rw_status rw_get_info(rw_ctx* ctx, rw_info* out);

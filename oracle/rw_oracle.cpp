@@ -1298,6 +1298,7 @@ int orc_get_info(void* hv, rw_info* out) {
     out->time = s.time;
     out->dt = (double)s.P.dt;
     out->h = (double)s.P.h;
+    out->dr = (double)s.P.dr;
   });
   return RW_OK;
 }

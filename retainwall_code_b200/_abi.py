@@ -84,7 +84,7 @@ class Info(ct.Structure):
         ("np", ct.c_int32), ("npb", ct.c_int32), ("npm", ct.c_int32), ("np_delete_m", ct.c_int32),
         ("ncell", ct.c_int32), ("step", ct.c_int32), ("scalar_bytes", ct.c_int32), ("device_err", ct.c_int32),
         ("cell_num", ct.c_int32 * 3), ("n_motion", ct.c_int32),
-        ("time", ct.c_double), ("dt", ct.c_double), ("h", ct.c_double),
+        ("time", ct.c_double), ("dt", ct.c_double), ("h", ct.c_double), ("dr", ct.c_double),
     ]
 
 

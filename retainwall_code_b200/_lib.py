@@ -19,7 +19,7 @@ EXPORTS = [
     "rw_particle_interaction", "rw_predictor", "rw_corrector", "rw_end_step", "rw_step", "rw_synchronize",
     "rw_wall_force", "rw_save", "rw_get_info", "rw_set_option", "rw_get_array", "rw_set_array", "rw_set_counters",
     "rw_profile", "rw_step_timed", "rw_cell_sort_noalloc", "rw_batch_create", "rw_batch_step",
-    "rw_batch_synchronize", "rw_batch_destroy", "rw_autotune",
+    "rw_batch_synchronize", "rw_batch_destroy", "rw_autotune", "rw_wall_profile",
 ]
 STAGE_NAMES = ["search_p", "rigid", "adami_p", "corner_p", "interaction_p", "predictor", "search_c", "adami_c",
                "corner_c", "interaction_c", "corrector"]
@@ -60,6 +60,7 @@ def lib() -> ct.CDLL:
     L.rw_batch_synchronize.argtypes = [P]
     L.rw_batch_destroy.argtypes = [P]
     L.rw_autotune.argtypes = [P, ct.c_int, ct.POINTER(ct.c_int)]
+    L.rw_wall_profile.argtypes = [P, ct.c_double, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(ct.c_double)]
     L.rw_cell_sort_noalloc.argtypes = [ct.c_void_p, ct.c_int32, ct.c_int32, ct.c_void_p, ct.c_void_p, ct.c_void_p]
     L.rw_wall_force.argtypes = [P, ct.c_int, ct.c_int, ct.c_void_p, ct.POINTER(ct.c_double)]
     L.rw_save.argtypes = [P, ct.c_char_p]

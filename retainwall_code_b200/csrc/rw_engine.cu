@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -54,6 +55,7 @@ struct EngineBase {
   virtual int set_array(int which, const void* src, size_t bytes) = 0;
   virtual void set_counters(double time, int step, int npm, int np_delete_m) = 0;
   virtual void profile(int nsteps, double* ms, int n, int* kps) = 0;
+  virtual void wall_profile(double x_wall, double z_top, double dz, int nbins, double* out) = 0;
   virtual double step_timed(int n) = 0;
   virtual cudaGraph_t step_graph() = 0;
   virtual cudaStream_t stream() const = 0;
@@ -555,6 +557,30 @@ template <class T> struct Engine final : EngineBase {
   }
 
   cudaGraph_t step_graph() override { return capture_step(); }
+
+  // Defaults of the reference's profile (src/utilities.cu:284-292,336): wall face at
+  // 0.04 + bound_thickness - 0.005 t, top at 0.04 + 1.0 + bound_thickness, bins of dr,
+  // (int)(1/dr) bins.  NaN arguments select them.
+  void wall_profile(double x_wall, double z_top, double dz, int nbins, double* out) override {
+    Dyn<T> d = dyn_host();
+    if (x_wall != x_wall) x_wall = (double)(T(0.04f) + P.bound_thickness) - (double)d.time_f * 0.005;
+    if (z_top != z_top) z_top = (double)(T(0.04f) + T(1.0f) + P.bound_thickness);
+    if (dz != dz || dz <= 0) dz = (double)P.dr;
+    if (nbins <= 0) nbins = (int)(T(1.0f) / P.dr);
+    int* last = nullptr;
+    double* dout = nullptr;
+    RW_CU(cudaMallocAsync((void**)&last, 3 * (size_t)nbins * sizeof(int), st));
+    RW_CU(cudaMallocAsync((void**)&dout, 4 * (size_t)nbins * sizeof(double), st));
+    RW_CU(cudaMemsetAsync(last, 0xff, 3 * (size_t)nbins * sizeof(int), st));
+    const int n = P.np - P.npb;
+    if (n > 0) k_profile_claim<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn, x_wall, z_top, dz, nbins, last);
+    k_profile_read<T><<<nblk(nbins, 128), 128, 0, st>>>(P, S, cpar, nbins, last, dout);
+    check_launch();
+    RW_CU(cudaMemcpyAsync(out, dout, 4 * (size_t)nbins * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaFreeAsync(last, st));
+    RW_CU(cudaFreeAsync(dout, st));
+    RW_CU(cudaStreamSynchronize(st));
+  }
   cudaStream_t stream() const override { return st; }
   int soil_count() override { return dyn_host().npm; }
 
@@ -584,6 +610,7 @@ template <class T> struct Engine final : EngineBase {
     o->time = d.time_d;
     o->dt = (double)P.dt;
     o->h = (double)P.h;
+    o->dr = (double)P.dr;
   }
 
   int set_option(int opt, double v) override {
@@ -860,6 +887,17 @@ template <class T> struct Engine final : EngineBase {
     if (P.output_format == 1) rc = write_frame_dat(dir + "/" + std::to_string(output_number) + ".dat", f);
     else rc = write_frame_vtu(dir, output_number, f);
     if (rc) throw Fail(rc, "cannot write particle output in " + dir);
+    {  // stress_zz<N>.txt: depth, then the three bands (GetValuesAlongLine, src/utilities.cu:324-367)
+      const int nb = (int)(T(1.0f) / P.dr);
+      std::vector<double> prof(4 * (size_t)std::max(nb, 1));
+      const double nan = std::numeric_limits<double>::quiet_NaN();
+      wall_profile(nan, nan, nan, nb, prof.data());
+      std::FILE* fz = std::fopen((dir + "/stress_zz" + std::to_string(output_number) + ".txt").c_str(), "w");
+      if (!fz) throw Fail(RW_EIO, "cannot write stress_zz file");
+      for (int b = 0; b < nb; ++b)
+        std::fprintf(fz, "%.9g %.9g %.9g %.9g\n", prof[4 * b], prof[4 * b + 1], prof[4 * b + 2], prof[4 * b + 3]);
+      std::fclose(fz);
+    }
     double wf[3];
     wall_force(1, 10, nullptr, wf);
     std::FILE* th = std::fopen((dir + "/time_history.txt").c_str(), "a");
@@ -1048,6 +1086,11 @@ rw_status rw_wall_force(rw_ctx* ctx, int mode, int wall_id, const double* strip,
 
 rw_status rw_save(rw_ctx* ctx, const char* outdir) {
   return guarded(ctx, [&](rw::EngineBase& e) { e.save(outdir); return RW_OK; });
+}
+
+rw_status rw_wall_profile(rw_ctx* ctx, double x_wall, double z_top, double dz, int nbins, double* out) {
+  if (!out || nbins <= 0) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { e.wall_profile(x_wall, z_top, dz, nbins, out); return RW_OK; });
 }
 
 rw_status rw_get_info(rw_ctx* ctx, rw_info* out) {

@@ -1372,6 +1372,46 @@ template <class T> __global__ void k_shepard_store(const Params<T> P, DevState<T
 // ---------------------------------------------------------------------------------
 constexpr int WF_THREADS = 256, WF_BLOCKS = 296;
 
+// ---------------------------------------------------------------------------------
+// Earth-pressure profile along the wall (cuGetValuesAlongLine, src/utilities.cu:266-322):
+// three bands of thickness dr next to the wall, depth bins of size dz from z_top.  The
+// reference's single loop keeps, per (band, bin), the value of the last particle in
+// index order; here each particle claims its bin with atomicMax on its index and a
+// second pass reads the winners' contact_mag.xx / dr, which is the same result.
+// ---------------------------------------------------------------------------------
+template <class T> __global__ void k_profile_claim(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, double x_wall,
+                                                   double z_top, double dz, int nbins, int* last) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  // The reference loops i over [npb, np): deleted particles take part too.
+  if (t >= P.np - P.npb) return;
+  const int i = P.npb + t;
+  const int c = dyn->cur_main;
+  const V4<T> ps = S.pos[c][i];
+  const int4 cp = S.cellpos[c][i];
+  const T h2 = (T)(2.0 * (double)P.h);
+  const double px = (double)(ps.x + (T)cp.x * h2);
+  const double pz = (double)(ps.z + (T)cp.z * h2);
+  if (!(pz >= z_top - 1.0 && pz <= z_top)) return;
+  const double dr = (double)P.dr;
+  for (int band = 0; band < 3; ++band) {
+    if (px >= x_wall + dr * band && px <= x_wall + dr * (band + 1)) {
+      const int b = (int)((z_top - pz) / dz);
+      if (b >= 0 && b < nbins) atomicMax(&last[band * nbins + b], i);
+    }
+  }
+}
+
+template <class T> __global__ void k_profile_read(const Params<T> P, DevState<T> S, int cpar, int nbins,
+                                                  const int* last, double* out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbins) return;
+  out[4 * b] = (double)b * (double)P.dr;
+  for (int band = 0; band < 3; ++band) {
+    const int i = last[band * nbins + b];
+    out[4 * b + 1 + band] = i >= 0 ? (double)(S.cf[cpar][i].x / P.dr) : 0.0;
+  }
+}
+
 template <class T> __global__ void __launch_bounds__(WF_THREADS) k_wall_force(const Params<T> P, DevState<T> S,
                                                                              const Dyn<T>* dyn, int cpar, int mode,
                                                                              int wall_id, double xmax, double zmin,

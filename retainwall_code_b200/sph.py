@@ -169,6 +169,16 @@ class LoquatSph:
         self._c(lib().rw_wall_force(self._h, mode, wall_id, sp, out), "rw_wall_force")
         return np.array(out[:])
 
+    def wall_profile(self, x_wall: float = float("nan"), z_top: float = float("nan"), dz: float = float("nan"),
+                     nbins: int = 0) -> np.ndarray:
+        """Earth-pressure profile along the wall: rows (depth, band 1, band 2, band 3).
+        Defaults are the reference's: (int)(1/dr) bins of dr below its hard-coded top."""
+        if nbins <= 0:
+            nbins = max(1, int(np.float32(1.0) / np.float32(self.info().dr)))
+        out = (ct.c_double * (4 * nbins))()
+        self._c(lib().rw_wall_profile(self._h, x_wall, z_top, dz, nbins, out), "rw_wall_profile")
+        return np.array(out[:]).reshape(nbins, 4)
+
     def save(self, outdir: Optional[str] = None) -> None:
         d = outdir or self.project or "."
         self._c(lib().rw_save(self._h, d.encode()), "rw_save")

@@ -1,0 +1,89 @@
+"""Output layout (src/loquat_io.cu:315-680, src/loquat.cu:439-482, src/utilities.cu:266-367)
+through the C ABI and the `loquat` command line."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from retainwall_code_b200 import LoquatSph, cases as C
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _wall_case():
+    return C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005, wall_friction=C.REFERENCE_WALL_FRICTION, name="io")
+
+
+def test_wall_profile_matches_reference_loop_semantics():
+    """Per (band, depth bin): value of the highest-index particle in it, as the
+    reference's sequential loop leaves it."""
+    s = LoquatSph(case=_wall_case())
+    s.step(40)
+    inf = s.info()
+    dr = inf.dr
+    x_wall, z_top, nb = 0.04 + 0.015 + 1e-4, 0.04 + 0.015 + 0.07, 30
+    prof = s.wall_profile(x_wall, z_top, dr, nb)
+    pos = s.get("pos_abs").astype(np.float32)
+    cm = s.get("contact_mag")
+    exp = np.zeros((nb, 4))
+    exp[:, 0] = np.arange(nb) * np.float64(np.float32(dr))
+    for i in range(inf.npb, inf.np):
+        px, pz = float(pos[i, 0]), float(pos[i, 2])
+        if not (z_top - 1.0 <= pz <= z_top):
+            continue
+        for band in range(3):
+            if x_wall + dr * band <= px <= x_wall + dr * (band + 1):
+                b = int((z_top - pz) / dr)
+                if 0 <= b < nb:
+                    exp[b, 1 + band] = float(np.float32(cm[i, 0]) / np.float32(dr))
+    np.testing.assert_allclose(prof, exp, rtol=1e-6, atol=1e-9)
+    assert (prof[:, 1] != 0).any()
+
+
+def test_save_writes_reference_layout(tmp_path):
+    case = _wall_case()
+    s = LoquatSph(case=case)
+    s.step(5)
+    out = str(tmp_path / "out")
+    s.save(out)
+    files = set(os.listdir(out))
+    assert {"output_1.xml", "time_history.txt", "stress_zz1.txt", "0_1.vtu", "100_1.vtu"} <= files
+    p = C.read_xml(os.path.join(out, "output_1"))
+    assert p["np"] == case.np_ and p["output_number"] == 1
+    th = np.loadtxt(os.path.join(out, "time_history.txt")).reshape(-1, 2)
+    assert th.shape[0] == 1 and np.isfinite(th).all()
+    zz = np.loadtxt(os.path.join(out, "stress_zz1.txt"))
+    assert zz.shape == (int(np.float32(1.0) / np.float32(s.info().dr)), 4)
+    vtu = open(os.path.join(out, "100_1.vtu")).read()
+    assert f'NumberOfPoints="{case.npm}"' in vtu and 'Name="Stress" NumberOfComponents="6"' in vtu
+
+
+def test_save_dat_format_roundtrips(tmp_path):
+    case = _wall_case()
+    case.params["output_format"] = 1
+    s = LoquatSph(case=case)
+    s.step(3)
+    out = str(tmp_path / "o")
+    s.save(out)
+    rows = open(os.path.join(out, "1.dat")).read().strip().split("\n")
+    assert len(rows) == case.np_
+    assert len(rows[0].split()) == 31 and len(rows[-1].split()) == 27
+    pos = np.array([list(map(float, r.split()[4:7])) for r in rows])
+    np.testing.assert_allclose(pos, s.get("pos_abs")[:, :3], rtol=1e-6, atol=1e-9)
+
+
+def test_cli_runs_project(tmp_path):
+    exe = os.path.join(ROOT, "retainwall_code_b200", "loquat")
+    case = _wall_case()
+    case.params["output_frequency"] = 2e-4
+    proj = str(tmp_path / "wall")
+    C.write_case(case, proj)
+    env = dict(os.environ, RW_TIME_MAX="5e-4")
+    r = subprocess.run([exe, proj, "0"], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, r.stderr
+    files = os.listdir(proj)
+    assert "output_0.xml" not in files and "output_1.xml" in files and "time_history.txt" in files
+    th = np.loadtxt(os.path.join(proj, "time_history.txt")).reshape(-1, 2)
+    assert th.shape[0] >= 2
