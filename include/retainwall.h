@@ -200,7 +200,9 @@ rw_status rw_wall_force(rw_ctx* ctx, int mode, int wall_id, const double* strip,
  * or dz select the reference's hard-coded values (face 0.04 + bound_thickness - 0.005 t,
  * top 0.04 + 1.0 + bound_thickness, dz = dr). */
 rw_status rw_wall_profile(rw_ctx* ctx, double x_wall, double z_top, double dz, int nbins, double* out);
-/* Saving (src/loquat.cu:439-482) through LoquatIo::SaveXml / SaveParticles: writes
+/* The first call writes the initial configuration as RunSimulation does (output number
+ * of the case, particles and parameters only, src/loquat.cu:533-537); later calls are
+ * Saving (src/loquat.cu:439-482) through LoquatIo::SaveXml / SaveParticles: writes
  * <outdir>/output_N.xml and N.dat (format 1) or <id>_N.vtu (format 2) with the
  * Shepard-smoothed stress, stress_zzN.txt (rw_wall_profile with the reference's
  * defaults) and appends "time F[kN]" to <outdir>/time_history.txt. */

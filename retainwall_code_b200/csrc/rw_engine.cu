@@ -79,6 +79,7 @@ template <class T> struct Engine final : EngineBase {
   int ncol = 0, max_chunks = 0;
   rw_case_params cparams{};
   int output_number = 0;
+  int saves = 0;  // the first save is RunSimulation's initial output
 
   ~Engine() override {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -880,13 +881,17 @@ template <class T> struct Engine final : EngineBase {
     f.str.assign(h6.begin(), h6.end());
     if (get_array(RW_ARR_STN, h6.data(), h6.size() * sizeof(T))) throw Fail(RW_ECUDA, "save: stn");
     f.stn.assign(h6.begin(), h6.end());
-    output_number++;
+    // RunSimulation writes the initial configuration with the case's output number
+    // (src/loquat.cu:533-537); every later Saving increments first (src/loquat.cu:456).
+    const bool initial = saves++ == 0;
+    if (!initial) output_number++;
     const std::string xmlp = dir + "/output_" + std::to_string(output_number) + ".xml";
     int rc = write_output_xml(xmlp, cparams, P.np, P.npb, d.npm, d.time_d, (double)P.dt, output_number);
     if (rc) throw Fail(rc, "cannot write " + xmlp);
     if (P.output_format == 1) rc = write_frame_dat(dir + "/" + std::to_string(output_number) + ".dat", f);
     else rc = write_frame_vtu(dir, output_number, f);
     if (rc) throw Fail(rc, "cannot write particle output in " + dir);
+    if (initial) return;
     {  // stress_zz<N>.txt: depth, then the three bands (GetValuesAlongLine, src/utilities.cu:324-367)
       const int nb = (int)(T(1.0f) / P.dr);
       std::vector<double> prof(4 * (size_t)std::max(nb, 1));

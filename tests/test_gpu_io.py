@@ -45,12 +45,14 @@ def test_wall_profile_matches_reference_loop_semantics():
 def test_save_writes_reference_layout(tmp_path):
     case = _wall_case()
     s = LoquatSph(case=case)
-    s.step(5)
     out = str(tmp_path / "out")
+    s.save(out)  # initial configuration: output_0, particles only
+    assert set(os.listdir(out)) == {"output_0.xml", "0_0.vtu", "100_0.vtu"}
+    s.step(5)
     s.save(out)
     files = set(os.listdir(out))
     assert {"output_1.xml", "time_history.txt", "stress_zz1.txt", "0_1.vtu", "100_1.vtu"} <= files
-    p = C.read_xml(os.path.join(out, "output_1"))
+    p = C.read_xml(os.path.join(out, "output_1.xml"))
     assert p["np"] == case.np_ and p["output_number"] == 1
     th = np.loadtxt(os.path.join(out, "time_history.txt")).reshape(-1, 2)
     assert th.shape[0] == 1 and np.isfinite(th).all()
@@ -64,8 +66,9 @@ def test_save_dat_format_roundtrips(tmp_path):
     case = _wall_case()
     case.params["output_format"] = 1
     s = LoquatSph(case=case)
-    s.step(3)
     out = str(tmp_path / "o")
+    s.save(out)
+    s.step(3)
     s.save(out)
     rows = open(os.path.join(out, "1.dat")).read().strip().split("\n")
     assert len(rows) == case.np_
@@ -84,6 +87,6 @@ def test_cli_runs_project(tmp_path):
     r = subprocess.run([exe, proj, "0"], capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0, r.stderr
     files = os.listdir(proj)
-    assert "output_0.xml" not in files and "output_1.xml" in files and "time_history.txt" in files
+    assert "output_0.xml" in files and "output_1.xml" in files and "time_history.txt" in files
     th = np.loadtxt(os.path.join(proj, "time_history.txt")).reshape(-1, 2)
     assert th.shape[0] >= 2
