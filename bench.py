@@ -332,6 +332,15 @@ def run_ours(args, ws, rank, local):
             "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": kind,
             "traffic": IX_DRAM_BYTES_PER_SOIL * npm, "algorithmic_bytes_per_launch": ib, "launch_ms": ix_ms,
             "note": "not HBM-bound: gather latency and pair arithmetic; see the issue entry"}
+    # whole step against the compulsory traffic of the algorithm: FP32 compact state of
+    # 104 B per soil particle moved through two sections (bin, sort, permute, contact
+    # preparation, interaction + integration) = 1276 B per soil particle, 644 B per
+    # boundary particle and 32 B per cell per step
+    b_alg = 1276 * npm + 644 * inf.npb + 32 * inf.ncell
+    step_ach = b_alg / (ms / args.steps * 1e-3) / 1e9
+    roof_step = {"bound": "hbm", "achieved": step_ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                 "frac": step_ach / pk["hbm_gbs"], "peak_source": kind, "algorithmic_bytes_per_step": b_alg,
+                 "note": "1276 B/soil + 644 B/boundary + 32 B/cell per step; FP32 issue is the tighter bound"}
     clocks = clk.summary()
     mhz = clocks.get("sm_mhz") or pk.get("sm_max_mhz", 1965.0)
     issue_peak = 148 * 4 * mhz * 1e6  # warp instructions per second
@@ -349,6 +358,7 @@ def run_ours(args, ws, rank, local):
                 "d2h_bytes_per_step": 24, "note": "case upload from host + per-step rw_step + wall-force read"},
         "roofline": roof,
         "roofline_issue": issue,
+        "roofline_step": roof_step,
         "stage_ms": stages,
         "gpu_launches": kps * args.steps,
         "clocks": clocks,

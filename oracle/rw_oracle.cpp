@@ -379,6 +379,8 @@ template <class T> struct Sim {
     return c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < P.cell_num.x && c.y < P.cell_num.y && c.z < P.cell_num.z;
   }
   T two_h() const { return (T)(2.0 * (double)P.h); }
+  bool period_image(I3 celli, V3<T> pos_i, bool abs_len, I3& cpb, V3<T>& ppb) const;
+  void period_wrap(I4& cp, V4<T>& ps) const;
 
   void init(const rw_case* cs);
   void neighbor_search(int section);
@@ -677,6 +679,49 @@ template <class T> void Sim<T>::rigid_body_update() {
         if (I3 off{cx, cy, cz}, cj{celli.x + cx, celli.y + cy, celli.z + cz}; !in_grid(cj)) { \
         } else
 
+// Periodic planes.  Dist2Plane / AbsDist2Plane (src/functions.h:134-139).
+template <class T> inline T plane_eval(V3<T> a, const V4<T>& pl) { return a.x * pl.x + a.y * pl.y + a.z * pl.z + pl.w; }
+template <class T> inline T plane_norm(const V4<T>& pl) { return std::sqrt(pl.x * pl.x + pl.y * pl.y + pl.z * pl.z); }
+
+// Periodic image of a particle within 2h of a periodic plane: its absolute position
+// moved by one period along that plane's normal, as a cell and an in-cell position
+// (the *LoopPeriod helpers: src/adami_boundary.cu:73-88, src/field_smoothing.cu:58-72,
+// src/particle_interaction.cu:243-257).  The period is |D_left + D_right| in the Adami
+// and Shepard loops (abs_len) and the signed sum in the interaction.
+template <class T> bool Sim<T>::period_image(I3 celli, V3<T> pos_i, bool abs_len, I3& cpb, V3<T>& ppb) const {
+  const T th = T(2.0f) * P.h;
+  const V3<T> pabs = pos_i + mulI(celli, th);
+  const bool left = std::fabs(plane_eval(pabs, P.planeleft)) / plane_norm(P.planeleft) < th;
+  const bool right = std::fabs(plane_eval(pabs, P.planeright)) / plane_norm(P.planeright) < th;
+  if (!left && !right) return false;
+  T len = P.planeleft.w + P.planeright.w;
+  if (abs_len) len = std::fabs(len);
+  const V4<T>& pl = left ? P.planeleft : P.planeright;
+  const V3<T> pb{pabs.x + pl.x * len, pabs.y + pl.y * len, pabs.z + pl.z * len};
+  const T s = T(0.5f) * P.i_h;
+  cpb = I3{int(pb.x * s), int(pb.y * s), int(pb.z * s)};
+  ppb = pb - mulI(cpb, th);
+  return true;
+}
+
+// A particle that left through a periodic plane re-enters through the other one
+// (cuCheckOutDomainPeriod, src/predictor_corrector.cu:26-40).
+template <class T> void Sim<T>::period_wrap(I4& cp, V4<T>& ps) const {
+  const T th = T(2.0f) * P.h;
+  const V3<T> pabs = xyz(ps) + mulI(I3{cp.x, cp.y, cp.z}, th);
+  const bool left = plane_eval(pabs, P.planeleft) / plane_norm(P.planeleft) < T(0.0);
+  const bool right = plane_eval(pabs, P.planeright) / plane_norm(P.planeright) < T(0.0);
+  if (!left && !right) return;
+  const T len = std::fabs(P.planeleft.w + P.planeright.w);
+  const V4<T>& pl = left ? P.planeleft : P.planeright;
+  const V3<T> pb{pabs.x + pl.x * len, pabs.y + pl.y * len, pabs.z + pl.z * len};
+  const T s = T(0.5f) * P.i_h;
+  const I3 c{int(pb.x * s), int(pb.y * s), int(pb.z * s)};
+  const V3<T> pr = pb - mulI(c, th);
+  cp = I4{c.x, c.y, c.z, cp.w};
+  ps = V4<T>{pr.x, pr.y, pr.z, ps.w};
+}
+
 // cuAdamiBoundaryMaterial (src/adami_boundary.cu:26-158).
 template <class T> void Sim<T>::adami() {
   Par<T>& p = P;
@@ -689,13 +734,14 @@ template <class T> void Sim<T>::adami() {
     I3 celli{cellpos[i].x, cellpos[i].y, cellpos[i].z};
     V3<T> n_i{T(0), T(0), T(0)};
     bool contact = codes[i].x >= 10;
-    ORC_FOR_NEIGHBOUR_CELLS(celli) {
+    auto scan = [&](I3 cc, V3<T> pp) {
+     ORC_FOR_NEIGHBOUR_CELLS(cc) {
       int k = key_of(cj);
       for (int pass = 0; pass < 2; ++pass) {
         bool bound = pass == 0;
         int kk = bound ? k : k + p.ncell_material;
         for (int j = cell_beg[kk]; j < cell_end[kk]; ++j) {
-          V3<T> dr = pos_i - xyz(pospres[j]);
+          V3<T> dr = pp - xyz(pospres[j]);
           dr = dr - mulI(off, th);
           T r = dist(dr);
           T q = r * p.i_h;
@@ -713,7 +759,12 @@ template <class T> void Sim<T>::adami() {
           }
         }
       }
-    }
+     }
+    };
+    scan(celli, pos_i);
+    I3 cpb;
+    V3<T> ppb;
+    if (p.periodbound && period_image(celli, pos_i, true, cpb, ppb)) scan(cpb, ppb);
     if (enorm(n_i) > T(0)) {
       cmag[i].yx = n_i.x / enorm(n_i);
       cmag[i].yy = n_i.y / enorm(n_i);
@@ -807,7 +858,7 @@ template <class T> void Sim<T>::find_corner() {
   });
 }
 
-// cuStressRegularizationShepard (src/field_smoothing.cu:239-325).
+// cuStressRegularizationShepard (src/field_smoothing.cu:26-111).
 template <class T> void Sim<T>::shepard(bool for_saving) {
   Par<T>& p = P;
   if (p.npm == 0) return;
@@ -819,20 +870,26 @@ template <class T> void Sim<T>::shepard(bool for_saving) {
     I3 celli{cellpos[i].x, cellpos[i].y, cellpos[i].z};
     S6<T> sh{T(0), T(0), T(0), T(0), T(0), T(0)};
     T sumker = T(0.0f);
-    ORC_FOR_NEIGHBOUR_CELLS(celli) {
-      int k = key_of(cj) + p.ncell_material;
-      for (int j = cell_beg[k]; j < cell_end[k]; ++j) {
-        V3<T> dr = pos_i - xyz(pospres[j]) - mulI(off, th);
-        T r = dist(dr);
-        T q = r * p.i_h;
-        if (q < T(2.0f)) {
-          T ker = kernel_w(p.knorm, q);
-          T vol = idm[j].y / velrhop[j].w;
-          sumker += ker * vol;
-          sh = sh + str[j] * (ker * vol);
+    auto scan = [&](I3 cc, V3<T> pp) {
+      ORC_FOR_NEIGHBOUR_CELLS(cc) {
+        int k = key_of(cj) + p.ncell_material;
+        for (int j = cell_beg[k]; j < cell_end[k]; ++j) {
+          V3<T> dr = pp - xyz(pospres[j]) - mulI(off, th);
+          T r = dist(dr);
+          T q = r * p.i_h;
+          if (q < T(2.0f)) {
+            T ker = kernel_w(p.knorm, q);
+            T vol = idm[j].y / velrhop[j].w;
+            sumker += ker * vol;
+            sh = sh + str[j] * (ker * vol);
+          }
         }
       }
-    }
+    };
+    scan(celli, pos_i);
+    I3 cpb;
+    V3<T> ppb;
+    if (p.periodbound && period_image(celli, pos_i, true, cpb, ppb)) scan(cpb, ppb);
     if (sumker != T(0.f)) sh = sh / sumker;
     tcache[i] = sh;
   });
@@ -859,13 +916,14 @@ template <class T> void Sim<T>::interaction() {
     int shift_i = (int)cvar0[i].z;
     T rho_i = vr_i.w;
     V3<T> vel_i = xyz(vr_i);
-    ORC_FOR_NEIGHBOUR_CELLS(celli) {
+    auto scan = [&](I3 cc, V3<T> pp) {
+     ORC_FOR_NEIGHBOUR_CELLS(cc) {
       int k = key_of(cj);
       for (int pass = 0; pass < 2; ++pass) {
         bool bound = pass == 0;
         int kk = bound ? k : k + p.ncell_material;
         for (int j = cell_beg[kk]; j < cell_end[kk]; ++j) {
-          V3<T> dr = pos_i - xyz(pospres[j]) - mulI(off, th);
+          V3<T> dr = pp - xyz(pospres[j]) - mulI(off, th);
           T r = dist(dr);
           T q = r * p.i_h;
           if (!(q < T(2.0f))) continue;
@@ -909,6 +967,13 @@ template <class T> void Sim<T>::interaction() {
           }
         }
       }
+     }
+    };
+    scan(celli, pos_i);
+    {
+      I3 cpb;
+      V3<T> ppb;
+      if (p.periodbound && period_image(celli, pos_i, false, cpb, ppb)) scan(cpb, ppb);
     }
     V3<T> acc_damp = vel_i * p.damping;
     V4<T> acc1 = v4(acc_s + acc_av + acc_as - acc_damp + p.gravity, accden);
@@ -1057,6 +1122,7 @@ template <class T> void Sim<T>::corrector() {
           int(pospres[i].z >= th) - int(pospres[i].z < T(0))};
     pospres[i] = sub3(pospres[i], mulI(dc, th));
     cellpos[i] = {cellpos[i].x + dc.x, cellpos[i].y + dc.y, cellpos[i].z + dc.z, cellpos[i].w};
+    if (p.periodbound) period_wrap(cellpos[i], pospres[i]);
     S6<T> sigma = str_ini[i];
     S6<T> dstn = acestn[i] * p.dt;
     stn[i] = stn_ini[i] + dstn;

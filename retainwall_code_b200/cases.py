@@ -276,7 +276,7 @@ def column_collapse(nx=24, ny=24, nz=48, dx=0.005, seed=1, phi_c=30.0, e0=0.70, 
 
 def retaining_wall(nx=200, ny=80, nz=120, dx=0.0025, seed=2, phi_c=30.0, e0=0.65, rho0=1850.0, hdr=1.2,
                    jitter=0.05, cs=60.0, cfl=0.1, mode="active", wall_speed=1.0e-3, rot_speed=0.005,
-                   wall_friction: Optional[float] = None, name="wall") -> Case:
+                   wall_friction: Optional[float] = None, periodic_y: bool = False, name="wall") -> Case:
     """Rigid retaining wall against hypoplastic sand.
 
     The soil block starts at x = 0.04 + bt, z = 0.04 + bt, the placement of the
@@ -287,6 +287,9 @@ def retaining_wall(nx=200, ny=80, nz=120, dx=0.0025, seed=2, phi_c=30.0, e0=0.65
     ``mode``: ``active`` (wall moves -x at wall_speed), ``passive`` (+x), or
     ``rotation`` (about the toe, top moving away from the soil at rot_speed rad/s).
     Wall friction defaults to delta = 2/3 phi_c (mu = tan delta).
+    ``periodic_y``: no y side walls; the planes y = y0 and y = y0 + W are periodic
+    (``period-bound``, planeleft = (0, 1, 0, -y0), planeright = (0, -1, 0, y0 + W)), and
+    the floor and both x walls span exactly one period in y.
     """
     rng = np.random.default_rng(seed)
     h = dx * hdr
@@ -297,11 +300,17 @@ def retaining_wall(nx=200, ny=80, nz=120, dx=0.0025, seed=2, phi_c=30.0, e0=0.65
     model = hypocs_model(phi_c, e0, rho0)
     p = _base_params(dx, hdr, cs, cfl, rho0, model)
     b = _Builder()
-    b.box((x0 - bt, y0 - bt, z0 - bt), (x0 + L + bt, y0 + W + bt, z0), dx, (0, FIX, INT_MIN, INT_MIN), (0, 0, 1, -1))
-    b.box((x0, y0 - bt, z0), (x0 + L, y0, top), dx, (2, FIX, INT_MIN, INT_MIN), (0, 1, 0, 1))
-    b.box((x0, y0 + W, z0), (x0 + L, y0 + W + bt, top), dx, (3, FIX, INT_MIN, INT_MIN), (0, -1, 0, 1))
-    b.box((x0 + L, y0 - bt, z0), (x0 + L + bt, y0 + W + bt, top), dx, (4, FIX, INT_MIN, INT_MIN), (-1, 0, 0, 1))
-    b.box((x0 - bt, y0 - bt, z0), (x0, y0 + W + bt, top), dx, (10, NONFIX, INT_MIN, 0), (1, 0, 0, 1))
+    yb = 0.0 if periodic_y else bt  # y extent of the floor and x walls beyond the soil
+    b.box((x0 - bt, y0 - yb, z0 - bt), (x0 + L + bt, y0 + W + yb, z0), dx, (0, FIX, INT_MIN, INT_MIN), (0, 0, 1, -1))
+    if not periodic_y:
+        b.box((x0, y0 - bt, z0), (x0 + L, y0, top), dx, (2, FIX, INT_MIN, INT_MIN), (0, 1, 0, 1))
+        b.box((x0, y0 + W, z0), (x0 + L, y0 + W + bt, top), dx, (3, FIX, INT_MIN, INT_MIN), (0, -1, 0, 1))
+    b.box((x0 + L, y0 - yb, z0), (x0 + L + bt, y0 + W + yb, top), dx, (4, FIX, INT_MIN, INT_MIN), (-1, 0, 0, 1))
+    b.box((x0 - bt, y0 - yb, z0), (x0, y0 + W + yb, top), dx, (10, NONFIX, INT_MIN, 0), (1, 0, 0, 1))
+    if periodic_y:
+        p["periodbound"] = 1
+        p["planeleft"] = [0.0, 1.0, 0.0, -f32(y0)]
+        p["planeright"] = [0.0, -1.0, 0.0, f32(y0 + W)]
     K0 = 1.0 - math.sin(math.radians(phi_c))
     _soil(b, x0, y0, z0, nx, ny, nz, dx, rng, jitter, rho0, -9.81, K0)
     margin = 0.04

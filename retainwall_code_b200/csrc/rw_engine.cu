@@ -126,7 +126,12 @@ template <class T> struct Engine final : EngineBase {
     cparams = q;
     output_number = q.output_number;
     if (q.dim != 3) throw Fail(RW_EINVAL, "only 3D cases are supported (dimension-of-problem must be 3)");
-    if (q.periodbound) throw Fail(RW_EINVAL, "periodic boundaries are not supported");
+    if (q.periodbound) {
+      const double nl = q.planeleft[0] * q.planeleft[0] + q.planeleft[1] * q.planeleft[1] + q.planeleft[2] * q.planeleft[2];
+      const double nr = q.planeright[0] * q.planeright[0] + q.planeright[1] * q.planeright[1] +
+                        q.planeright[2] * q.planeright[2];
+      if (!(nl > 0.0) || !(nr > 0.0)) throw Fail(RW_EINVAL, "periodic plane with a zero normal");
+    }
     if (q.np != q.npb + q.npm || q.np <= 0 || q.npb < 0 || q.npm < 0)
       throw Fail(RW_EINVAL, "Error! Wrong number of particles ...");
     if (q.np >= (1 << 27)) throw Fail(RW_EINVAL, "more than 2^27 particles");
@@ -143,7 +148,7 @@ template <class T> struct Engine final : EngineBase {
       }
     }
     P.dim = q.dim;
-    P.periodbound = 0;
+    P.periodbound = q.periodbound ? 1 : 0;
     P.n_motion = q.n_motion;
     P.n_model = q.n_model;
     P.np = q.np;

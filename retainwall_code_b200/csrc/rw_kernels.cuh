@@ -403,6 +403,63 @@ template <class T> __global__ void k_end(const Params<T> P, Dyn<T>* dyn) {
 }
 
 // ---------------------------------------------------------------------------------
+// Periodic planes (period-bound cases).  Dist2Plane / AbsDist2Plane
+// (src/functions.h:134-139); every operation separately rounded, so the decisions and
+// the image coordinates match the oracle bit for bit.
+// ---------------------------------------------------------------------------------
+template <class T> RWD T plane_dist(const T* pl, const V3<T> a) {
+  using F = Fp<true>;
+  const T num = F::mad(a.z, pl[2], F::mad(a.y, pl[1], F::mul(a.x, pl[0]))) + pl[3];
+  return num / pair_r(pair_r2(pl[0], pl[1], pl[2]));
+}
+
+template <class T> RWD V3<T> abs_pos(const V3<T> p, const I3 c, T th) {
+  using F = Fp<true>;
+  return V3<T>{F::mad((T)c.x, th, p.x), F::mad((T)c.y, th, p.y), F::mad((T)c.z, th, p.z)};
+}
+
+// Absolute position pabs moved by one period along the plane pl, as a cell and an
+// in-cell position.
+template <class T> RWD void period_shift(const Params<T>& P, const V3<T> pabs, const T* pl, T len, I3& cpb,
+                                         V3<T>& ppb) {
+  using F = Fp<true>;
+  const V3<T> pb{F::mad(pl[0], len, pabs.x), F::mad(pl[1], len, pabs.y), F::mad(pl[2], len, pabs.z)};
+  const T s = F::mul(T(0.5f), P.i_h);
+  cpb = I3{int(F::mul(pb.x, s)), int(F::mul(pb.y, s)), int(F::mul(pb.z, s))};
+  ppb = V3<T>{F::msub((T)cpb.x, P.two_h, pb.x), F::msub((T)cpb.y, P.two_h, pb.y), F::msub((T)cpb.z, P.two_h, pb.z)};
+}
+
+// Periodic image of a particle within 2h of a periodic plane (the *LoopPeriod helpers:
+// src/adami_boundary.cu:73-88, src/field_smoothing.cu:58-72,
+// src/particle_interaction.cu:243-257).  The period is |D_left + D_right| in the Adami
+// and Shepard loops (abs_len) and the signed sum in the interaction.
+template <class T> RWD bool period_image(const Params<T>& P, const I3 celli, const V3<T> pos_i, bool abs_len,
+                                         I3& cpb, V3<T>& ppb) {
+  const V3<T> pabs = abs_pos(pos_i, celli, P.two_h);
+  const bool left = f_abs(plane_dist(P.planeleft, pabs)) < P.two_h;
+  const bool right = f_abs(plane_dist(P.planeright, pabs)) < P.two_h;
+  if (!left && !right) return false;
+  T len = P.planeleft[3] + P.planeright[3];
+  if (abs_len) len = f_abs(len);
+  period_shift(P, pabs, left ? P.planeleft : P.planeright, len, cpb, ppb);
+  return true;
+}
+
+// A particle that left through a periodic plane re-enters through the other one
+// (cuCheckOutDomainPeriod, src/predictor_corrector.cu:26-40).
+template <class T> RWD void period_wrap(const Params<T>& P, int4& cp, V4<T>& ps) {
+  const V3<T> pabs = abs_pos(xyz(ps), I3{cp.x, cp.y, cp.z}, P.two_h);
+  const bool left = plane_dist(P.planeleft, pabs) < T(0.0);
+  const bool right = plane_dist(P.planeright, pabs) < T(0.0);
+  if (!left && !right) return;
+  I3 c;
+  V3<T> pr;
+  period_shift(P, pabs, left ? P.planeleft : P.planeright, f_abs(P.planeleft[3] + P.planeright[3]), c, pr);
+  cp = int4{c.x, c.y, c.z, cp.w};
+  ps = V4<T>{pr.x, pr.y, pr.z, ps.w};
+}
+
+// ---------------------------------------------------------------------------------
 // Adami boundary (src/adami_boundary.cu:26-158).
 // ---------------------------------------------------------------------------------
 template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
@@ -423,16 +480,17 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
   V4<T> rps{T(0), T(0), T(0), T(0)}, rvr{T(0), T(0), T(0), T(0)};
   V3<T> n_i{T(0), T(0), T(0)};
   const T th = P.two_h;
+  auto scan = [&](const I3 cc, const V3<T> pp) {
   for (int oc = 0; oc < 27; ++oc) {
     const I3 off = off_of(oc);
-    const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+    const I3 cj{cc.x + off.x, cc.y + off.y, cc.z + off.z};
     if (!in_grid(P, cj)) continue;
     const int k = key_of(P, cj);
     const V3<T> o = mulI(off, th);
     if (contact) {
       const int2 rg = S.range[k];
       for (int j = rg.x; j < rg.y; ++j) {
-        V3<T> dr = pos_i - ld3(pos, j);
+        V3<T> dr = pp - ld3(pos, j);
         dr = dr - o;
         T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
         T q = r * P.i_h;
@@ -445,7 +503,7 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
     }
     const int2 rg = S.range[k + P.ncell_material];
     for (int j = rg.x; j < rg.y; ++j) {
-      V3<T> dr = pos_i - ld3(pos, j);
+      V3<T> dr = pp - ld3(pos, j);
       dr = dr - o;
       T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
       T q = r * P.i_h;
@@ -460,6 +518,13 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
         rvr = rvr + vj * kv;
       }
     }
+  }
+  };
+  scan(celli, pos_i);
+  if (P.periodbound) {
+    I3 cpb;
+    V3<T> ppb;
+    if (period_image(P, celli, pos_i, true, cpb, ppb)) scan(cpb, ppb);
   }
   if (enorm(n_i) > T(0)) {
     T nn = enorm(n_i);
@@ -769,6 +834,36 @@ template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, cons
   ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
 }
 
+// Second pass of a particle within 2h of a periodic plane, over the neighbours of its
+// periodic image (cuParticleInteractionMaterialLoopPeriod,
+// src/particle_interaction.cu:243-257): same order, evaluated directly (few particles).
+template <bool Strict, class T> RWD void ix_period(const Params<T>& P, const DevState<T>& S, int c, int i,
+                                                   const I3 celli, IState<T>& I, Acc<T>& A) {
+  I3 cpb;
+  V3<T> ppb;
+  if (!period_image(P, celli, I.pos, false, cpb, ppb)) return;
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const V3<T> keep = I.pos;
+  I.pos = ppb;
+  for (int oc = 0; oc < 27; ++oc) {
+    const I3 off = off_of(oc);
+    const I3 cj{cpb.x + off.x, cpb.y + off.y, cpb.z + off.z};
+    if (!in_grid(P, cj)) continue;
+    const int k = key_of(P, cj);
+    const V3<T> o = mulI(off, P.two_h);
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      const int2 rg = S.range[pass ? k + P.ncell_material : k];
+#pragma unroll 1
+      for (int j = rg.x; j < rg.y; ++j) {
+        const V4<T> pj = pos[j];
+        pair_term<Strict>(P, I, I.pos - V3<T>{pj.x, pj.y, pj.z} - o, S.rec, j, A);
+      }
+    }
+  }
+  I.pos = keep;
+}
+
 // End of cuParticleInteractionMaterial: provisional velocity, wall contact
 // (cuParticleInteractionMaterialLoopContact, src/particle_interaction.cu:142-241) and
 // the stage outputs (src/particle_interaction.cu:284-295).
@@ -880,6 +975,7 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX_THREADS) k_
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
   ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A);
+  if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
 
@@ -1083,6 +1179,7 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
     // Too big for the tile: same arithmetic from global memory, list in the round buffer.
     ix_sums_global<Strict>(P, S, c, celli, I, reinterpret_cast<unsigned*>(&sm.list[0][0]) + tid, IX2_TB,
                            IX2_CAP / 2, A);
+    if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
     ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
     return;
   }
@@ -1138,6 +1235,7 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
     }
   }
   flush();
+  if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
 
@@ -1279,6 +1377,7 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
   }
   int4 cp = S.cellpos[c][i];
   cp = int4{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z, cp.w};
+  if (P.periodbound) period_wrap(P, cp, ps);
   S6<T> sg = ld6(S.stri_a[ci], S.stri_b[ci], i);
   const S6<T> D = ld6(S.ace_a, S.ace_b, i);
   const S6<T> sn = ld6(S.stni_a[ci], S.stni_b[ci], i) + D * P.dt;
@@ -1306,7 +1405,7 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
 }
 
 // ---------------------------------------------------------------------------------
-// Shepard stress filter (src/field_smoothing.cu:239-314).  store != 0 copies the
+// Shepard stress filter (src/field_smoothing.cu:26-111).  store != 0 copies the
 // result back into the stress (StressRegularization) and refreshes the records.
 // ---------------------------------------------------------------------------------
 template <class T> __global__ void __launch_bounds__(128) k_shepard(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
@@ -1327,23 +1426,31 @@ template <class T> __global__ void __launch_bounds__(128) k_shepard(const Params
   S6<T> sh = zero6<T>();
   T sumker = T(0.0f);
   const T th = P.two_h;
-  for (int oc = 0; oc < 27; ++oc) {
-    const I3 off = off_of(oc);
-    const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
-    if (!in_grid(P, cj)) continue;
-    const int2 rg = S.range[key_of(P, cj) + P.ncell_material];
-    const V3<T> o = mulI(off, th);
-    for (int j = rg.x; j < rg.y; ++j) {
-      V3<T> dr = pos_i - ld3(pos, j) - o;
-      T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
-      T q = r * P.i_h;
-      if (q < T(2.0f)) {
-        T ker = kernel_w(P.knorm, q);
-        T vol = S.idm[c][j].y / S.vel[c][j].w;
-        sumker += ker * vol;
-        sh = sh + ld6(S.str_a[c], S.str_b[c], j) * (ker * vol);
+  auto scan = [&](const I3 cc, const V3<T> pp) {
+    for (int oc = 0; oc < 27; ++oc) {
+      const I3 off = off_of(oc);
+      const I3 cj{cc.x + off.x, cc.y + off.y, cc.z + off.z};
+      if (!in_grid(P, cj)) continue;
+      const int2 rg = S.range[key_of(P, cj) + P.ncell_material];
+      const V3<T> o = mulI(off, th);
+      for (int j = rg.x; j < rg.y; ++j) {
+        V3<T> dr = pp - ld3(pos, j) - o;
+        T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+        T q = r * P.i_h;
+        if (q < T(2.0f)) {
+          T ker = kernel_w(P.knorm, q);
+          T vol = S.idm[c][j].y / S.vel[c][j].w;
+          sumker += ker * vol;
+          sh = sh + ld6(S.str_a[c], S.str_b[c], j) * (ker * vol);
+        }
       }
     }
+  };
+  scan(celli, pos_i);
+  if (P.periodbound) {
+    I3 cpb;
+    V3<T> ppb;
+    if (period_image(P, celli, pos_i, true, cpb, ppb)) scan(cpb, ppb);
   }
   if (sumker != T(0.f)) sh = sh / sumker;
   st6(S.tc_a, S.tc_b, i, sh);

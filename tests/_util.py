@@ -22,6 +22,25 @@ def rel(a, b) -> float:
     return float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(a))
 
 
+def far_from_contact(case, cellpos, pospres, contact_var):
+    """Material rows farther than one kernel support (2h) from every particle of the
+    contact zone (contact_var.y <= 2h).  Inside the zone the reference's contact
+    redistribution reads state that other threads are rewriting
+    (src/particle_interaction.cu:147-166), which the oracle and the product resolve as
+    a start-of-stage snapshot; its rounding-level differences reach the first ring of
+    neighbours through the SPH sums."""
+    from scipy.spatial import cKDTree
+
+    h = case.params["dr"] * case.params["hdr"]
+    mat = np.arange(case.np_) >= case.npb
+    zone = mat & (contact_var[:, 1] <= 2.0 * h + 1e-12)
+    if not zone.any():
+        return mat
+    pabs = pospres[:, :3].astype(np.float64) + cellpos[:, :3].astype(np.float64) * (2.0 * h)
+    d, _ = cKDTree(pabs[zone]).query(pabs)
+    return mat & ~zone & (d > 2.0 * h)
+
+
 def golden(name: str):
     return np.load(os.path.join(GOLDEN, f"{name}_ref.npz"))
 

@@ -11,12 +11,15 @@ own sources).  For each mini case it:
    and after steps 10 and 100, plus the reference's wall-strip force every step;
 3. packs the arrays the parity tests compare into ``<case>_ref.npz``.
 
-Usage:  python tests/golden/make_golden.py OUTDIR_FOR_RAW_DUMPS
+Usage:  python tests/golden/make_golden.py OUTDIR_FOR_RAW_DUMPS [CASE ...]
+(no CASE: every case; the fixtures are written next to this script and copied into
+OUTDIR_FOR_RAW_DUMPS)
 """
 from __future__ import annotations
 
 import hashlib
 import os
+import shutil
 import struct
 import subprocess
 import sys
@@ -37,12 +40,15 @@ STAGES = ["p0_sorted", "p1_adami", "p2_corner", "p3_interaction", "p4_predictor"
 
 
 def mini_cases():
-    """The two fixture cases: a column collapse and a retaining wall with a contact wall.
-    The wall case uses the reference's hard-coded wall friction (0.58108)."""
+    """The fixture cases: a column collapse, a retaining wall with a contact wall, and
+    the same wall periodic in y (no side walls, period-bound planes).  The wall cases
+    use the reference's hard-coded wall friction (0.58108)."""
     return {
         "col_mini": C.column_collapse(nx=8, ny=8, nz=16, runout=1.0, name="col_mini"),
         "wall_mini": C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005, wall_friction=C.REFERENCE_WALL_FRICTION,
                                       name="wall_mini"),
+        "per_mini": C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005, wall_friction=C.REFERENCE_WALL_FRICTION,
+                                     periodic_y=True, name="per_mini"),
     }
 
 
@@ -99,11 +105,13 @@ STAGE_KEYS = {
 STEP_KEYS = ["cellpos", "pospres", "velrhop", "str", "idmassidx", "contact_mag", "contact_var"]
 
 
-def main(raw_dir: str) -> None:
+def main(raw_dir: str, only=None) -> None:
     drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver_f32")
     if not os.path.exists(drv):
         raise SystemExit(f"missing {drv}; run oracle/build_ref.sh where the reference sources exist")
     for name, case in mini_cases().items():
+        if only and name not in only:
+            continue
         d = os.path.join(raw_dir, name)
         os.makedirs(os.path.join(d, "stage"), exist_ok=True)
         proj = os.path.join(d, name)
@@ -131,8 +139,9 @@ def main(raw_dir: str) -> None:
         fx["wall_force_kN"] = th.reshape(-1, 2)
         out = os.path.join(HERE, f"{name}_ref.npz")
         np.savez_compressed(out, **fx)
+        shutil.copy(out, os.path.join(raw_dir, f"{name}_ref.npz"))
         print(name, case.np_, case.npb, case.npm, os.path.getsize(out), "bytes")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden_raw"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden_raw"), sys.argv[2:])

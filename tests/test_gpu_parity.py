@@ -7,11 +7,11 @@ import pytest
 
 from oracle.oracle import Oracle
 from retainwall_code_b200 import LoquatSph
-from tests._util import STEP_STAGES, boundary_normal_mask, golden, load_state, mini_cases, rel
+from tests._util import STEP_STAGES, boundary_normal_mask, far_from_contact, golden, load_state, mini_cases, rel
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["col_mini", "wall_mini"]
+CASES = ["col_mini", "wall_mini", "per_mini"]
 GPU_STAGE = {
     "begin_step": lambda s: s.step_calculation(),
     "neighbor_search_p": lambda s: s.neighbor_search(0),
@@ -87,9 +87,7 @@ def test_trajectory_100_steps_graph(cases, name):
         wf.append(s.wall_force(1)[0] * 1e-3)
         if st in (1, 10, 100):
             np.testing.assert_array_equal(s.get("cellpos"), g[f"step{st}/cellpos"])
-            cv = g[f"step{st}/contact_var"]
-            mat = np.arange(c.np_) >= c.npb
-            far = mat & ~(cv[:, 1] <= 2.0 * c.params["dr"] * c.params["hdr"] + 1e-12)
+            far = far_from_contact(c, g[f"step{st}/cellpos"], g[f"step{st}/pospres"], g[f"step{st}/contact_var"])
             for key in ("pospres", "velrhop", "str"):
                 a, b = s.get(key), g[f"step{st}/{key}"]
                 assert rel(a[far], b[far]) < 1e-5, (st, key, rel(a[far], b[far]))
@@ -156,7 +154,7 @@ def test_device_error_word_on_wall_leaving_grid():
     assert s.info().device_err & 1
 
 
-@pytest.mark.parametrize("build", ["col_mini", "wall_mini", "thin_column", "wall_medium"])
+@pytest.mark.parametrize("build", ["col_mini", "wall_mini", "per_mini", "thin_column", "wall_medium"])
 def test_chunked_interaction_equals_global_path(cases, build):
     """The chunked interaction (neighbour tile in shared memory) and the global-memory
     path run the same arithmetic in the same order: states must be bit-identical.
@@ -261,3 +259,24 @@ def test_autotune_picks_a_kernel():
     k = s.autotune(2)
     assert k in (0, 1)
     assert s.info().step == 6 and s.info().device_err == 0
+
+
+def test_periodic_wrap_matches_oracle():
+    """Particles leaving through a periodic plane re-enter through the other one; after
+    the wraps the GPU's cell coordinates equal the oracle's and no particle is lost."""
+    from tests.test_oracle_golden import _periodic_drift_case
+
+    c = _periodic_drift_case()
+    s = LoquatSph(case=c)
+    o = Oracle(c, 4)
+    s.step(10)
+    o.step(10)
+    yl, yr = -c.params["planeleft"][3], c.params["planeright"][3]
+    for sim in (s, o):
+        inf = sim.info()
+        assert inf.npm == c.npm and inf.np_delete_m == 0
+        y = sim.get("pos_abs")[c.npb:, 1]
+        assert y.min() >= yl - 1e-6 and y.max() <= yr + 1e-6
+    np.testing.assert_array_equal(s.get("cellpos"), o.get("cellpos"))
+    assert rel(s.get("pos_abs"), o.get("pos_abs")) < 1e-5
+    assert s.info().device_err == 0

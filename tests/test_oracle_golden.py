@@ -10,9 +10,9 @@ import numpy as np
 import pytest
 
 from oracle.oracle import Oracle
-from tests._util import STEP_STAGES, boundary_normal_mask, golden, load_state, mini_cases, rel
+from tests._util import STEP_STAGES, boundary_normal_mask, far_from_contact, golden, load_state, mini_cases, rel
 
-CASES = ["col_mini", "wall_mini"]
+CASES = ["col_mini", "wall_mini", "per_mini"]
 
 
 @pytest.fixture(scope="module")
@@ -70,11 +70,7 @@ def test_trajectory_100_steps(cases, name):
         wf.append(o.wall_force(2)[0])
         if s in (1, 10, 100):
             np.testing.assert_array_equal(o.get("cellpos"), g[f"step{s}/cellpos"])
-            cv = g[f"step{s}/contact_var"]
-            mat = np.arange(c.np_) >= c.npb
-            contact_zone = cv[:, 1] <= 2.0 * c.params["dr"] * c.params["hdr"] + 1e-12
-            # boundary rows adjacent to the contact zone take the Adami average of it
-            far = mat & ~contact_zone
+            far = far_from_contact(c, g[f"step{s}/cellpos"], g[f"step{s}/pospres"], g[f"step{s}/contact_var"])
             for key in ("pospres", "velrhop", "str"):
                 a, b = o.get(key), g[f"step{s}/{key}"]
                 assert rel(a[far], b[far]) < 1e-5, (s, key, "far", rel(a[far], b[far]))
@@ -83,3 +79,43 @@ def test_trajectory_100_steps(cases, name):
     wf = np.asarray(wf)
     scale = max(np.abs(ref).max(), 1e-30)
     assert np.max(np.abs(wf - ref)) / scale < 5e-3
+
+
+def _periodic_drift_case():
+    """Periodic-in-y wall case whose left plane sits 0.52 dx above the soil's first row,
+    so the first corrector already finds jittered particles outside it; the soil also
+    drifts in +y.  The period stays the soil width W."""
+    from retainwall_code_b200 import cases as C
+
+    c = C.retaining_wall(nx=12, ny=6, nz=8, dx=0.005, periodic_y=True, wall_friction=0.58108)
+    dx = c.params["dr"]
+    c.params["planeleft"] = [0.0, 1.0, 0.0, c.params["planeleft"][3] - 0.52 * dx]
+    c.params["planeright"] = [0.0, -1.0, 0.0, c.params["planeright"][3] + 0.52 * dx]
+    c.velrhop[c.npb:, 1] = 0.5
+    return c
+
+
+def test_periodic_wrap_conserves_particles():
+    """Particles leaving through one periodic plane re-enter through the other
+    (cuCheckOutDomainPeriod, src/predictor_corrector.cu:26-40): nothing is deleted,
+    every particle stays within one period, and the wrapped ones moved by -+W."""
+    c = _periodic_drift_case()
+    o = Oracle(c, 4)
+    yl, yr = -c.params["planeleft"][3], c.params["planeright"][3]
+    W = yr - yl
+
+    def by_id(sim):
+        ids = sim.get("idmassidx")[:, 2].astype(np.int64)
+        y = np.empty(c.np_)
+        y[ids] = sim.get("pos_abs")[:, 1]
+        return y[c.npb:]
+
+    y_before = by_id(o)
+    o.step(10)
+    inf = o.info()
+    assert inf.npm == c.npm and inf.np_delete_m == 0
+    y = by_id(o)
+    assert y.min() >= yl - 1e-6 and y.max() <= yr + 1e-6
+    jumped = np.abs((y - y_before) - W) < 0.1 * c.params["dr"]
+    assert jumped.sum() > 0
+    assert np.all(np.abs(y - y_before)[~jumped] < 0.1 * c.params["dr"])
