@@ -286,6 +286,8 @@ def run_ours(args, ws, rank, local):
         sim.set_option(_abi.OPT_INTERACTION_KERNEL, args.ix_kernel)
     if args.strict:
         sim.set_option(_abi.OPT_STRICT_FP, 1)
+    if args.skin is not None:
+        sim.set_option(_abi.OPT_LIST_SKIN, args.skin)
     inf = sim.info()
     sim.step(args.warmup)
     sim.synchronize()
@@ -298,6 +300,8 @@ def run_ours(args, ws, rank, local):
     npm = sim.info().npm
     value = ws * npm * args.steps / (ms * 1e-3)
     inf = sim.info()
+    lists = {"skin_h": 0.02 if args.skin is None else args.skin, "sections_that_sorted": inf.n_sorts,
+             "interactions_on_kept_lists": inf.n_list_reuse, "interactions": 2 * inf.step}
     if inf.device_err:
         raise SystemExit(f"device error word {inf.device_err}")
     if args.no_e2e:
@@ -360,6 +364,7 @@ def run_ours(args, ws, rank, local):
         "roofline_issue": issue,
         "roofline_step": roof_step,
         "stage_ms": stages,
+        "candidate_lists": lists,
         "gpu_launches": kps * args.steps,
         "clocks": clocks,
     }
@@ -446,7 +451,8 @@ def main():
     ap.add_argument("--workload", default="wall2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and stage-profile passes")
-    ap.add_argument("--ix-kernel", type=int, default=None, help="interaction kernel: 1 chunked (default), 0 global")
+    ap.add_argument("--ix-kernel", type=int, default=None, help="interaction kernel: 0 global (default), 1 chunked")
+    ap.add_argument("--skin", type=float, default=None, help="kept candidate-list skin in units of h (0: scan cells)")
     ap.add_argument("--strict", action="store_true", help="separately rounded interaction arithmetic")
     ap.add_argument("--precision-report", action="store_true", help="precision form vs FP64 (configs 1 and 3)")
     ap.add_argument("--precision-steps", type=int, default=2000)

@@ -121,6 +121,8 @@ typedef struct rw_info {
   int32_t np, npb, npm, np_delete_m, ncell, step, scalar_bytes, device_err;
   int32_t cell_num[3], n_motion;
   double time, dt, h, dr;
+  int32_t n_sorts;       /* neighbour-search sections whose sort permuted the particles     */
+  int32_t n_list_reuse;  /* corrector-section interactions that walked the predictor's lists */
 } rw_info;
 
 typedef struct rw_ctx rw_ctx;
@@ -136,10 +138,15 @@ enum {
   RW_OPT_STRICT_FP = 3,         /* interaction arithmetic: 0 (default) fused multiply-adds at fixed places;
                                    1 every product and sum rounded separately, the written order of the
                                    reference's expressions (slower; for bit-level comparisons) */
-  RW_OPT_MIXED_PRECISION = 4    /* precision form (float contexts): 1 = compensated (Kahan) position and
+  RW_OPT_MIXED_PRECISION = 4,   /* precision form (float contexts): 1 = compensated (Kahan) position and
                                    velocity integration and an FP64 strain-rate norm in the hypoplastic
                                    update; the wall resultant is always accumulated in FP64.  Set before
                                    stepping. */
+  RW_OPT_LIST_SKIN = 5          /* skin of the kept candidate lists, in units of h (default 0.02; 0 = scan
+                                   the cells in every interaction).  The interaction keeps each particle's
+                                   candidates within 2h + skin and walks them instead of the 27 cells until
+                                   a sort permutes, a particle changes cell, or a particle may have moved
+                                   0.45 skin; results do not depend on it. */
 };
 
 const char* rw_status_string(rw_status s);

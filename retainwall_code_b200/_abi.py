@@ -11,6 +11,7 @@ STATUS_NAMES = {0: "RW_OK", 1: "RW_EINVAL", 2: "RW_ENOENT", 3: "RW_EIO", 4: "RW_
                 6: "RW_ENOMEM", 7: "RW_EDEVICE", 8: "RW_ETIMEDOUT", 9: "RW_ESTATE"}
 MODEL_MAX, MATERIAL_SIZE, MOTION_MAX, TABLE_MAX = 10, 15, 10, 10
 OPT_WALL_FRICTION, OPT_COMPAT_CONTACT, OPT_INTERACTION_KERNEL, OPT_STRICT_FP, OPT_MIXED_PRECISION = 0, 1, 2, 3, 4
+OPT_LIST_SKIN = 5
 
 # rw_array ids and their row shapes (columns, integer?)
 ARRAYS: Dict[str, int] = {
@@ -85,6 +86,7 @@ class Info(ct.Structure):
         ("ncell", ct.c_int32), ("step", ct.c_int32), ("scalar_bytes", ct.c_int32), ("device_err", ct.c_int32),
         ("cell_num", ct.c_int32 * 3), ("n_motion", ct.c_int32),
         ("time", ct.c_double), ("dt", ct.c_double), ("h", ct.c_double), ("dr", ct.c_double),
+        ("n_sorts", ct.c_int32), ("n_list_reuse", ct.c_int32),
     ]
 
 

@@ -201,6 +201,7 @@ template <class T> struct Engine final : EngineBase {
     P.two_h = (T)(2.0 * (double)P.h);
     const double rpre = 2.0 * h_d * (1.0 + 1e-4);
     P.r2_prefilter = (T)(rpre * rpre);
+    set_skin(0.02);
     P.dt = P.cfl * (P.h / P.cs_m);  // StepCalculation (src/loquat.cu:368-369)
 
     const size_t np = P.np, npb = P.npb;
@@ -259,6 +260,13 @@ template <class T> struct Engine final : EngineBase {
     S.col_cnt = dalloc<int>(ncol);
     S.col_off = dalloc<int>(ncol);
     S.chunks = dalloc<Chunk>(max_chunks);
+    S.nbg_stride = (int)(np - npb);
+    if ((size_t)IX_CAP * (np - npb) < ((size_t)1 << 31)) {  // list indices stay 32-bit
+      S.nbg = dalloc<unsigned>((size_t)IX_CAP * (np - npb));
+      S.nbg_cnt = dalloc<int>(np - npb);
+    }
+    S.dacc = dalloc<float>(np);
+    RW_CU(cudaMemsetAsync(S.dacc, 0, np * sizeof(float), st));
     d_dyn = dalloc<Dyn<T>>(1);
 
     // Host-side conversion to structure-of-arrays, with the reference's
@@ -617,10 +625,32 @@ template <class T> struct Engine final : EngineBase {
     o->dt = (double)P.dt;
     o->h = (double)P.h;
     o->dr = (double)P.dr;
+    o->n_sorts = d.n_sorts;
+    o->n_list_reuse = d.n_reuse;
+  }
+
+  // Kept candidate lists: radius 2h + skin; dropped once any particle may have moved
+  // 0.45 skin since they were built (two particles then close in by at most 0.9 skin,
+  // so every pair within 2h is still listed).
+  void set_skin(double skin_h) {
+    const double h_d = (double)P.h;
+    const double skin = skin_h * h_d;
+    const double rlist = (2.0 * h_d + skin) * (1.0 + 1e-4);
+    P.keep_lists = skin_h > 0.0 ? 1 : 0;
+    P.r2_list = (T)(rlist * rlist);
+    P.disp_lim = (float)(0.45 * skin);
+    P.disp_eps = (float)(std::ldexp(2.0 * h_d, -20));
   }
 
   int set_option(int opt, double v) override {
-    if (opt == RW_OPT_WALL_FRICTION) {
+    if (opt == RW_OPT_LIST_SKIN) {
+      if (!(v >= 0.0 && v <= 1.0)) {
+        err = "list skin must be within [0, 1] h";
+        return RW_EINVAL;
+      }
+      set_skin(v);
+      drop_lists();
+    } else if (opt == RW_OPT_WALL_FRICTION) {
       P.wall_fric = (T)v;
     } else if (opt == RW_OPT_MIXED_PRECISION) {
       if (sizeof(T) != 4 && v != 0.0) {
@@ -814,8 +844,17 @@ template <class T> struct Engine final : EngineBase {
       case RW_ARR_STN_INI: get6(S.stni_a[ci], S.stni_b[ci]); break;
       default: return RW_EINVAL;
     }
-    RW_CU(cudaStreamSynchronize(st));
+    drop_lists();
     return RW_OK;
+  }
+
+  // State written from the host: the kept candidate lists no longer describe it.
+  void drop_lists() {
+    Dyn<T> d = dyn_host();
+    d.list_ok = 0;
+    d.ix_mode = 0;
+    RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
+    RW_CU(cudaStreamSynchronize(st));
   }
 
   void set_counters(double time, int step_, int npm, int np_delete_m) override {
@@ -825,6 +864,8 @@ template <class T> struct Engine final : EngineBase {
     d.step = step_;
     d.npm = npm;
     d.np_delete_m = np_delete_m;
+    d.list_ok = 0;
+    d.ix_mode = 0;
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     RW_CU(cudaStreamSynchronize(st));
   }

@@ -79,6 +79,12 @@ template <class T> struct DevState {
   int* col_cnt;
   int* col_off;
   struct Chunk* chunks;
+  // Candidate lists of the soil particles (entry e of soil slot t at nbg[e * nbg_stride + t],
+  // encoded like the shared-memory lists), count per slot (-1: not kept).
+  unsigned* nbg;
+  int* nbg_cnt;
+  int nbg_stride;
+  float* dacc;    // per slot: bound on the distance moved since the lists were built (not permuted)
 };
 
 template <class T> RWD V3<T> ld3(const V4<T>* p, int i) { V4<T> v = p[i]; return {v.x, v.y, v.z}; }
@@ -354,6 +360,21 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
     dyn->cur_main ^= 1;
     if (section == 0) dyn->cur_nrm ^= 1;
     else dyn->cur_ini ^= 1;
+    dyn->n_sorts += 1;
+  }
+  // Candidate lists: an interaction walks the kept lists when nothing was permuted and
+  // no particle changed cell or moved more than the skin allows since they were built
+  // (the integrators raise list_kill); otherwise it scans the cells and keeps new lists.
+  // Lists built in the corrector section, from mid-step positions, are not kept.
+  if (section >= 0) {
+    const int reuse = (!dyn->need_sort && dyn->list_ok && !dyn->list_kill) ? 1 : 0;
+    dyn->ix_mode = reuse;
+    dyn->n_reuse += reuse;
+    if (!reuse) {
+      dyn->list_ok = 0;
+      dyn->list_kill = 0;
+      dyn->build_kill = section;
+    }
   }
   if (!rigid) return;
   const T dt = P.dt;
@@ -464,7 +485,9 @@ template <class T> RWD void period_wrap(const Params<T>& P, int4& cp, V4<T>& ps)
 // ---------------------------------------------------------------------------------
 template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.npb || dyn->npm == 0) return;
+  if (i >= P.npb) return;
+  if (dyn->ix_mode == 0) S.dacc[i] = 0.0f;  // candidate lists are rebuilt from these positions
+  if (dyn->npm == 0) return;
   const int c = dyn->cur_main;
   const V4<T>* __restrict__ pos = S.pos[c];
   const V4<T>* __restrict__ vel = S.vel[c];
@@ -802,11 +825,13 @@ template <bool Strict, class T> RWD void ix_list_eval(const Params<T>& P, const 
 // shared memory (my[k * stride]), phase 2 evaluates them in order.  A list that fills
 // up is evaluated and emptied, and the scan resumes (order preserved).
 template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
-                                                        const IState<T>& I, unsigned* my, int stride, int cap, Acc<T>& A) {
+                                                        const IState<T>& I, unsigned* my, int stride, int cap, Acc<T>& A,
+                                                        int keep_slot = -1) {
   const V4<T>* __restrict__ pos = S.pos[c];
   const T th = P.two_h;
-  const T r2max = P.r2_prefilter;
+  const T r2max = keep_slot >= 0 ? P.r2_list : P.r2_prefilter;
   int cnt = 0;
+  bool spilled = false;
   for (int oc = 0; oc < 27; ++oc) {
     const I3 off = off_of(oc);
     const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
@@ -824,12 +849,18 @@ template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, cons
           if (cnt == cap) {
             ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
             cnt = 0;
+            spilled = true;
           }
           my[cnt * stride] = (unsigned)j | ((unsigned)oc << 27);
           ++cnt;
         }
       }
     }
+  }
+  if (keep_slot >= 0) {  // keep the list for the corrector section (unless it spilled)
+    if (!spilled)
+      for (int e = 0; e < cnt; ++e) S.nbg[(size_t)e * S.nbg_stride + keep_slot] = my[e * stride];
+    S.nbg_cnt[keep_slot] = spilled ? -1 : cnt;
   }
   ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
 }
@@ -968,13 +999,23 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX_THREADS) k_
     return;
   }
   const int c = dyn->cur_main;
+  const bool keep = S.nbg && P.keep_lists;
+  const int mode = keep ? dyn->ix_mode : 0;
+  if (mode == 0 && t == 0 && keep) {
+    Dyn<T>* d = const_cast<Dyn<T>*>(dyn);
+    d->list_ok = 1;
+    d->list_kill = d->build_kill;
+  }
+  if (mode == 0) S.dacc[i] = 0.0f;
   const int4 cp = S.cellpos[c][i];
   const I3 celli{cp.x, cp.y, cp.z};
   const V4<T> cv = S.cv[cpar][i];
   IState<T> I;
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
-  ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A);
+  const int kept = mode == 1 ? S.nbg_cnt[t] : -1;
+  if (kept >= 0) ix_list_eval<Strict>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, A);
+  else ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A, (mode == 0 && keep) ? t : -1);
   if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
@@ -1281,6 +1322,10 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
     vr = vr + acc * hdt;
     ps = add3(ps, xyz(vr) * hdt);
   }
+  {  // distance since the lists were built, after this half step
+    const float a = (float)(f_sqrt(vr.x * vr.x + vr.y * vr.y + vr.z * vr.z) * hdt);
+    if (S.dacc[i] + a + P.disp_eps > P.disp_lim) const_cast<Dyn<T>*>(dyn)->list_kill = 1;
+  }
   const T* mp = P.model_par[code.w];
   vr.w = f_max(vr.w, mp[kMatSize - 2]);
   vr.w = f_min(vr.w, mp[kMatSize - 1]);
@@ -1311,6 +1356,16 @@ template <class T> RWD I3 rebin(V4<T>& ps, T th) {
   return dc;
 }
 
+// Bookkeeping of the kept candidate lists for one particle's full step: a cell change
+// reorders its pairs and kills the lists; otherwise its distance bound grows by the
+// step (plus a rounding allowance) and must stay within the skin's share.
+template <class T> RWD void list_account(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, int i, float step,
+                                         int cell_moved) {
+  const float d = S.dacc[i] + step + P.disp_eps;
+  S.dacc[i] = d;
+  if (cell_moved || d > P.disp_lim) const_cast<Dyn<T>*>(dyn)->list_kill = 1;
+}
+
 template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int npm = dyn->npm;
@@ -1339,6 +1394,7 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
     const I3 dc = rebin(ps, th);
     S.pos[c][i] = ps;
     S.cellpos[c][i] = int4{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z, cp.w};
+    list_account(P, S, dyn, i, (float)(f_sqrt(dot(vel, vel)) * P.dt), dc.x | dc.y | dc.z);
     return;
   }
   const V4<T> vri = S.vel_ini[ci][i];
@@ -1375,9 +1431,13 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
     S.cmp_p[c][i] = kp;
     S.cmp_v[c][i] = kv;
   }
-  int4 cp = S.cellpos[c][i];
-  cp = int4{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z, cp.w};
+  const int4 cp0 = S.cellpos[c][i];
+  int4 cp = int4{cp0.x + dc.x, cp0.y + dc.y, cp0.z + dc.z, cp0.w};
   if (P.periodbound) period_wrap(P, cp, ps);
+  {
+    const V3<T> inc = xyz(vr + vri) * (T(0.5f) * P.dt);
+    list_account(P, S, dyn, i, (float)f_sqrt(dot(inc, inc)), (cp.x - cp0.x) | (cp.y - cp0.y) | (cp.z - cp0.z));
+  }
   S6<T> sg = ld6(S.stri_a[ci], S.stri_b[ci], i);
   const S6<T> D = ld6(S.ace_a, S.ace_b, i);
   const S6<T> sn = ld6(S.stni_a[ci], S.stni_b[ci], i) + D * P.dt;

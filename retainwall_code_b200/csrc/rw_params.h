@@ -52,6 +52,10 @@ template <class T> struct Params {
   T time_max, dt, output_frequency;
   T wall_fric;               // wall-soil Coulomb coefficient
   T r2_prefilter;            // conservative (2h)^2 bound for the candidate pre-test
+  T r2_list;                 // conservative (2h + skin)^2: radius of the kept candidate lists
+  float disp_lim;            // a particle's displacement since the lists were built may not pass this
+  float disp_eps;            // rounding allowance added per position update
+  int keep_lists;            // 0: every interaction scans the cells
   int mixed;                 // precision form: compensated integration, FP64 strain-rate norm
   int pad_m;
 };
@@ -67,7 +71,12 @@ template <class T> struct Dyn {
   unsigned err;              // RW_DERR_* bits
   int step;
   int nchunks;               // live entries of the interaction chunk list
-  int pad1_;
+  // Candidate lists kept across sections and steps: ix_mode 0 = scan the cells (and
+  // keep the lists), 1 = walk the kept lists.  list_kill: some particle changed cell or
+  // moved too far since the lists were built; build_kill: lists built in this section
+  // are not to be kept (a corrector-section rebuild).
+  int ix_mode, list_ok, list_kill, build_kill;
+  int n_sorts, n_reuse;      // sections that permuted / corrector sections that reused lists
   Motion<T> mv[kMotionMax];
   Table<T> tab[kMotionMax];
 };

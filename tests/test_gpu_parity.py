@@ -170,6 +170,7 @@ def test_chunked_interaction_equals_global_path(cases, build):
         c = C.retaining_wall(nx=48, ny=24, nz=36, dx=0.0025, wall_friction=0.58108)
     a = LoquatSph(case=c)
     b = LoquatSph(case=c)
+    a.set_option(_abi.OPT_INTERACTION_KERNEL, 1)
     b.set_option(_abi.OPT_INTERACTION_KERNEL, 0)
     a.step(10)
     b.step(10)
@@ -280,3 +281,37 @@ def test_periodic_wrap_matches_oracle():
     np.testing.assert_array_equal(s.get("cellpos"), o.get("cellpos"))
     assert rel(s.get("pos_abs"), o.get("pos_abs")) < 1e-5
     assert s.info().device_err == 0
+
+
+def test_kept_candidate_lists_reused_and_dropped(cases):
+    """Interactions walk the candidate lists kept by an earlier scan while no particle
+    changed cell or moved more than the skin allows (a quasi-static case: every
+    interaction after the first); in a fast case (a half step beyond the skin's share)
+    every interaction scans the cells again.  Either way the result equals the chunked
+    kernel, which never keeps lists, bit for bit."""
+    from retainwall_code_b200 import _abi
+
+    c = cases["wall_mini"]
+    s = LoquatSph(case=c)
+    s.step(5)
+    assert s.info().n_list_reuse == 9
+    b = LoquatSph(case=c)
+    b.set_option(_abi.OPT_INTERACTION_KERNEL, 1)
+    b.step(5)
+    d = LoquatSph(case=c)
+    d.set_option(_abi.OPT_LIST_SKIN, 0.0)
+    d.step(5)
+    assert d.info().n_list_reuse == 0
+    for key in ("cellpos", "pospres", "velrhop", "str", "contact_var", "accad"):
+        np.testing.assert_array_equal(s.get(key), b.get(key), err_msg=key)
+        np.testing.assert_array_equal(s.get(key), d.get(key), err_msg=key)
+    fast = mini_cases()["wall_mini"]
+    fast.velrhop[fast.npb:, 0] = 40.0  # a half step of 0.2 mm > 0.45 x skin (0.054 mm)
+    a = LoquatSph(case=fast)
+    b = LoquatSph(case=fast)
+    b.set_option(_abi.OPT_INTERACTION_KERNEL, 1)
+    a.step(3)
+    b.step(3)
+    assert a.info().n_list_reuse == 0
+    for key in ("cellpos", "pospres", "velrhop", "str", "contact_var", "accad"):
+        np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
