@@ -349,9 +349,9 @@ template <class T> struct Engine final : EngineBase {
       }
     }
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
-    RW_CU(cudaFuncSetAttribute(k_interaction<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RW_CU(cudaFuncSetAttribute(k_interaction<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                IX_CAP * IX_THREADS * (int)sizeof(unsigned)));
-    RW_CU(cudaFuncSetAttribute(k_interaction<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RW_CU(cudaFuncSetAttribute(k_interaction<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                IX_CAP * IX_THREADS * (int)sizeof(unsigned)));
     RW_CU(cudaFuncSetAttribute(k_interaction2<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(Ix2Smem<T>)));
@@ -429,8 +429,14 @@ template <class T> struct Engine final : EngineBase {
         if (strict_fp) k_interaction2<T, true><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
         else k_interaction2<T, false><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
       } else {
-        if (strict_fp) k_interaction<T, true><<<nblk(n, IX_THREADS), IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
-        else k_interaction<T, false><<<nblk(n, IX_THREADS), IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
+        const unsigned g = nblk(n, IX_THREADS);
+        if (strict_fp) {
+          k_interaction<T, true, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
+          k_interaction<T, true, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
+        } else {
+          k_interaction<T, false, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
+          k_interaction<T, false, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
+        }
       }
       check_launch();
     }
@@ -504,7 +510,8 @@ template <class T> struct Engine final : EngineBase {
   // Kernels launched by one whole step (launch_step), for launch accounting.
   int kernels_per_step() const {
     const int search = 2 + 3 * S.sort_passes + 4 + (ncol > 0 ? 3 : 0);  // keys, check, sort, ranges, count, permute, flip, chunks
-    int k = 1 + 2 * search + 2 * 3 + 1 + 1 + 1;     // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
+    const int ix = ix_kernel == 1 ? 1 : 2;             // chunked, or scan + walk
+    int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
     if (P.stress_shepard_filter != 0) k += 2;
     if (P.npb == 0) k -= 2;

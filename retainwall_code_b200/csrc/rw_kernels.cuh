@@ -14,6 +14,7 @@ namespace rw {
 // computed once per particle per section.  48 bytes in float: the contact-wall flag
 // travels as the sign of the (always positive) volume.
 template <class T> struct Rec {
+  V4<T> p;   // in-cell position (w unused): one aligned 64-byte record per neighbour in float
   V4<T> vr;  // velocity xyz, density
   V4<T> a;   // mass, +-volume (negative: contact-wall particle), sigma/rho^2 xx, yy
   V4<T> b;   // sigma/rho^2 zz, xy, xz, yz
@@ -114,11 +115,13 @@ RWD double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
 // Neighbour record of particle i (boundary: mass = V0 rho; material: idmassidx.y),
 // with the reference's per-pair expressions (src/particle_interaction.cu:44-49,71).
-template <class T> RWD void write_rec(const Params<T>& P, Rec<T>* rec, int i, V4<T> vr, S6<T> s, T mass, bool contact) {
+template <class T> RWD void write_rec(const Params<T>& P, Rec<T>* rec, int i, V4<T> pos, V4<T> vr, S6<T> s, T mass,
+                                      bool contact) {
   const T rho = vr.w;
   const S6<T> sor = s / rmul(rho, rho);
   const T vol = mass / rho;
   Rec<T> r;
+  r.p = V4<T>{pos.x, pos.y, pos.z, T(0)};
   r.vr = vr;
   r.a = V4<T>{mass, contact ? -vol : vol, sor.xx, sor.yy};
   r.b = V4<T>{sor.zz, sor.xy, sor.xz, sor.yz};
@@ -594,7 +597,7 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
     str_out = zero6<T>();
   }
   st6(S.str_a[c], S.str_b[c], i, str_out);
-  write_rec(P, S.rec, i, vr_out, str_out, P.vol_def * vr_out.w, contact);
+  write_rec(P, S.rec, i, S.pos[c][i], vr_out, str_out, P.vol_def * vr_out.w, contact);
 }
 
 // ---------------------------------------------------------------------------------
@@ -658,7 +661,8 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
   S.cv[cpar][i] = cv;
   S.cny[i] = ny;
   S.cvz[i] = vz;
-  write_rec(P, S.rec, i, S.vel[c][i], ld6(S.str_a[c], S.str_b[c], i), S.idm[c][i].y, S.codes[c][i].x >= 10);
+  write_rec(P, S.rec, i, S.pos[c][i], S.vel[c][i], ld6(S.str_a[c], S.str_b[c], i), S.idm[c][i].y,
+            S.codes[c][i].x >= 10);
 }
 
 // ---------------------------------------------------------------------------------
@@ -688,10 +692,11 @@ template <class T> struct IState {
 
 // The neighbour-side values one pair term needs.
 template <class T> struct NbVals {
-  V4<T> vr, a, b;
+  V4<T> p, vr, a, b;
 };
 template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) {
   NbVals<T> v;
+  v.p = rec[j].p;
   v.vr = rec[j].vr;
   v.a = rec[j].a;
   v.b = rec[j].b;
@@ -706,7 +711,6 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
   T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
   T q = F::mul(r, P.i_h);
   if (!(q < T(2.0f))) return;
-  T ker = kernel_w(P.knorm, q);
   const T t = T(2.0f) - q;
   T dwdr = F::mul(F::mul(F::mul(P.kgrad, t), t), t);
   const V3<T> gker{F::mul(dr.x, dwdr), F::mul(dr.y, dwdr), F::mul(dr.z, dwdr)};
@@ -752,7 +756,8 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
     if (rj > T(0.0f)) rj = F::mul(rj, P.art_coef);
     else rj = T(0.0f);
     T artp = I.ri + rj;
-    if (artp > T(0.0f)) {
+    if (artp > T(0.0f)) {  // W itself is only needed here (a double expression, as GetKernel)
+      const T ker = kernel_w(P.knorm, q);
       artp = F::mul(artp, f_pow(ker / P.kernel_dr, P.kernel_zero / P.kernel_dr));
       const T m = F::mul(mass_j, artp);
       A.as.x = F::msub(gker.x, m, A.as.x);
@@ -796,28 +801,24 @@ constexpr int IX_THREADS = 128, IX_CAP = 96;
 template <bool Strict, class T> RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c,
                                                       const IState<T>& I, const unsigned* my, int stride, int cnt,
                                                       Acc<T>& A) {
-  const V4<T>* __restrict__ pos = S.pos[c];
   const Rec<T>* __restrict__ rec = S.rec;
   const T th = P.two_h;
   if (cnt <= 0) return;
   unsigned ent = my[0];
   int jj = (int)(ent & 0x7ffffffu);
   int oc = (int)(ent >> 27);
-  V4<T> pj = pos[jj];
   NbVals<T> nb = load_nb(rec, jj);
-  for (int e = 0; e < cnt; ++e) {  // next entry's position and record prefetched
-    const V4<T> pc = pj;
+  for (int e = 0; e < cnt; ++e) {  // next entry's record (with its position) prefetched
     const NbVals<T> cur = nb;
     const int occ = oc;
     if (e + 1 < cnt) {
       ent = my[(e + 1) * stride];
       jj = (int)(ent & 0x7ffffffu);
       oc = (int)(ent >> 27);
-      pj = pos[jj];
       nb = load_nb(rec, jj);
     }
     const V3<T> o = mulI(off_of(occ), th);
-    pair_eval<Strict>(P, I, I.pos - V3<T>{pc.x, pc.y, pc.z} - o, cur, A);
+    pair_eval<Strict>(P, I, I.pos - V3<T>{cur.p.x, cur.p.y, cur.p.z} - o, cur, A);
   }
 }
 
@@ -982,39 +983,48 @@ template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const Dev
   S.spin[i] = v4(skewpart(A.gv), T(0.f));
 }
 
-// Interaction, one thread per soil particle, neighbours read from global memory.
-// Used for whole launches when the chunked kernel is disabled, and by the chunked
-// kernel for chunks whose neighbour tile does not fit in shared memory.
-template <class T, bool Strict> __global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S,
-                                                                                           const Dyn<T>* dyn, int cpar) {
-  extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread
+// Interaction, one thread per soil particle, neighbours read from global memory, as
+// two launches that split the particles between them:
+//  - scan (Walk = false): scans the 27 cells (keeping the candidate lists when the
+//    step's mode is 0), and handles deleted slots and particles without a kept list;
+//  - walk (Walk = true): in mode 1, walks the kept lists of the other particles.  It
+//    carries no scan state, so it runs with fewer registers.
+template <class T, bool Strict, bool Walk>
+__global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
+                                                            int cpar) {
+  extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread (scan only)
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int total = P.np - P.npb;
   if (t >= total) return;
   const int i = P.npb + t;
   const int npm = dyn->npm;
-  if (t >= npm) {  // deleted slots keep their contact state
+  const bool keep = S.nbg && P.keep_lists;
+  const int mode = keep ? dyn->ix_mode : 0;
+  if (Walk) {
+    if (mode != 1 || t >= npm) return;
+  } else if (t >= npm) {  // deleted slots keep their contact state
     S.cv[cpar ^ 1][i] = S.cv[cpar][i];
     S.cf[cpar ^ 1][i] = S.cf[cpar][i];
     return;
   }
+  const int kept = mode == 1 ? S.nbg_cnt[t] : -1;
+  if (Walk != (kept >= 0)) return;  // the other launch takes this particle
   const int c = dyn->cur_main;
-  const bool keep = S.nbg && P.keep_lists;
-  const int mode = keep ? dyn->ix_mode : 0;
-  if (mode == 0 && t == 0 && keep) {
-    Dyn<T>* d = const_cast<Dyn<T>*>(dyn);
-    d->list_ok = 1;
-    d->list_kill = d->build_kill;
+  if (!Walk) {
+    if (mode == 0 && t == 0 && keep) {
+      Dyn<T>* d = const_cast<Dyn<T>*>(dyn);
+      d->list_ok = 1;
+      d->list_kill = d->build_kill;
+    }
+    if (mode == 0) S.dacc[i] = 0.0f;
   }
-  if (mode == 0) S.dacc[i] = 0.0f;
   const int4 cp = S.cellpos[c][i];
   const I3 celli{cp.x, cp.y, cp.z};
   const V4<T> cv = S.cv[cpar][i];
   IState<T> I;
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
-  const int kept = mode == 1 ? S.nbg_cnt[t] : -1;
-  if (kept >= 0) ix_list_eval<Strict>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, A);
+  if (Walk) ix_list_eval<Strict>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, A);
   else ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A, (mode == 0 && keep) ? t : -1);
   if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
@@ -1529,7 +1539,7 @@ template <class T> __global__ void k_shepard_store(const Params<T> P, DevState<T
   const int c = dyn->cur_main;
   const S6<T> sh = ld6(S.tc_a, S.tc_b, i);
   st6(S.str_a[c], S.str_b[c], i, sh);
-  write_rec(P, S.rec, i, S.vel[c][i], sh, S.idm[c][i].y, S.codes[c][i].x >= 10);
+  write_rec(P, S.rec, i, S.pos[c][i], S.vel[c][i], sh, S.idm[c][i].y, S.codes[c][i].x >= 10);
 }
 
 // ---------------------------------------------------------------------------------
