@@ -199,6 +199,7 @@ template <class T> struct Engine final : EngineBase {
     P.kernel_zero = P.knorm * T(2.0f) * T(2.0f) * T(2.0f) * T(2.0f) * T(0.5f);
     P.kernel_dr = P.knorm * (T(2.0f) - qq) * (T(2.0f) - qq) * (T(2.0f) - qq) * (T(2.0f) - qq) * (qq + T(0.5f));
     P.two_h = (T)(2.0 * (double)P.h);
+    P.visc_k = P.alpha_m * P.cs_m * P.h;
     const double rpre = 2.0 * h_d * (1.0 + 1e-4);
     P.r2_prefilter = (T)(rpre * rpre);
     set_skin(0.02);

@@ -743,8 +743,12 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
     T artv = T(0.0f);
     const T visc = F::dot3(dvel.x, dvel.y, dvel.z, dr.x, dr.y, dr.z);
     if (visc < T(0.0f)) {
-      const T phi = F::mul(P.h, visc) / F::mad(r, r, P.eta);
-      artv = F::mul(F::mul(P.alpha_m, P.cs_m), phi) / F::mul(T(0.5f), I.rho + rho_j);
+      if constexpr (Strict) {
+        const T phi = F::mul(P.h, visc) / F::mad(r, r, P.eta);
+        artv = F::mul(F::mul(P.alpha_m, P.cs_m), phi) / F::mul(T(0.5f), I.rho + rho_j);
+      } else {  // the same quotient with one division
+        artv = F::mul(P.visc_k, visc) / F::mul(F::mad(r, r, P.eta), F::mul(T(0.5f), I.rho + rho_j));
+      }
     }
     const T m = F::mul(mass_j, artv);
     A.av.x = F::mad(gker.x, m, A.av.x);
@@ -798,27 +802,35 @@ constexpr int IX_THREADS = 128, IX_CAP = 96;
 
 // Pair sums of particle i straight from global memory: phase 1 lists candidates in
 // shared memory (my[k * stride]), phase 2 evaluates them in order.
+// otab[oc] = cell offset oc times 2h (a shared-memory table: no per-pair decode).
+template <class T> RWD void fill_offsets(V4<T>* otab, T th) {
+  if (threadIdx.x < 27) {
+    const I3 f = off_of((int)threadIdx.x);
+    otab[threadIdx.x] = V4<T>{(T)f.x * th, (T)f.y * th, (T)f.z * th, T(0)};
+  }
+}
+
 template <bool Strict, class T> RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c,
                                                       const IState<T>& I, const unsigned* my, int stride, int cnt,
-                                                      Acc<T>& A) {
+                                                      const V4<T>* otab, Acc<T>& A) {
   const Rec<T>* __restrict__ rec = S.rec;
-  const T th = P.two_h;
   if (cnt <= 0) return;
+  // Entries are read two ahead and records one ahead, so a record's index is in hand
+  // when its load is issued.
   unsigned ent = my[0];
-  int jj = (int)(ent & 0x7ffffffu);
+  unsigned ent1 = cnt > 1 ? my[stride] : 0u;
   int oc = (int)(ent >> 27);
-  NbVals<T> nb = load_nb(rec, jj);
-  for (int e = 0; e < cnt; ++e) {  // next entry's record (with its position) prefetched
+  NbVals<T> nb = load_nb(rec, (int)(ent & 0x7ffffffu));
+  for (int e = 0; e < cnt; ++e) {
     const NbVals<T> cur = nb;
     const int occ = oc;
     if (e + 1 < cnt) {
-      ent = my[(e + 1) * stride];
-      jj = (int)(ent & 0x7ffffffu);
-      oc = (int)(ent >> 27);
-      nb = load_nb(rec, jj);
+      oc = (int)(ent1 >> 27);
+      nb = load_nb(rec, (int)(ent1 & 0x7ffffffu));
+      if (e + 2 < cnt) ent1 = my[(e + 2) * stride];
     }
-    const V3<T> o = mulI(off_of(occ), th);
-    pair_eval<Strict>(P, I, I.pos - V3<T>{cur.p.x, cur.p.y, cur.p.z} - o, cur, A);
+    const V4<T> o = otab[occ];
+    pair_eval<Strict>(P, I, V3<T>{I.pos.x - cur.p.x - o.x, I.pos.y - cur.p.y - o.y, I.pos.z - cur.p.z - o.z}, cur, A);
   }
 }
 
@@ -826,8 +838,8 @@ template <bool Strict, class T> RWD void ix_list_eval(const Params<T>& P, const 
 // shared memory (my[k * stride]), phase 2 evaluates them in order.  A list that fills
 // up is evaluated and emptied, and the scan resumes (order preserved).
 template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
-                                                        const IState<T>& I, unsigned* my, int stride, int cap, Acc<T>& A,
-                                                        int keep_slot = -1) {
+                                                        const IState<T>& I, unsigned* my, int stride, int cap,
+                                                        const V4<T>* otab, Acc<T>& A, int keep_slot = -1) {
   const V4<T>* __restrict__ pos = S.pos[c];
   const T th = P.two_h;
   const T r2max = keep_slot >= 0 ? P.r2_list : P.r2_prefilter;
@@ -848,7 +860,7 @@ template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, cons
         const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
         if (dx * dx + dy * dy + dz * dz < r2max) {
           if (cnt == cap) {
-            ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
+            ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, otab, A);
             cnt = 0;
             spilled = true;
           }
@@ -863,7 +875,7 @@ template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, cons
       for (int e = 0; e < cnt; ++e) S.nbg[(size_t)e * S.nbg_stride + keep_slot] = my[e * stride];
     S.nbg_cnt[keep_slot] = spilled ? -1 : cnt;
   }
-  ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
+  ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, otab, A);
 }
 
 // Second pass of a particle within 2h of a periodic plane, over the neighbours of its
@@ -989,10 +1001,16 @@ template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const Dev
 //    step's mode is 0), and handles deleted slots and particles without a kept list;
 //  - walk (Walk = true): in mode 1, walks the kept lists of the other particles.  It
 //    carries no scan state, so it runs with fewer registers.
+#ifndef RW_WALK_MIN_BLOCKS
+#define RW_WALK_MIN_BLOCKS 1  // resident blocks per SM the walk kernel's register budget aims at
+#endif
 template <class T, bool Strict, bool Walk>
-__global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
-                                                            int cpar) {
+__global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 1)
+    k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, int cpar) {
   extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread (scan only)
+  __shared__ V4<T> otab[27];
+  fill_offsets(otab, P.two_h);
+  __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int total = P.np - P.npb;
   if (t >= total) return;
@@ -1024,8 +1042,10 @@ __global__ void __launch_bounds__(IX_THREADS) k_interaction(const Params<T> P, D
   IState<T> I;
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
-  if (Walk) ix_list_eval<Strict>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, A);
-  else ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A, (mode == 0 && keep) ? t : -1);
+  if (Walk) ix_list_eval<Strict>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, otab, A);
+  else
+    ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, otab, A,
+                           (mode == 0 && keep) ? t : -1);
   if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
@@ -1137,6 +1157,8 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
                                                                                        const Dyn<T>* dyn, int cpar) {
   extern __shared__ __align__(16) unsigned char smraw[];
   Ix2Smem<T>& sm = *reinterpret_cast<Ix2Smem<T>*>(smraw);
+  __shared__ V4<T> otab[27];
+  fill_offsets(otab, P.two_h);
   const int tid = threadIdx.x;
   // Deleted slots keep their contact state (the chunk list covers live particles only).
   {
@@ -1229,7 +1251,7 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
   if (fallback) {
     // Too big for the tile: same arithmetic from global memory, list in the round buffer.
     ix_sums_global<Strict>(P, S, c, celli, I, reinterpret_cast<unsigned*>(&sm.list[0][0]) + tid, IX2_TB,
-                           IX2_CAP / 2, A);
+                           IX2_CAP / 2, otab, A);
     if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
     ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
     return;

@@ -49,6 +49,7 @@ template <class T> struct Params {
   T model_par[kModelMax][kMatSize];
   T knorm, kgrad;            // Wendland normalisations (src/loquat.cu:163-166)
   T alpha_m, cs_m, eta, cfl, art_coef, kernel_zero, kernel_dr;
+  T visc_k;                  // alpha_m * cs_m * h (artificial viscosity, one-division form)
   T time_max, dt, output_frequency;
   T wall_fric;               // wall-soil Coulomb coefficient
   T r2_prefilter;            // conservative (2h)^2 bound for the candidate pre-test
