@@ -260,6 +260,7 @@ template <class T> struct Engine final : EngineBase {
     S.col_len = dalloc<int>(ncol);
     S.col_cnt = dalloc<int>(ncol);
     S.col_off = dalloc<int>(ncol);
+    S.near_wall = dalloc<unsigned char>(P.ncell_material);
     S.chunks = dalloc<Chunk>(max_chunks);
     S.nbg_stride = (int)(np - npb);
     if ((size_t)IX_CAP * (np - npb) < ((size_t)1 << 31)) {  // list indices stay 32-bit
@@ -392,6 +393,10 @@ template <class T> struct Engine final : EngineBase {
     k_count<T><<<1, 1, 0, st>>>(P, S, d_dyn);
     k_permute<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn, section, compat_contact ? 1 : 0);
     k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
+    if (P.npb > 0) {  // cells near contact walls, for the corner search
+      RW_CU(cudaMemsetAsync(S.near_wall, 0, (size_t)P.ncell_material, st));
+      k_mark_near_wall<T><<<nblk(P.npb, 256), 256, 0, st>>>(P, S, d_dyn);
+    }
     if (ncol > 0) {  // column chunks of the interaction
       k_col_count<T><<<nblk(ncol, 256), 256, 0, st>>>(P, S);
       k_col_scan<T><<<1, 1024, 0, st>>>(P, S, d_dyn);
@@ -510,7 +515,8 @@ template <class T> struct Engine final : EngineBase {
 
   // Kernels launched by one whole step (launch_step), for launch accounting.
   int kernels_per_step() const {
-    const int search = 2 + 3 * S.sort_passes + 4 + (ncol > 0 ? 3 : 0);  // keys, check, sort, ranges, count, permute, flip, chunks
+    // keys, check, sort, ranges, count, permute, flip, contact-wall cells, chunks
+    const int search = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 1 : 0) + (ncol > 0 ? 3 : 0);
     const int ix = ix_kernel == 1 ? 1 : 2;             // chunked, or scan + walk
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;

@@ -86,6 +86,7 @@ template <class T> struct DevState {
   int* nbg_cnt;
   int nbg_stride;
   float* dacc;    // per slot: bound on the distance moved since the lists were built (not permuted)
+  unsigned char* near_wall;  // per cell: a contact-wall particle lies in its 27-cell neighbourhood
 };
 
 template <class T> RWD V3<T> ld3(const V4<T>* p, int i) { V4<T> v = p[i]; return {v.x, v.y, v.z}; }
@@ -604,6 +605,22 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
 // Nearest contact-wall particle / corner rule (src/adami_boundary.cu:209-292), plus
 // the material neighbour records for the interaction.
 // ---------------------------------------------------------------------------------
+// Cells within one cell of a contact-wall particle (codes.x >= 10): the only cells whose
+// soil particles can find a contact wall in cuFindCornerParticleMaterial's 27-cell scan.
+// near_wall is cleared before each search's marking.
+template <class T> __global__ void k_mark_near_wall(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.npb) return;
+  const int c = dyn->cur_main;
+  if (S.codes[c][i].x < 10) return;
+  const int4 cp = S.cellpos[c][i];
+  for (int oc = 0; oc < 27; ++oc) {
+    const I3 off = off_of(oc);
+    const I3 cj{cp.x + off.x, cp.y + off.y, cp.z + off.z};
+    if (in_grid(P, cj)) S.near_wall[key_of(P, cj)] = 1;
+  }
+}
+
 template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
                                                                   int cpar) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -622,7 +639,8 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
   V4<T> ny = S.cny[i];
   V4<T> vz = S.cvz[i];
   const T th = P.two_h;
-  if (P.npb > 0) {
+  // No contact-wall particle within the 27 cells: the scan would find nothing.
+  if (P.npb > 0 && in_grid(P, celli) && S.near_wall[key_of(P, celli)]) {
     for (int oc = 0; oc < 27; ++oc) {
       const I3 off = off_of(oc);
       const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
@@ -810,15 +828,21 @@ template <class T> RWD void fill_offsets(V4<T>* otab, T th) {
   }
 }
 
-template <bool Strict, class T> RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c,
-                                                      const IState<T>& I, const unsigned* my, int stride, int cnt,
-                                                      const V4<T>* otab, Acc<T>& A) {
+template <bool Strict, class T, bool Kept = false>
+RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const IState<T>& I, const unsigned* my,
+                      int stride, int cnt, const V4<T>* otab, Acc<T>& A) {
   const Rec<T>* __restrict__ rec = S.rec;
   if (cnt <= 0) return;
+  // Kept lists (global memory) are read once per interaction: streaming loads, so they
+  // do not push the neighbour records out of L2.
+  auto entry = [&](int k) -> unsigned {
+    if constexpr (Kept) return __ldcs(my + k);
+    else return my[k];
+  };
   // Entries are read two ahead and records one ahead, so a record's index is in hand
   // when its load is issued.
-  unsigned ent = my[0];
-  unsigned ent1 = cnt > 1 ? my[stride] : 0u;
+  unsigned ent = entry(0);
+  unsigned ent1 = cnt > 1 ? entry(stride) : 0u;
   int oc = (int)(ent >> 27);
   NbVals<T> nb = load_nb(rec, (int)(ent & 0x7ffffffu));
   for (int e = 0; e < cnt; ++e) {
@@ -827,7 +851,7 @@ template <bool Strict, class T> RWD void ix_list_eval(const Params<T>& P, const 
     if (e + 1 < cnt) {
       oc = (int)(ent1 >> 27);
       nb = load_nb(rec, (int)(ent1 & 0x7ffffffu));
-      if (e + 2 < cnt) ent1 = my[(e + 2) * stride];
+      if (e + 2 < cnt) ent1 = entry((e + 2) * stride);
     }
     const V4<T> o = otab[occ];
     pair_eval<Strict>(P, I, V3<T>{I.pos.x - cur.p.x - o.x, I.pos.y - cur.p.y - o.y, I.pos.z - cur.p.z - o.z}, cur, A);
@@ -1002,10 +1026,10 @@ template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const Dev
 //  - walk (Walk = true): in mode 1, walks the kept lists of the other particles.  It
 //    carries no scan state, so it runs with fewer registers.
 #ifndef RW_WALK_MIN_BLOCKS
-#define RW_WALK_MIN_BLOCKS 1  // resident blocks per SM the walk kernel's register budget aims at
+#define RW_WALK_MIN_BLOCKS 0  // resident blocks per SM the walk kernel's register budget aims at (0: none)
 #endif
 template <class T, bool Strict, bool Walk>
-__global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 1)
+__global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
     k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, int cpar) {
   extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread (scan only)
   __shared__ V4<T> otab[27];
@@ -1042,7 +1066,7 @@ __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 1)
   IState<T> I;
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
-  if (Walk) ix_list_eval<Strict>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, otab, A);
+  if (Walk) ix_list_eval<Strict, T, true>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, otab, A);
   else
     ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, otab, A,
                            (mode == 0 && keep) ? t : -1);
