@@ -321,6 +321,7 @@ template <class T> struct Engine final : EngineBase {
     d.time_d = q.time;
     d.time_f = (T)q.time;
     d.npm = q.npm;
+    d.host_dirty = 1;  // soil neighbour records are first written by the corner search
     for (int i = 0; i < P.n_motion; ++i) {
       const rw_motion& m = q.motion[i];
       Table<T>& tb = d.tab[i];
@@ -867,6 +868,7 @@ template <class T> struct Engine final : EngineBase {
     Dyn<T> d = dyn_host();
     d.list_ok = 0;
     d.ix_mode = 0;
+    d.host_dirty = 1;
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     RW_CU(cudaStreamSynchronize(st));
   }
@@ -880,6 +882,7 @@ template <class T> struct Engine final : EngineBase {
     d.np_delete_m = np_delete_m;
     d.list_ok = 0;
     d.ix_mode = 0;
+    d.host_dirty = 1;
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     RW_CU(cudaStreamSynchronize(st));
   }

@@ -371,6 +371,8 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
   // (the integrators raise list_kill); otherwise it scans the cells and keeps new lists.
   // Lists built in the corrector section, from mid-step positions, are not kept.
   if (section >= 0) {
+    if (dyn->need_sort || dyn->host_dirty) dyn->rec_stale = 1;  // until the next interaction
+    dyn->host_dirty = 0;
     const int reuse = (!dyn->need_sort && dyn->list_ok && !dyn->list_kill) ? 1 : 0;
     dyn->ix_mode = reuse;
     dyn->n_reuse += reuse;
@@ -633,14 +635,25 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
   const int4 cp = S.cellpos[c][i];
   const I3 celli{cp.x, cp.y, cp.z};
   V4<T> cv = S.cv[cpar][i];
+  const bool near = P.npb > 0 && in_grid(P, celli) && S.near_wall[key_of(P, celli)];
+  if (!near) {  // no contact-wall particle within the 27 cells: the scan would find nothing
+    if (cv.x != T(0.0f) || cv.y != T(999)) {
+      cv.x = T(0.0f);
+      cv.y = T(999);
+      S.cv[cpar][i] = cv;
+    }
+    if (dyn->rec_stale)
+      write_rec(P, S.rec, i, S.pos[c][i], S.vel[c][i], ld6(S.str_a[c], S.str_b[c], i), S.idm[c][i].y,
+                S.codes[c][i].x >= 10);
+    return;
+  }
   cv.x = T(0.0f);
   cv.y = T(999);
   T d_ij = T(999);
   V4<T> ny = S.cny[i];
   V4<T> vz = S.cvz[i];
   const T th = P.two_h;
-  // No contact-wall particle within the 27 cells: the scan would find nothing.
-  if (P.npb > 0 && in_grid(P, celli) && S.near_wall[key_of(P, celli)]) {
+  {
     for (int oc = 0; oc < 27; ++oc) {
       const I3 off = off_of(oc);
       const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
@@ -679,8 +692,9 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
   S.cv[cpar][i] = cv;
   S.cny[i] = ny;
   S.cvz[i] = vz;
-  write_rec(P, S.rec, i, S.pos[c][i], S.vel[c][i], ld6(S.str_a[c], S.str_b[c], i), S.idm[c][i].y,
-            S.codes[c][i].x >= 10);
+  if (dyn->rec_stale)
+    write_rec(P, S.rec, i, S.pos[c][i], S.vel[c][i], ld6(S.str_a[c], S.str_b[c], i), S.idm[c][i].y,
+              S.codes[c][i].x >= 10);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1036,6 +1050,7 @@ __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
   fill_offsets(otab, P.two_h);
   __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!Walk && t == 0) const_cast<Dyn<T>*>(dyn)->rec_stale = 0;  // the corner search has refreshed the records
   const int total = P.np - P.npb;
   if (t >= total) return;
   const int i = P.npb + t;
@@ -1184,6 +1199,7 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
   __shared__ V4<T> otab[27];
   fill_offsets(otab, P.two_h);
   const int tid = threadIdx.x;
+  if (blockIdx.x == 0 && tid == 0) const_cast<Dyn<T>*>(dyn)->rec_stale = 0;  // records refreshed by the corner search
   // Deleted slots keep their contact state (the chunk list covers live particles only).
   {
     const int npm = dyn->npm;
@@ -1364,6 +1380,7 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
   if (i < P.npb) return;
   const int4 code = S.codes[c][i];
   if (code.y != 1) return;
+  const T mass = S.idm[c][i].y;  // for the neighbour record (read early: the stores below may alias)
   const T hdt = T(0.5f) * P.dt;
   const V4<T> acc = S.accad[i];
   if (P.mixed) {  // compensated half step; the compensation itself is not kept
@@ -1395,6 +1412,7 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
   st6(S.stn_a[c], S.stn_b[c], i, sn);
   st6(S.str_a[c], S.str_b[c], i, sg);
   if (!yld) S.idm[c][i].x = T(100);
+  write_rec(P, S.rec, i, ps, vr, sg, mass, code.x >= 10);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1454,6 +1472,7 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
     return;
   }
   const V4<T> vri = S.vel_ini[ci][i];
+  V4<T> id = S.idm[c][i];  // read early: the stores below may alias
   V4<T> vr, ps;
   V4<T> kp{T(0), T(0), T(0), T(0)}, kv{T(0), T(0), T(0), T(0)};
   if (P.mixed) {  // compensated full step (position and velocity keep their lost low bits)
@@ -1500,7 +1519,6 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
   bool yld = false;
   T mcrt = T(0);
   constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
-  V4<T> id = S.idm[c][i];
   if (!yld) id.x = T(100);
   id.w = mcrt;
   if (!in_grid(P, I3{cp.x, cp.y, cp.z})) {
@@ -1518,6 +1536,7 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
   S.idm[c][i] = id;
   S.pos_ori[c][i] = po;
   S.accad[i] = po;
+  write_rec(P, S.rec, i, ps, vr, sg, id.y, code.x >= 10);
 }
 
 // ---------------------------------------------------------------------------------

@@ -77,7 +77,11 @@ template <class T> struct Dyn {
   // moved too far since the lists were built; build_kill: lists built in this section
   // are not to be kept (a corrector-section rebuild).
   int ix_mode, list_ok, list_kill, build_kill;
-  int n_sorts, n_reuse;      // sections that permuted / corrector sections that reused lists
+  int n_sorts, n_reuse;      // sections that permuted / interactions that walked kept lists
+  // Soil neighbour records: the integrators rewrite them; the corner search rewrites
+  // them after a permutation or a host write (rec_stale: set by the search, cleared by
+  // the interaction that follows).
+  int rec_stale, host_dirty;
   Motion<T> mv[kMotionMax];
   Table<T> tab[kMotionMax];
 };
