@@ -270,6 +270,41 @@ rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen);
 rw_status rw_cell_sort_noalloc(const int32_t* d_keys, int32_t n, int32_t max_key, int32_t* d_sorted_keys,
                                int32_t* d_perm, void* stream);
 
+/* ---------------------------------------------------------------------------------
+ * Learned constitutive closure.  No counterpart in the reference: a surrogate of the
+ * objective (Jaumann-free) part of the HypoCS stress rate (src/constitutive_model.h:269),
+ * a 16-64-64-64-64-6 perceptron with SiLU hidden units, BF16 weights and activations and
+ * FP32 accumulation, evaluated and trained on the tensor cores (tcgen05).
+ *   features  x[16]: stress / p (6), strain rate / |D| (6), relative void ratio
+ *             (e - e_min) / (e_c(p) - e_min), (sin phi_c - 0.556) / 0.087, 0, 0;
+ *   target    t[6]:  R / (p |D|) / 1000, R the objective stress rate.
+ * Parameters (RW_MLP_NPARAM floats): W1[16][64] b1[64] W2[64][64] b2 W3 b3 W4 b4
+ * W5[64][6] b5[6] (y = x W + b).  Host arrays are row-major.
+ * --------------------------------------------------------------------------------- */
+typedef struct rw_mlp rw_mlp;
+#define RW_MLP_IN 16
+#define RW_MLP_OUT 6
+#define RW_MLP_NPARAM 13958
+const char* rw_mlp_last_error(rw_mlp* m);
+/* Xavier-uniform weights from `seed`, zero biases; room for sample_capacity samples. */
+rw_status rw_mlp_create(int device, uint64_t seed, int64_t sample_capacity, rw_mlp** out);
+rw_status rw_mlp_destroy(rw_mlp* m);
+rw_status rw_mlp_get_params(rw_mlp* m, float* out, size_t n);
+rw_status rw_mlp_set_params(rw_mlp* m, const float* in, size_t n);
+/* y[n][6] = net(x[n][16]). */
+rw_status rw_mlp_forward(rw_mlp* m, const float* x, int64_t n, float* y);
+/* Mean squared error over n samples and 6 outputs, and its gradient (RW_MLP_NPARAM). */
+rw_status rw_mlp_grad(rw_mlp* m, const float* x, const float* t, int64_t n, double* loss, float* grad);
+/* Training samples kept on the device. */
+rw_status rw_mlp_add_samples(rw_mlp* m, const float* x, const float* t, int64_t n);
+rw_status rw_mlp_samples(rw_mlp* m, int64_t* count, float* x, float* t, int64_t n);
+rw_status rw_mlp_clear_samples(rw_mlp* m);
+/* Adam (beta 0.9 / 0.999) over the stored samples, shuffled per epoch; *last_loss =
+ * mean squared error over the last epoch. */
+rw_status rw_mlp_train(rw_mlp* m, int epochs, int batch, float lr, uint64_t seed, double* last_loss);
+/* Per-feature minimum / maximum of the stored samples and the largest |target|. */
+rw_status rw_mlp_feature_ranges(rw_mlp* m, float* lo, float* hi, float* tmax);
+
 #ifdef __cplusplus
 }
 #endif

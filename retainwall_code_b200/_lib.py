@@ -20,6 +20,9 @@ EXPORTS = [
     "rw_wall_force", "rw_save", "rw_get_info", "rw_set_option", "rw_get_array", "rw_set_array", "rw_set_counters",
     "rw_profile", "rw_step_timed", "rw_cell_sort_noalloc", "rw_batch_create", "rw_batch_step",
     "rw_batch_synchronize", "rw_batch_destroy", "rw_autotune", "rw_wall_profile",
+    "rw_mlp_last_error", "rw_mlp_create", "rw_mlp_destroy", "rw_mlp_get_params", "rw_mlp_set_params",
+    "rw_mlp_forward", "rw_mlp_grad", "rw_mlp_add_samples", "rw_mlp_samples", "rw_mlp_clear_samples",
+    "rw_mlp_train", "rw_mlp_feature_ranges",
 ]
 STAGE_NAMES = ["search_p", "rigid", "adami_p", "corner_p", "interaction_p", "predictor", "search_c", "adami_c",
                "corner_c", "interaction_c", "corrector"]
@@ -70,6 +73,20 @@ def lib() -> ct.CDLL:
     L.rw_set_array.argtypes = [P, ct.c_int, ct.c_void_p, ct.c_size_t]
     L.rw_set_counters.argtypes = [P, ct.c_double, ct.c_int, ct.c_int, ct.c_int]
     L.rw_profile.argtypes = [P, ct.c_int, ct.POINTER(ct.c_double), ct.c_int, ct.POINTER(ct.c_int)]
+    # learned closure
+    L.rw_mlp_last_error.restype = ct.c_char_p
+    L.rw_mlp_last_error.argtypes = [P]
+    L.rw_mlp_create.argtypes = [ct.c_int, ct.c_uint64, ct.c_int64, ct.POINTER(P)]
+    L.rw_mlp_destroy.argtypes = [P]
+    L.rw_mlp_get_params.argtypes = [P, ct.c_void_p, ct.c_size_t]
+    L.rw_mlp_set_params.argtypes = [P, ct.c_void_p, ct.c_size_t]
+    L.rw_mlp_forward.argtypes = [P, ct.c_void_p, ct.c_int64, ct.c_void_p]
+    L.rw_mlp_grad.argtypes = [P, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.POINTER(ct.c_double), ct.c_void_p]
+    L.rw_mlp_add_samples.argtypes = [P, ct.c_void_p, ct.c_void_p, ct.c_int64]
+    L.rw_mlp_samples.argtypes = [P, ct.POINTER(ct.c_int64), ct.c_void_p, ct.c_void_p, ct.c_int64]
+    L.rw_mlp_clear_samples.argtypes = [P]
+    L.rw_mlp_train.argtypes = [P, ct.c_int, ct.c_int, ct.c_float, ct.c_uint64, ct.POINTER(ct.c_double)]
+    L.rw_mlp_feature_ranges.argtypes = [P, ct.c_void_p, ct.c_void_p, ct.c_void_p]
     _lib = L
     return L
 

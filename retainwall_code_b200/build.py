@@ -18,7 +18,7 @@ CLI = os.path.join(PKG, "loquat")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
-SOURCES = ["rw_engine.cu", "rw_io.cpp", "rw_noalloc.cu"]
+SOURCES = ["rw_engine.cu", "rw_io.cpp", "rw_noalloc.cu", "rw_mlp.cu"]
 
 
 def _nvcc() -> str:
