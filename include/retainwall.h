@@ -40,7 +40,8 @@ enum {
   RW_DERR_CELL_RANGE = 1,   /* a live particle's cell left the grid (reference: out-of-bounds write) */
   RW_DERR_COUNT = 2,        /* particle-count invariant npb+npm+deleted != np (src/loquat_grid.cu:251-254) */
   RW_DERR_LIST = 4,         /* neighbour list exceeded its per-cell capacity (handled, reported)  */
-  RW_DERR_PERM = 8          /* sort produced an index outside [0, np) (guarded; never expected)  */
+  RW_DERR_PERM = 8,         /* sort produced an index outside [0, np) (guarded; never expected)  */
+  RW_DERR_CLOSURE = 16      /* a tensor-core wait of the learned closure gave up                  */
 };
 
 #define RW_MODEL_MAX 10
@@ -304,6 +305,22 @@ rw_status rw_mlp_clear_samples(rw_mlp* m);
 rw_status rw_mlp_train(rw_mlp* m, int epochs, int batch, float lr, uint64_t seed, double* last_loss);
 /* Per-feature minimum / maximum of the stored samples and the largest |target|. */
 rw_status rw_mlp_feature_ranges(rw_mlp* m, float* lo, float* hi, float* tmax);
+/* Appends training samples (features and exact targets) from a context's current state:
+ * every `stride`-th soil particle with a HypoCS update; *added = samples kept (bounded by
+ * the network's free capacity).  The context and the network share a device. */
+rw_status rw_mlp_collect(rw_mlp* m, rw_ctx* ctx, int stride, int64_t* added);
+/* Uses the network for the objective stress rate of this context's HypoCS particles
+ * (NULL: exact updates again).  A particle uses it only when all its features lie within
+ * the ranges of the network's stored samples, each widened by `margin` times its width,
+ * and every output within (1 + margin) times the largest stored |target|; otherwise, and
+ * for the zero-stress reset, the exact update runs.  The Jaumann term, the tension
+ * cut-off and the cone projection stay exact.  Ranges are taken at this call; the
+ * weights are read at every step. */
+rw_status rw_set_closure(rw_ctx* ctx, rw_mlp* m, double margin);
+/* Since rw_set_closure: [0] HypoCS updates offered to the network, [1] updates that used
+ * it, [2] mean and [3] largest relative error (L2 over the six components) of its
+ * objective rate against the exact one, over the updates that used it. */
+rw_status rw_closure_stats(rw_ctx* ctx, double* out);
 
 #ifdef __cplusplus
 }

@@ -22,7 +22,7 @@ EXPORTS = [
     "rw_batch_synchronize", "rw_batch_destroy", "rw_autotune", "rw_wall_profile",
     "rw_mlp_last_error", "rw_mlp_create", "rw_mlp_destroy", "rw_mlp_get_params", "rw_mlp_set_params",
     "rw_mlp_forward", "rw_mlp_grad", "rw_mlp_add_samples", "rw_mlp_samples", "rw_mlp_clear_samples",
-    "rw_mlp_train", "rw_mlp_feature_ranges",
+    "rw_mlp_train", "rw_mlp_feature_ranges", "rw_mlp_collect", "rw_set_closure", "rw_closure_stats",
 ]
 STAGE_NAMES = ["search_p", "rigid", "adami_p", "corner_p", "interaction_p", "predictor", "search_c", "adami_c",
                "corner_c", "interaction_c", "corrector"]
@@ -87,6 +87,9 @@ def lib() -> ct.CDLL:
     L.rw_mlp_clear_samples.argtypes = [P]
     L.rw_mlp_train.argtypes = [P, ct.c_int, ct.c_int, ct.c_float, ct.c_uint64, ct.POINTER(ct.c_double)]
     L.rw_mlp_feature_ranges.argtypes = [P, ct.c_void_p, ct.c_void_p, ct.c_void_p]
+    L.rw_mlp_collect.argtypes = [P, P, ct.c_int, ct.POINTER(ct.c_int64)]
+    L.rw_set_closure.argtypes = [P, P, ct.c_double]
+    L.rw_closure_stats.argtypes = [P, ct.POINTER(ct.c_double)]
     _lib = L
     return L
 

@@ -101,6 +101,16 @@ class Mlp:
         _check(lib().rw_mlp_train(self._h, epochs, batch, lr, seed, ct.byref(loss)), "rw_mlp_train", self._h)
         return loss.value
 
+    def collect(self, sim, stride: int = 1) -> int:
+        """Appends samples from a LoquatSph's current state (every stride-th soil
+        particle); returns how many were kept."""
+        n = ct.c_int64()
+        check_ctx = lib().rw_mlp_collect(self._h, sim.handle, stride, ct.byref(n))
+        if check_ctx != 0:
+            d = lib().rw_last_error(sim.handle)
+            raise RwError(check_ctx, "rw_mlp_collect", d.decode() if d else "")
+        return n.value
+
     def feature_ranges(self):
         lo = np.empty(IN, np.float32)
         hi = np.empty(IN, np.float32)
@@ -108,3 +118,17 @@ class Mlp:
         _check(lib().rw_mlp_feature_ranges(self._h, lo.ctypes.data, hi.ctypes.data, tm.ctypes.data),
                "rw_mlp_feature_ranges", self._h)
         return lo, hi, float(tm[0])
+
+
+def training_run(net: Mlp, case, steps: int, every: int, stride: int = 1, device: int = 0) -> int:
+    """Runs the plain step on ``case`` for ``steps`` steps and stores samples in ``net``
+    every ``every`` steps; returns the number of samples added."""
+    from .sph import LoquatSph
+
+    sim = LoquatSph(case=case, device=device)
+    added = 0
+    for s in range(0, steps, every):
+        sim.step(min(every, steps - s))
+        added += net.collect(sim, stride)
+    sim.close()
+    return added

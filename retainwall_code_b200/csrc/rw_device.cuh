@@ -272,40 +272,68 @@ template <class T> RWD void mat_hypo_basic(T dt, V3<T> om, S6<T> D, S6<T>& sigma
   sigma = dev + ident6<T>() * (sph + coh);
 }
 
-// cuMatModHypo (critical state, HypoCS), src/constitutive_model.h:209-299.
-template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, T& M_crt,
-                                        bool dnorm = false) {
+// cuMatModHypo (critical state, HypoCS), src/constitutive_model.h:209-299, in three
+// pieces so that the learned closure can replace the objective stress rate alone:
+// hypo_cs_pre (state quantities, :211-264), hypo_cs_rate (:269, Jaumann term first, in
+// the reference's order) and hypo_cs_post (tension cut-off and cone projection, :270-298).
+template <class T> struct HypoPre {
+  S6<T> str, dev, jau;
+  T tr_str, tr_D, tr_sD, nD, p, e, e_crt, fd, coh;
+  HypoC<T> c;
+};
+
+// false: the zero-stress reset branch (I1 > -4) was taken and sigma is final.
+template <class T> RWD bool hypo_cs_pre(T density, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, T& M_crt, bool dnorm,
+                                        HypoPre<T>& h) {
   T Ei = mp[0], Vi = mp[1], phi_c = mp[2], coh = mp[3], p_ref = mp[4], void_co = mp[5], lambda = mp[6];
   T xi = mp[7], alpha = mp[8], void_min = mp[9], void_max = mp[10], void_0 = mp[11], rho0 = mp[12];
-  HypoC<T> c = hypo_coef(Ei, Vi, phi_c, p_ref);
+  h.c = hypo_coef(Ei, Vi, phi_c, p_ref);
+  h.coh = coh;
   F9<T> sf = sym2full(sigma);
   if (coh > T(0)) sf = sf - identF<T>() * coh;
-  S6<T> jau = jaumann(om, sf);
-  S6<T> str = full2sym(sf);
-  T I1 = trace(str);
+  h.jau = jaumann(om, sf);
+  h.str = full2sym(sf);
+  T I1 = trace(h.str);
   if ((double)I1 > -4.0) {
     sigma = {T(-1), T(-1), T(-2), T(0), T(0), T(0)};
-    return;
+    return false;
   }
-  S6<T> dev = str - ident6<T>() * (T)((double)I1 / 3.0);
-  T tr_str = trace(str), tr_D = trace(D), tr_sD = trace2(str, D);
-  T nD = rate_norm(D, dnorm);
-  T p = (T)(-(double)I1 / 3.0);
+  h.dev = h.str - ident6<T>() * (T)((double)I1 / 3.0);
+  h.tr_str = trace(h.str);
+  h.tr_D = trace(D);
+  h.tr_sD = trace2(h.str, D);
+  h.nD = rate_norm(D, dnorm);
+  h.p = (T)(-(double)I1 / 3.0);
   T e = (T)((1.0 + (double)void_0) * (double)rho0 / (double)density - 1.0);
   e = f_max(e, void_min);
-  e = f_min(e, void_max);
-  T e_crt = void_co * f_exp(-lambda * f_pow(p / p_ref, xi));
-  T fd = f_pow((e - void_min) / (e_crt - void_min), alpha);
-  M_crt = e - e_crt;
-  S6<T> rate = jau + D * (c.C1 * tr_str) + str * (c.C2 * tr_D) + str * (c.C3 * tr_sD / tr_str) +
-               (str + dev) * (fd * c.C4 * nD);
-  str = sigma + rate * dt;
+  h.e = f_min(e, void_max);
+  h.e_crt = void_co * f_exp(-lambda * f_pow(h.p / p_ref, xi));
+  h.fd = f_pow((h.e - void_min) / (h.e_crt - void_min), alpha);
+  M_crt = h.e - h.e_crt;
+  return true;
+}
+
+// Jaumann term plus the objective rate, as the reference sums them.
+template <class T> RWD S6<T> hypo_cs_rate(const HypoPre<T>& h, S6<T> D) {
+  return h.jau + D * (h.c.C1 * h.tr_str) + h.str * (h.c.C2 * h.tr_D) + h.str * (h.c.C3 * h.tr_sD / h.tr_str) +
+         (h.str + h.dev) * (h.fd * h.c.C4 * h.nD);
+}
+// The objective rate alone (what the learned closure predicts).
+template <class T> RWD S6<T> hypo_cs_objective(const HypoPre<T>& h, S6<T> D) {
+  return D * (h.c.C1 * h.tr_str) + h.str * (h.c.C2 * h.tr_D) + h.str * (h.c.C3 * h.tr_sD / h.tr_str) +
+         (h.str + h.dev) * (h.fd * h.c.C4 * h.nD);
+}
+
+template <class T> RWD void hypo_cs_post(T dt, const HypoPre<T>& h, S6<T> rate, S6<T>& sigma) {
+  const T coh = h.coh, fd = h.fd;
+  const HypoC<T>& c = h.c;
+  S6<T> str = sigma + rate * dt;
   T sph = (T)((double)trace(str) / 3.0);
   if ((double)sph > 0.0) {
     sigma = {(T)(-1.0 + (double)coh), (T)(-1.0 + (double)coh), (T)(-2.0 + (double)coh), T(0), T(0), T(0)};
     return;
   }
-  dev = str - ident6<T>() * sph;
+  S6<T> dev = str - ident6<T>() * sph;
   T fa = c.C2 / c.C1, fb = c.C3 / c.C1, fc = c.C4 / c.C1;
   double t1 = 1.0 + (double)fa + (double)fb / 3.0;
   T A = (T)((double)(fd * fd * fc * fc) / 3.0 - t1 * t1);
@@ -321,6 +349,13 @@ template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T
     dev = dev * ratio;
   }
   sigma = dev + ident6<T>() * (sph + coh);
+}
+
+template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, T& M_crt,
+                                        bool dnorm = false) {
+  HypoPre<T> h;
+  if (!hypo_cs_pre(density, om, D, sigma, mp, M_crt, dnorm, h)) return;
+  hypo_cs_post(dt, h, hypo_cs_rate(h, D), sigma);
 }
 
 // Strain-rate norm sqrt(D:D).  The precision form evaluates it in double (the

@@ -60,6 +60,9 @@ struct EngineBase {
   virtual cudaGraph_t step_graph() = 0;
   virtual cudaStream_t stream() const = 0;
   virtual int soil_count() = 0;
+  virtual int set_closure(rw_mlp* net, double margin) = 0;
+  virtual void closure_stats(double* out) = 0;
+  virtual long long collect(rw_mlp* net, int stride) = 0;
 };
 
 static inline unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -80,6 +83,11 @@ template <class T> struct Engine final : EngineBase {
   rw_case_params cparams{};
   int output_number = 0;
   int saves = 0;  // the first save is RunSimulation's initial output
+  rw_mlp* cl_net = nullptr;  // learned closure (P.closure), its trust region and statistics
+  ClosureTrust cl_trust{};
+  double* d_clstats = nullptr;
+  unsigned long long* d_count = nullptr;
+  int nsm = 148;
 
   ~Engine() override {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -268,6 +276,9 @@ template <class T> struct Engine final : EngineBase {
       S.nbg_cnt = dalloc<int>(np - npb);
     }
     S.dacc = dalloc<float>(np);
+    d_clstats = dalloc<double>(4);
+    d_count = dalloc<unsigned long long>(1);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     RW_CU(cudaMemsetAsync(S.dacc, 0, np * sizeof(float), st));
     d_dyn = dalloc<Dyn<T>>(1);
 
@@ -452,10 +463,84 @@ template <class T> struct Engine final : EngineBase {
   void predictor() override {
     k_predictor<T><<<nblk(P.np, 256), 256, 0, st>>>(P, S, d_dyn);
     check_launch();
+    if (P.closure) launch_closure(0);
   }
   void corrector() override {
     k_corrector<T><<<nblk(P.npb + P.npm0, 256), 256, 0, st>>>(P, S, d_dyn);
     check_launch();
+    if (P.closure) launch_closure(1);
+  }
+  void launch_closure(int stage) {
+    const long tiles = nblk(P.npm0, mlp::TILE);
+    const unsigned grid = (unsigned)std::max(1L, std::min(tiles, 4L * nsm));
+    k_closure<T><<<grid, mlp::TILE, sizeof(mlp::FwdSmem), st>>>(P, S, d_dyn, mlp::net_view(cl_net), cl_trust,
+                                                                 d_clstats, stage);
+    check_launch();
+  }
+
+  // ------------------------------------------------------------------------------
+  // Learned closure.
+  // ------------------------------------------------------------------------------
+  int set_closure(rw_mlp* net, double margin) override {
+    if (gexec) {  // the closure launches are part of the captured step
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    if (!net) {
+      P.closure = 0;
+      cl_net = nullptr;
+      return RW_OK;
+    }
+    if (mlp::device_of(net) != device) {
+      err = "rw_set_closure: the network lives on another device";
+      return RW_EINVAL;
+    }
+    float lo[mlp::IN], hi[mlp::IN], tmax = 0.0f;
+    const rw_status s = rw_mlp_feature_ranges(net, lo, hi, &tmax);
+    if (s != RW_OK) {
+      err = std::string("rw_set_closure: ") + rw_mlp_last_error(net);
+      return s;
+    }
+    for (int k = 0; k < mlp::IN; ++k) {
+      const float w = hi[k] - lo[k];
+      cl_trust.lo[k] = lo[k] - (float)margin * w;
+      cl_trust.hi[k] = hi[k] + (float)margin * w;
+    }
+    cl_trust.out_max = tmax * (1.0f + (float)margin);
+    RW_CU(cudaSetDevice(device));
+    RW_CU(cudaFuncSetAttribute(k_closure<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(mlp::FwdSmem)));
+    RW_CU(cudaMemsetAsync(d_clstats, 0, 4 * sizeof(double), st));
+    RW_CU(cudaStreamSynchronize(st));
+    P.closure = 1;
+    cl_net = net;
+    return RW_OK;
+  }
+  void closure_stats(double* out) override {
+    double s[4];
+    RW_CU(cudaMemcpyAsync(s, d_clstats, sizeof(s), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaStreamSynchronize(st));
+    out[0] = s[0];
+    out[1] = s[1];
+    out[2] = s[1] > 0 ? s[2] / s[1] : 0.0;
+    out[3] = s[3];
+  }
+  long long collect(rw_mlp* net, int stride) override {
+    if (mlp::device_of(net) != device) throw Fail(RW_EINVAL, "rw_mlp_collect: the network lives on another device");
+    const long long avail = mlp::free_slots(net);
+    if (avail <= 0) return 0;
+    float *x = nullptr, *t = nullptr;
+    mlp::next_slot(net, &x, &t);
+    RW_CU(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st));
+    const long n = (P.npm0 + stride - 1) / stride;
+    k_collect<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn, x, t, avail, d_count, stride);
+    check_launch();
+    unsigned long long cnt = 0;
+    RW_CU(cudaMemcpyAsync(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaStreamSynchronize(st));
+    const long long added = std::min((long long)cnt, avail);
+    mlp::commit(net, added);
+    return added;
   }
 
   // One whole step (RunSimulation's loop body, src/loquat.cu:548-561).
@@ -522,6 +607,7 @@ template <class T> struct Engine final : EngineBase {
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
     if (P.stress_shepard_filter != 0) k += 2;
+    if (P.closure) k += 2;
     if (P.npb == 0) k -= 2;
     return k;
   }
@@ -1259,6 +1345,28 @@ rw_status rw_batch_destroy(rw_batch* b) {
   cudaSetDevice(b->b.device);
   delete b;
   return RW_OK;
+}
+
+rw_status rw_set_closure(rw_ctx* ctx, rw_mlp* net, double margin) {
+  if (!(margin >= 0.0)) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) { return (rw_status)e.set_closure(net, margin); });
+}
+
+rw_status rw_closure_stats(rw_ctx* ctx, double* out) {
+  if (!out) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) {
+    e.closure_stats(out);
+    return RW_OK;
+  });
+}
+
+rw_status rw_mlp_collect(rw_mlp* net, rw_ctx* ctx, int stride, int64_t* added) {
+  if (!net || stride < 1) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) {
+    const long long a = e.collect(net, stride);
+    if (added) *added = a;
+    return RW_OK;
+  });
 }
 
 rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen) {

@@ -5,6 +5,7 @@
 // per layer and neighbour reads of consecutive particles hit the same lines.
 #pragma once
 #include "rw_device.cuh"
+#include "rw_mlp.cuh"
 #include "rw_params.h"
 
 namespace rw {
@@ -1406,13 +1407,14 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
   sn = sn + D * hdt;
   bool yld = false;
   T mcrt = T(0);
-  constitutive(code.z, mp, hdt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
+  const bool by_closure = P.closure && code.z == RW_MODEL_HYPO_CS;  // k_closure updates the stress
+  if (!by_closure) constitutive(code.z, mp, hdt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
   S.pos[c][i] = ps;
   S.vel[c][i] = vr;
   st6(S.stn_a[c], S.stn_b[c], i, sn);
   st6(S.str_a[c], S.str_b[c], i, sg);
   if (!yld) S.idm[c][i].x = T(100);
-  write_rec(P, S.rec, i, ps, vr, sg, mass, code.x >= 10);
+  if (!by_closure) write_rec(P, S.rec, i, ps, vr, sg, mass, code.x >= 10);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1518,7 +1520,8 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
   const S6<T> sn = ld6(S.stni_a[ci], S.stni_b[ci], i) + D * P.dt;
   bool yld = false;
   T mcrt = T(0);
-  constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
+  const bool by_closure = P.closure && code.z == RW_MODEL_HYPO_CS;  // k_closure updates the stress
+  if (!by_closure) constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
   if (!yld) id.x = T(100);
   id.w = mcrt;
   if (!in_grid(P, I3{cp.x, cp.y, cp.z})) {
@@ -1536,7 +1539,7 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
   S.idm[c][i] = id;
   S.pos_ori[c][i] = po;
   S.accad[i] = po;
-  write_rec(P, S.rec, i, ps, vr, sg, id.y, code.x >= 10);
+  if (!by_closure) write_rec(P, S.rec, i, ps, vr, sg, id.y, code.x >= 10);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1698,6 +1701,189 @@ static __global__ void k_wall_force_final(double* wsum, int nblocks) {
   for (int b = 0; b < nblocks; ++b)
     for (int k = 0; k < 3; ++k) a[k] += wsum[3 * b + k];
   for (int k = 0; k < 3; ++k) wsum[3 * nblocks + k] = a[k];
+}
+
+// ---------------------------------------------------------------------------------
+// Learned constitutive closure (no counterpart in the reference): samples for its
+// training and its use inside the step.  Features and target as in rw_mlp.cuh.
+// ---------------------------------------------------------------------------------
+struct ClosureTrust {
+  float lo[mlp::IN], hi[mlp::IN];  // accepted feature ranges
+  float out_max;                   // accepted |output|
+};
+
+template <class T> RWD void closure_features(const HypoPre<T>& h, const S6<T>& D, const T* mp, float* f) {
+  const T ip = T(1) / h.p, inD = T(1) / h.nD;
+  f[0] = (float)(h.str.xx * ip);
+  f[1] = (float)(h.str.yy * ip);
+  f[2] = (float)(h.str.zz * ip);
+  f[3] = (float)(h.str.xy * ip);
+  f[4] = (float)(h.str.xz * ip);
+  f[5] = (float)(h.str.yz * ip);
+  f[6] = (float)(D.xx * inD);
+  f[7] = (float)(D.yy * inD);
+  f[8] = (float)(D.zz * inD);
+  f[9] = (float)(D.xy * inD);
+  f[10] = (float)(D.xz * inD);
+  f[11] = (float)(D.yz * inD);
+  const T void_min = mp[9];
+  f[12] = (float)((h.e - void_min) / (h.e_crt - void_min));
+  f[13] = ((float)f_sin(mp[2]) - mlp::SIN_MID) / mlp::SIN_HALF;
+  f[14] = 0.0f;
+  f[15] = 0.0f;
+}
+
+template <class T> RWD S6<T> closure_scale_out(const HypoPre<T>& h, const float* y) {
+  const T sc = h.p * h.nD * (T)mlp::TARGET_SCALE;
+  return S6<T>{(T)y[0] * sc, (T)y[1] * sc, (T)y[2] * sc, (T)y[3] * sc, (T)y[4] * sc, (T)y[5] * sc};
+}
+
+// Appends (features, exact normalised objective rate) of every stride-th soil particle
+// with a HypoCS update, from the current stress, strain rate and density.
+template <class T> __global__ void k_collect(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, float* X, float* Tg,
+                                             long long cap, unsigned long long* count, int stride) {
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) * stride;
+  const int npm = dyn->npm, c = dyn->cur_main;
+  bool ok = false;
+  float f[mlp::IN], tg[mlp::OUT];
+  if (t < npm) {
+    const int i = P.npb + t;
+    const int4 code = S.codes[c][i];
+    if (code.y == 1 && code.z == RW_MODEL_HYPO_CS) {
+      const T* mp = P.model_par[code.w];
+      const S6<T> D = ld6(S.ace_a, S.ace_b, i);
+      S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
+      HypoPre<T> h;
+      T mcrt;
+      if (hypo_cs_pre(S.vel[c][i].w, V3<T>{T(0), T(0), T(0)}, D, sg, mp, mcrt, P.mixed != 0, h) && h.nD > T(0)) {
+        closure_features(h, D, mp, f);
+        const S6<T> R = hypo_cs_objective(h, D);
+        const T sc = T(1) / (h.p * h.nD * (T)mlp::TARGET_SCALE);
+        tg[0] = (float)(R.xx * sc);
+        tg[1] = (float)(R.yy * sc);
+        tg[2] = (float)(R.zz * sc);
+        tg[3] = (float)(R.xy * sc);
+        tg[4] = (float)(R.xz * sc);
+        tg[5] = (float)(R.yz * sc);
+        ok = true;
+#pragma unroll
+        for (int k = 0; k < mlp::IN; ++k) ok = ok && isfinite(f[k]);
+#pragma unroll
+        for (int o = 0; o < mlp::OUT; ++o) ok = ok && isfinite(tg[o]);
+      }
+    }
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, ok);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (!ok) return;
+  const long long idx = (long long)base + __popc(mask & ((1u << lane) - 1u));
+  if (idx >= cap) return;
+#pragma unroll
+  for (int k = 0; k < mlp::IN; ++k) X[idx * mlp::IN + k] = f[k];
+#pragma unroll
+  for (int o = 0; o < mlp::OUT; ++o) Tg[idx * mlp::OUT + o] = tg[o];
+}
+
+// The HypoCS updates of one integrator stage (0: predictor half step, 1: corrector full
+// step) with the learned objective rate: 128 soil slots per tile on the tensor cores;
+// the Jaumann term, the cut-offs and every particle outside the trust region (or whose
+// output leaves it) stay exact.  Every closure update is judged against the exact rate:
+// stats = [offered, used, sum of relative errors, largest relative error].
+template <class T>
+__global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevState<T> S, Dyn<T>* dyn, mlp::Net net,
+                                                        ClosureTrust tr, double* stats, int stage) {
+  extern __shared__ __align__(128) unsigned char raw[];
+  mlp::FwdSmem& sm = *reinterpret_cast<mlp::FwdSmem*>(raw);
+  mlp::load_fwd(sm, net);
+  if (threadIdx.x == 0) sm.err = 0;
+  mlp::block_setup(&sm.bar, &sm.tmem, 64);
+  const int npm = dyn->npm, c = dyn->cur_main;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const T dt = stage == 0 ? T(0.5f) * P.dt : P.dt;
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile * mlp::TILE < npm; tile += gridDim.x) {
+    const int t = tile * mlp::TILE + tid, i = P.npb + t;
+    bool mine = false, act = false;
+    float f[mlp::IN];
+#pragma unroll
+    for (int k = 0; k < mlp::IN; ++k) f[k] = 0.0f;
+    int4 code{0, 0, 0, 0};
+    if (t < npm) {
+      code = S.codes[c][i];
+      mine = code.y == 1 && code.z == RW_MODEL_HYPO_CS;
+      if (mine) {
+        const T* mp = P.model_par[code.w];
+        const S6<T> D = ld6(S.ace_a, S.ace_b, i);
+        S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
+        HypoPre<T> h;
+        T mcrt;
+        if (hypo_cs_pre(S.vel[c][i].w, V3<T>{T(0), T(0), T(0)}, D, sg, mp, mcrt, P.mixed != 0, h) && h.nD > T(0)) {
+          closure_features(h, D, mp, f);
+          act = true;
+#pragma unroll
+          for (int k = 0; k < mlp::IN; ++k) act = act && f[k] >= tr.lo[k] && f[k] <= tr.hi[k];
+          if (!act)
+#pragma unroll
+            for (int k = 0; k < mlp::IN; ++k) f[k] = 0.0f;
+        }
+      }
+    }
+    mlp::store_row<mlp::IN>(sm.x, tid, f);
+    float y[mlp::OUT];
+    mlp::forward_tile(sm, 0, phase, y);
+    float used = 0.0f, offered = 0.0f, err = 0.0f;
+    if (mine) {
+      const T* mp = P.model_par[code.w];
+      const S6<T> D = ld6(S.ace_a, S.ace_b, i);
+      const V4<T> om4 = S.spin[i];
+      S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
+      HypoPre<T> h;
+      T mcrt = T(0);
+      if (hypo_cs_pre(S.vel[c][i].w, V3<T>{om4.x, om4.y, om4.z}, D, sg, mp, mcrt, P.mixed != 0, h)) {
+        S6<T> rate;
+        bool use = act && !sm.err;
+#pragma unroll
+        for (int o = 0; o < mlp::OUT; ++o) use = use && fabsf(y[o]) <= tr.out_max;
+        if (h.nD > T(0)) offered = 1.0f;
+        if (use) {
+          const S6<T> Rm = closure_scale_out(h, y);
+          const S6<T> Rx = hypo_cs_objective(h, D);
+          const S6<T> d = Rm - Rx;
+          const T nx = f_sqrt(trace2(Rx, Rx)), nd = f_sqrt(trace2(d, d));
+          err = (float)(nd / (nx + T(1e-30)));
+          used = 1.0f;
+          rate = h.jau + Rm;
+        } else {
+          rate = hypo_cs_rate(h, D);
+        }
+        hypo_cs_post(dt, h, rate, sg);
+      }
+      st6(S.str_a[c], S.str_b[c], i, sg);
+      if (stage == 1) S.idm[c][i].w = mcrt;
+      write_rec(P, S.rec, i, S.pos[c][i], S.vel[c][i], sg, S.idm[c][i].y, code.x >= 10);
+    }
+    // statistics: one atomic per warp and counter
+    float so = offered, su = used, se = err, sx = err;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      so += __shfl_xor_sync(0xffffffffu, so, o);
+      su += __shfl_xor_sync(0xffffffffu, su, o);
+      se += __shfl_xor_sync(0xffffffffu, se, o);
+      sx = fmaxf(sx, __shfl_xor_sync(0xffffffffu, sx, o));
+    }
+    if (lane == 0 && so > 0.0f) {
+      atomicAdd(&stats[0], (double)so);
+      atomicAdd(&stats[1], (double)su);
+      atomicAdd(&stats[2], (double)se);
+      atomicMax(reinterpret_cast<unsigned long long*>(&stats[3]), (unsigned long long)__double_as_longlong((double)sx));
+    }
+  }
+  mlp::block_teardown(sm.tmem, 64);
+  if (tid == 0 && sm.err) atomicOr(&dyn->err, 16u);
 }
 
 }  // namespace rw

@@ -686,14 +686,11 @@ namespace rw {
 namespace mlp {
 Net net_view(const rw_mlp* m) { return net_of(m); }
 int device_of(const rw_mlp* m) { return m->device; }
-// Reserves n sample slots; returns the device pointers of the first one (or false).
-bool reserve(rw_mlp* m, long long n, float** x, float** t, long long* first) {
-  if (m->n + n > m->cap) return false;
-  *first = m->n;
+long long free_slots(const rw_mlp* m) { return m->cap - m->n; }
+void next_slot(rw_mlp* m, float** x, float** t) {
   *x = m->sx + m->n * IN;
   *t = m->stg + m->n * OUT;
-  return true;
 }
-void commit(rw_mlp* m, long long n) { m->n += n; }
+void commit(rw_mlp* m, long long n) { m->n += std::min(n, m->cap - m->n); }
 }  // namespace mlp
 }  // namespace rw

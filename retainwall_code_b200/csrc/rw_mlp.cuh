@@ -19,6 +19,8 @@
 
 #include "rw_tc.cuh"
 
+struct rw_mlp;
+
 namespace rw {
 namespace mlp {
 
@@ -194,6 +196,14 @@ __device__ __forceinline__ void block_teardown(uint32_t tmem, uint32_t ncols) {
     tc::tmem_dealloc(tmem, ncols);
   }
 }
+
+// Host-side access of the time step to a network object (defined in rw_mlp.cu).
+Net net_view(const rw_mlp* m);
+int device_of(const rw_mlp* m);
+long long free_slots(const rw_mlp* m);
+// Device pointers of the next free sample slot.
+void next_slot(rw_mlp* m, float** x, float** t);
+void commit(rw_mlp* m, long long n);
 
 }  // namespace mlp
 }  // namespace rw

@@ -57,6 +57,7 @@ template <class T> struct Params {
   float disp_lim;            // a particle's displacement since the lists were built may not pass this
   float disp_eps;            // rounding allowance added per position update
   int keep_lists;            // 0: every interaction scans the cells
+  int closure;               // 1: HypoCS stress updates by the learned closure (k_closure)
   int mixed;                 // precision form: compensated integration, FP64 strain-rate norm
   int pad_m;
 };

@@ -56,6 +56,20 @@ class LoquatSph:
     def _c(self, st: int, what: str) -> None:
         check(st, what, self._h)
 
+    @property
+    def handle(self):
+        return self._h
+
+    # -- learned closure ----------------------------------------------------------------
+    def set_closure(self, net=None, margin: float = 0.0) -> None:
+        """Use ``net`` (closure.Mlp) for the HypoCS objective stress rate (None: exact)."""
+        self._c(lib().rw_set_closure(self._h, net.handle if net is not None else None, margin), "rw_set_closure")
+
+    def closure_stats(self) -> dict:
+        out = (ct.c_double * 4)()
+        self._c(lib().rw_closure_stats(self._h, out), "rw_closure_stats")
+        return {"offered": out[0], "used": out[1], "mean_rel_err": out[2], "max_rel_err": out[3]}
+
     # -- the reference's stage methods --------------------------------------------------
     def step_calculation(self):
         self._c(lib().rw_begin_step(self._h), "rw_begin_step")

@@ -1,0 +1,117 @@
+"""The learned closure inside the step: samples collected from the live state against a
+float64 restatement of the HypoCS objective rate (src/constitutive_model.h:211-269), the
+trust-region fallback, and a trained network in the step against the plain method."""
+import numpy as np
+import pytest
+
+from retainwall_code_b200 import LoquatSph, cases as C
+from retainwall_code_b200.closure import Mlp, training_run
+from tests._util import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _objective_np(sig, D, rho, mp):
+    """Features and normalised objective rate, float64 (the reference's expressions)."""
+    Ei, Vi, phi, coh, pref, eco, lam, xi, alpha, emin, emax, e0, rho0 = [float(v) for v in mp[:13]]
+    C1 = -Ei / (3.0 * pref * (1.0 + Vi))
+    a = 3.0 / (np.sqrt(2.0) * np.sin(phi))
+    C2 = C1 * ((3.0 * Vi + a * np.sqrt(1.0 + Vi * Vi)) / (1.0 - Vi) - a * a / 3.0)
+    C3, C4 = a * a * C1, a * C1
+    s = sig.astype(np.float64).copy()
+    s[:, :3] -= coh
+    D = D.astype(np.float64)
+    I1 = s[:, :3].sum(1)
+    p = -I1 / 3.0
+    dev = s.copy()
+    dev[:, :3] -= (I1 / 3.0)[:, None]
+    trD = D[:, :3].sum(1)
+    trsD = (s[:, :3] * D[:, :3]).sum(1) + 2.0 * (s[:, 3:] * D[:, 3:]).sum(1)
+    nD = np.sqrt((D[:, :3] ** 2).sum(1) + 2.0 * (D[:, 3:] ** 2).sum(1))
+    e = np.clip((1.0 + e0) * rho0 / rho.astype(np.float64) - 1.0, emin, emax)
+    ecrt = eco * np.exp(-lam * (p / pref) ** xi)
+    psi = (e - emin) / (ecrt - emin)
+    fd = psi ** alpha
+    R = (D * (C1 * I1)[:, None] + s * (C2 * trD)[:, None] + s * (C3 * trsD / I1)[:, None]
+         + (s + dev) * (fd * C4 * nD)[:, None])
+    f = np.zeros((len(s), 16))
+    f[:, 0:6] = s / p[:, None]
+    f[:, 6:12] = D / nD[:, None]
+    f[:, 12] = psi
+    f[:, 13] = (np.sin(np.float32(phi)) - 0.556) / 0.087
+    return f, R / (p * nD)[:, None] / 1000.0
+
+
+def test_collected_samples_match_float64_restatement():
+    c = C.column_collapse(nx=8, ny=8, nz=16, runout=1.0)
+    s = LoquatSph(case=c)
+    s.step(3)
+    net = Mlp(sample_capacity=100_000)
+    added = net.collect(s, stride=1)
+    inf = s.info()
+    assert 0 < added <= inf.npm
+    x, t = net.samples()
+    # the same particles from the exported state: soil rows in slot order
+    sig = s.get("str")[inf.npb:inf.npb + inf.npm]
+    D = s.get("acestn")[inf.npb:inf.npb + inf.npm]
+    rho = s.get("velrhop")[inf.npb:inf.npb + inf.npm, 3]
+    mp = np.array([c.params[f"model-0-par-{j}"] for j in range(15)])
+    f, tgt = _objective_np(sig, D, rho, mp)
+    # collection order follows the warps: match each sample to its particle by features
+    from scipy.spatial import cKDTree
+
+    dist, idx = cKDTree(f).query(x.astype(np.float64))
+    assert len(np.unique(idx)) == len(idx)
+    assert dist.max() < 1e-4
+    assert rel(x, f[idx]) < 1e-5
+    assert rel(t, tgt[idx]) < 1e-4
+
+
+def test_closure_falls_back_outside_trust_region():
+    """A network whose outputs leave the trust region is never used: the step equals the
+    plain method (the exact update runs in the closure kernel instead)."""
+    c = C.column_collapse(nx=8, ny=8, nz=16, runout=1.0)
+    plain = LoquatSph(case=c)
+    net = Mlp(seed=3, sample_capacity=100_000)
+    training_run(net, c, steps=4, every=2)
+    p = net.params()
+    p[-6:] = 1e6  # output biases far beyond every stored target
+    net.set_params(p)
+    clo = LoquatSph(case=c)
+    clo.set_closure(net, margin=0.0)
+    plain.step(10)
+    clo.step(10)
+    st = clo.closure_stats()
+    assert st["offered"] > 0 and st["used"] == 0
+    for key in ("pospres", "velrhop", "str", "cellpos"):
+        a, b = clo.get(key), plain.get(key)
+        if key == "cellpos":
+            np.testing.assert_array_equal(a, b)
+        else:
+            assert rel(a, b) < 1e-6, (key, rel(a, b))
+    assert clo.info().device_err == 0
+
+
+def test_trained_closure_tracks_the_plain_method():
+    """A network trained on samples of plain runs (several friction angles and void
+    ratios) drives the HypoCS updates of a new case; the states stay close to the plain
+    run and the judged error of the objective rate is reported."""
+    net = Mlp(seed=7, sample_capacity=2_000_000)
+    for phi, e0, seed in ((30.0, 0.70, 1), (34.0, 0.62, 2), (28.0, 0.76, 3)):
+        training_run(net, C.column_collapse(nx=12, ny=12, nz=24, phi_c=phi, e0=e0, seed=seed, runout=1.0),
+                     steps=60, every=3)
+    n = net.sample_count()
+    assert n > 100_000
+    loss = net.train(epochs=30, batch=128 * 148, lr=2e-3, seed=1)
+    c = C.column_collapse(nx=12, ny=12, nz=24, phi_c=31.0, e0=0.68, seed=9, runout=1.0)
+    plain = LoquatSph(case=c)
+    clo = LoquatSph(case=c)
+    clo.set_closure(net, margin=0.05)
+    plain.step(40)
+    clo.step(40)
+    st = clo.closure_stats()
+    assert st["used"] > 0.5 * st["offered"], st
+    assert st["mean_rel_err"] < 0.1, (st, loss)
+    assert rel(clo.get("pos_abs"), plain.get("pos_abs")) < 1e-5
+    assert rel(clo.get("str"), plain.get("str")) < 5e-2
+    assert clo.info().device_err == 0
