@@ -442,6 +442,141 @@ def precision_report(args):
     print(json.dumps(out), flush=True)
 
 
+def closure_accuracy(net, steps, device):
+    """FP64 runs against plain FP32 and FP32 with the learned closure, same seeds: the
+    column collapse (config 1's case) for positions and stress invariants, a 41k
+    retaining wall for the wall resultant (largest deviation over the run)."""
+    import numpy as np
+
+    from retainwall_code_b200 import LoquatSph, cases as C
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
+
+    out = {"steps": steps}
+    for name, case in (("column_collapse_27648", C.column_collapse()),
+                       ("retaining_wall_41472", C.retaining_wall(nx=48, ny=24, nz=36, dx=0.0025))):
+        res = {}
+        for mode in ("f64", "f32", "closure"):
+            sim = LoquatSph(case=case, precision=8 if mode == "f64" else 4, device=device)
+            if mode == "closure":
+                sim.set_closure(net, margin=0.05)
+            x0 = sim.get("pos_abs")[:, :3].astype(np.float64)
+            wf, done, chunk = [], 0, max(1, steps // 20)
+            while done < steps:
+                n = min(chunk, steps - done)
+                sim.step(n)
+                done += n
+                wf.append(sim.wall_force(0)[0])
+            inf = sim.info()
+            mat = slice(inf.npb, inf.npb + inf.npm)
+            res[mode] = dict(x=sim.get("pos_abs")[:, :3].astype(np.float64)[mat], x0=x0[mat], sig=sim.get("str")[mat],
+                             wf=np.array(wf), stats=sim.closure_stats() if mode == "closure" else None)
+            sim.close()
+        ref = res["f64"]
+        p64, q64 = invariants(ref["sig"])
+        entry = {}
+        for mode in ("f32", "closure"):
+            r = res[mode]
+            p, q = invariants(r["sig"])
+            entry[mode] = {"displacement_rel_l2": rel(r["x"] - r["x0"], ref["x"] - ref["x0"]),
+                           "p_rel_l2": rel(p, p64), "q_rel_l2": rel(q, q64)}
+            if np.abs(ref["wf"]).max() > 0:
+                entry[mode]["wall_force_max_rel"] = float(np.max(np.abs(r["wf"] - ref["wf"])) /
+                                                          np.abs(ref["wf"]).max())
+        entry["closure"]["judged"] = res["closure"]["stats"]
+        out[name] = entry
+    return out
+
+
+def run_closure(args, ws, rank, local):
+    """The learned-closure form: a network trained on plain runs of the column collapse
+    and retaining-wall configurations (phi_c 28-40 deg, e0 0.55-0.80), then the 1.92M
+    retaining wall stepped with and without it.  value = particle-updates/s with the
+    closure; the plain throughput, the closure's judged error, its fallback share and the
+    wall force against the plain run are reported beside it."""
+    import numpy as np
+
+    from retainwall_code_b200 import LoquatSph, cases as C
+    from retainwall_code_b200.closure import Mlp, training_run
+
+    net = Mlp(device=local, seed=1, sample_capacity=args.closure_samples)
+    t0 = time.perf_counter()
+    runs = 0
+    while net.sample_count() < args.closure_samples:
+        # low-discrepancy sweep of the friction angle and the initial void ratio, so that
+        # a few runs already span both ranges (end points first)
+        u = (0.0, 1.0)[runs] if runs < 2 else (runs * 0.6180339887) % 1.0
+        v = (1.0, 0.0)[runs] if runs < 2 else (runs * 0.7548776662) % 1.0
+        phi, e0 = 28.0 + 12.0 * u, 0.55 + 0.25 * v
+        if runs % 2 == 0:  # the column collapse (24 x 24 x 48, 5 mm), every 2nd particle
+            case, stride = C.column_collapse(phi_c=phi, e0=e0, seed=100 + runs), 2
+        else:  # a retaining wall of the batched sweep's kind (102k soil particles), every 16th
+            mode = ("active", "passive", "rotation")[runs % 3]
+            case = C.retaining_wall(nx=80, ny=32, nz=40, dx=0.004, phi_c=phi, e0=e0, mode=mode, seed=100 + runs)
+            stride = 16
+        training_run(net, case, steps=args.closure_run_steps, every=max(4, args.closure_run_steps // 100),
+                     stride=stride, device=local, seed=runs)
+        runs += 1
+    collect_s = time.perf_counter() - t0
+    n_samples = net.sample_count()
+    t0 = time.perf_counter()
+    loss = net.train(epochs=args.closure_epochs, batch=8192, lr=2e-3, seed=1)
+    train_s = time.perf_counter() - t0
+
+    acc = closure_accuracy(net, args.closure_acc_steps, local)
+    case, cfg = make_case("wall2")
+    res = {}
+    for mode in ("plain", "closure"):
+        sim = LoquatSph(case=case, device=local)
+        if mode == "closure":
+            sim.set_closure(net, margin=0.05)
+        sim.step(args.warmup)
+        sim.synchronize()
+        barrier(ws)
+        with ClockSampler(local) as clk:
+            ms = sim.step_timed(args.steps)
+        ms = allreduce_max(ms, ws)
+        stages, kps = sim.profile(3)
+        res[mode] = {"ms": ms, "npm": sim.info().npm, "stages": stages, "kps": kps, "clocks": clk.summary(),
+                     "wall_force_N": float(sim.wall_force(0)[0]), "stats": sim.closure_stats(),
+                     "err": sim.info().device_err}
+        sim.close()
+    npm = res["closure"]["npm"]
+    value = ws * npm * args.steps / (res["closure"]["ms"] * 1e-3)
+    plain = ws * res["plain"]["npm"] * args.steps / (res["plain"]["ms"] * 1e-3)
+    st = res["closure"]["stats"]
+    # tensor work of one closure launch: 128-row tiles of five layers (K, N padded)
+    macs = 16 * 64 + 3 * 64 * 64 + 64 * 16
+    extra_ms = 0.5 * ((res["closure"]["stages"]["predictor"] - res["plain"]["stages"]["predictor"]) +
+                      (res["closure"]["stages"]["corrector"] - res["plain"]["stages"]["corrector"]))
+    pk, kind = peaks()
+    tflops = 2.0 * macs * npm / (max(extra_ms, 1e-6) * 1e-3) / 1e12
+    wf_p, wf_c = res["plain"]["wall_force_N"], res["closure"]["wall_force_N"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC + " (learned closure)", "value": value, "unit": "particle-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["closure"]["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+            "data": "synthetic (seeded generator)", "config": dict(cfg, parallelism=f"replicas x{ws}"),
+            "plain": {"value": plain, "ms_per_step": res["plain"]["ms"] / args.steps},
+            "closure": {"offered": st["offered"], "used": st["used"],
+                        "used_share": st["used"] / max(st["offered"], 1.0), "mean_rel_err": st["mean_rel_err"],
+                        "max_rel_err": st["max_rel_err"],
+                        "wall_force_rel_diff_vs_plain": abs(wf_c - wf_p) / max(abs(wf_p), 1e-30),
+                        "extra_ms_per_launch": extra_ms,
+                        "tensor_roofline": {"bound": "tensor", "achieved": tflops, "peak": pk["bf16_tflops"] * 1.0,
+                                            "unit": "TFLOP/s", "frac": tflops / pk["bf16_tflops"],
+                                            "note": "two launches per step; MACs of the padded 16-64-64-64-64-16 net"}},
+            "accuracy_vs_fp64": acc,
+            "training": {"samples": n_samples, "runs": runs, "collect_s": collect_s, "epochs": args.closure_epochs,
+                         "train_s": train_s, "samples_per_s": n_samples * args.closure_epochs / train_s,
+                         "final_mse": loss},
+            "stage_ms": res["closure"]["stages"], "gpu_launches": res["closure"]["kps"] * args.steps,
+            "clocks": res["closure"]["clocks"], "device_err": res["closure"]["err"],
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -457,6 +592,10 @@ def main():
     ap.add_argument("--precision-report", action="store_true", help="precision form vs FP64 (configs 1 and 3)")
     ap.add_argument("--precision-steps", type=int, default=2000)
     ap.add_argument("--batch-cases", type=int, default=64)
+    ap.add_argument("--closure-samples", type=int, default=10_000_000)
+    ap.add_argument("--closure-epochs", type=int, default=20)
+    ap.add_argument("--closure-run-steps", type=int, default=2000)
+    ap.add_argument("--closure-acc-steps", type=int, default=2000)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.precision_report:
@@ -470,6 +609,8 @@ def main():
     try:
         if args.workload == "batch64":
             run_batch(args, ws, rank, local)
+        elif args.workload == "closure":
+            run_closure(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

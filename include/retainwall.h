@@ -277,7 +277,8 @@ rw_status rw_cell_sort_noalloc(const int32_t* d_keys, int32_t n, int32_t max_key
  * a 16-64-64-64-64-6 perceptron with SiLU hidden units, BF16 weights and activations and
  * FP32 accumulation, evaluated and trained on the tensor cores (tcgen05).
  *   features  x[16]: stress / p (6), strain rate / |D| (6), relative void ratio
- *             (e - e_min) / (e_c(p) - e_min), (sin phi_c - 0.556) / 0.087, 0, 0;
+ *             psi = (e - e_min) / (e_c(p) - e_min), (sin phi_c - 0.556) / 0.087,
+ *             psi^alpha, 0;
  *   target    t[6]:  R / (p |D|) / 1000, R the objective stress rate.
  * Parameters (RW_MLP_NPARAM floats): W1[16][64] b1[64] W2[64][64] b2 W3 b3 W4 b4
  * W5[64][6] b5[6] (y = x W + b).  Host arrays are row-major.
@@ -300,15 +301,19 @@ rw_status rw_mlp_grad(rw_mlp* m, const float* x, const float* t, int64_t n, doub
 rw_status rw_mlp_add_samples(rw_mlp* m, const float* x, const float* t, int64_t n);
 rw_status rw_mlp_samples(rw_mlp* m, int64_t* count, float* x, float* t, int64_t n);
 rw_status rw_mlp_clear_samples(rw_mlp* m);
-/* Adam (beta 0.9 / 0.999) over the stored samples, shuffled per epoch; *last_loss =
- * mean squared error over the last epoch. */
+/* Adam (beta 0.9 / 0.999) over the stored samples, shuffled per epoch, the step size
+ * decaying from lr to lr / 20 (cosine) over the call; *last_loss = mean squared error
+ * over the last epoch. */
 rw_status rw_mlp_train(rw_mlp* m, int epochs, int batch, float lr, uint64_t seed, double* last_loss);
 /* Per-feature minimum / maximum of the stored samples and the largest |target|. */
 rw_status rw_mlp_feature_ranges(rw_mlp* m, float* lo, float* hi, float* tmax);
 /* Appends training samples (features and exact targets) from a context's current state:
  * every `stride`-th soil particle with a HypoCS update; *added = samples kept (bounded by
- * the network's free capacity).  The context and the network share a device. */
-rw_status rw_mlp_collect(rw_mlp* m, rw_ctx* ctx, int stride, int64_t* added);
+ * the network's free capacity).  augment = {phi_c min, phi_c max [deg], e0 min, e0 max}
+ * or NULL: with it, each sample's friction angle and initial void ratio are drawn
+ * uniformly (seeded) from those ranges and its target is the exact rate of that material
+ * at the solver's state.  The context and the network share a device. */
+rw_status rw_mlp_collect(rw_mlp* m, rw_ctx* ctx, int stride, const double* augment, uint64_t seed, int64_t* added);
 /* Uses the network for the objective stress rate of this context's HypoCS particles
  * (NULL: exact updates again).  A particle uses it only when all its features lie within
  * the ranges of the network's stored samples, each widened by `margin` times its width,

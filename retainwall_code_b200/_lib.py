@@ -87,7 +87,7 @@ def lib() -> ct.CDLL:
     L.rw_mlp_clear_samples.argtypes = [P]
     L.rw_mlp_train.argtypes = [P, ct.c_int, ct.c_int, ct.c_float, ct.c_uint64, ct.POINTER(ct.c_double)]
     L.rw_mlp_feature_ranges.argtypes = [P, ct.c_void_p, ct.c_void_p, ct.c_void_p]
-    L.rw_mlp_collect.argtypes = [P, P, ct.c_int, ct.POINTER(ct.c_int64)]
+    L.rw_mlp_collect.argtypes = [P, P, ct.c_int, ct.c_void_p, ct.c_uint64, ct.POINTER(ct.c_int64)]
     L.rw_set_closure.argtypes = [P, P, ct.c_double]
     L.rw_closure_stats.argtypes = [P, ct.POINTER(ct.c_double)]
     _lib = L

@@ -101,11 +101,16 @@ class Mlp:
         _check(lib().rw_mlp_train(self._h, epochs, batch, lr, seed, ct.byref(loss)), "rw_mlp_train", self._h)
         return loss.value
 
-    def collect(self, sim, stride: int = 1) -> int:
+    def collect(self, sim, stride: int = 1, augment=None, seed: int = 0) -> int:
         """Appends samples from a LoquatSph's current state (every stride-th soil
-        particle); returns how many were kept."""
+        particle); ``augment`` = (phi min, phi max [deg], e0 min, e0 max) draws each
+        sample's material from those ranges.  Returns how many were kept."""
         n = ct.c_int64()
-        check_ctx = lib().rw_mlp_collect(self._h, sim.handle, stride, ct.byref(n))
+        aug = None
+        if augment is not None:
+            arr = (ct.c_double * 4)(*augment)
+            aug = ct.cast(arr, ct.c_void_p)
+        check_ctx = lib().rw_mlp_collect(self._h, sim.handle, stride, aug, seed, ct.byref(n))
         if check_ctx != 0:
             d = lib().rw_last_error(sim.handle)
             raise RwError(check_ctx, "rw_mlp_collect", d.decode() if d else "")
@@ -120,15 +125,22 @@ class Mlp:
         return lo, hi, float(tm[0])
 
 
-def training_run(net: Mlp, case, steps: int, every: int, stride: int = 1, device: int = 0) -> int:
+# Material ranges of the learned closure's training set: friction angle [deg] and
+# initial void ratio.
+TRAIN_RANGES = (28.0, 40.0, 0.55, 0.80)
+
+
+def training_run(net: Mlp, case, steps: int, every: int, stride: int = 1, device: int = 0, augment=TRAIN_RANGES,
+                 seed: int = 0) -> int:
     """Runs the plain step on ``case`` for ``steps`` steps and stores samples in ``net``
-    every ``every`` steps; returns the number of samples added."""
+    every ``every`` steps (materials drawn from ``augment``, None: the case's own);
+    returns the number of samples added."""
     from .sph import LoquatSph
 
     sim = LoquatSph(case=case, device=device)
     added = 0
-    for s in range(0, steps, every):
+    for k, s in enumerate(range(0, steps, every)):
         sim.step(min(every, steps - s))
-        added += net.collect(sim, stride)
+        added += net.collect(sim, stride, augment, seed * 1000003 + k)
     sim.close()
     return added

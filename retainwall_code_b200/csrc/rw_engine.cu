@@ -62,7 +62,7 @@ struct EngineBase {
   virtual int soil_count() = 0;
   virtual int set_closure(rw_mlp* net, double margin) = 0;
   virtual void closure_stats(double* out) = 0;
-  virtual long long collect(rw_mlp* net, int stride) = 0;
+  virtual long long collect(rw_mlp* net, int stride, const Augment& aug) = 0;
 };
 
 static inline unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -525,7 +525,7 @@ template <class T> struct Engine final : EngineBase {
     out[2] = s[1] > 0 ? s[2] / s[1] : 0.0;
     out[3] = s[3];
   }
-  long long collect(rw_mlp* net, int stride) override {
+  long long collect(rw_mlp* net, int stride, const Augment& aug) override {
     if (mlp::device_of(net) != device) throw Fail(RW_EINVAL, "rw_mlp_collect: the network lives on another device");
     const long long avail = mlp::free_slots(net);
     if (avail <= 0) return 0;
@@ -533,7 +533,7 @@ template <class T> struct Engine final : EngineBase {
     mlp::next_slot(net, &x, &t);
     RW_CU(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st));
     const long n = (P.npm0 + stride - 1) / stride;
-    k_collect<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn, x, t, avail, d_count, stride);
+    k_collect<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn, x, t, avail, d_count, stride, aug);
     check_launch();
     unsigned long long cnt = 0;
     RW_CU(cudaMemcpyAsync(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost, st));
@@ -1360,10 +1360,20 @@ rw_status rw_closure_stats(rw_ctx* ctx, double* out) {
   });
 }
 
-rw_status rw_mlp_collect(rw_mlp* net, rw_ctx* ctx, int stride, int64_t* added) {
+rw_status rw_mlp_collect(rw_mlp* net, rw_ctx* ctx, int stride, const double* augment, uint64_t seed,
+                         int64_t* added) {
   if (!net || stride < 1) return RW_EINVAL;
+  rw::Augment aug{};
+  if (augment) {
+    if (!(augment[0] > 0.0 && augment[1] >= augment[0] && augment[1] < 90.0 && augment[2] > 0.0 &&
+          augment[3] >= augment[2]))
+      return RW_EINVAL;
+    const double d2r = 3.14159265358979323846 / 180.0;
+    aug = rw::Augment{(float)(augment[0] * d2r), (float)(augment[1] * d2r), (float)augment[2], (float)augment[3],
+                      (unsigned long long)seed, 1};
+  }
   return guarded(ctx, [&](rw::EngineBase& e) {
-    const long long a = e.collect(net, stride);
+    const long long a = e.collect(net, stride, aug);
     if (added) *added = a;
     return RW_OK;
   });

@@ -1729,7 +1729,7 @@ template <class T> RWD void closure_features(const HypoPre<T>& h, const S6<T>& D
   const T void_min = mp[9];
   f[12] = (float)((h.e - void_min) / (h.e_crt - void_min));
   f[13] = ((float)f_sin(mp[2]) - mlp::SIN_MID) / mlp::SIN_HALF;
-  f[14] = 0.0f;
+  f[14] = (float)h.fd;  // the law's own void-ratio factor psi^alpha
   f[15] = 0.0f;
 }
 
@@ -1738,10 +1738,29 @@ template <class T> RWD S6<T> closure_scale_out(const HypoPre<T>& h, const float*
   return S6<T>{(T)y[0] * sc, (T)y[1] * sc, (T)y[2] * sc, (T)y[3] * sc, (T)y[4] * sc, (T)y[5] * sc};
 }
 
+// Uniform in [0, 1) from a 64-bit key (splitmix64 finaliser).
+RWD float hash_unit(unsigned long long k) {
+  k += 0x9E3779B97F4A7C15ull;
+  k = (k ^ (k >> 30)) * 0xBF58476D1CE4E5B9ull;
+  k = (k ^ (k >> 27)) * 0x94D049BB133111EBull;
+  k ^= k >> 31;
+  return (float)(k >> 40) * (1.0f / 16777216.0f);
+}
+
+// Friction angle [rad] and initial void ratio ranges for augmented samples.
+struct Augment {
+  float phi_lo, phi_hi, e0_lo, e0_hi;
+  unsigned long long seed;
+  int on;
+};
+
 // Appends (features, exact normalised objective rate) of every stride-th soil particle
-// with a HypoCS update, from the current stress, strain rate and density.
+// with a HypoCS update, from the current stress, strain rate and density.  With
+// augmentation each sample takes a friction angle and an initial void ratio drawn
+// uniformly from the given ranges: the state comes from the solver, the target from the
+// exact law for that material.
 template <class T> __global__ void k_collect(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, float* X, float* Tg,
-                                             long long cap, unsigned long long* count, int stride) {
+                                             long long cap, unsigned long long* count, int stride, Augment aug) {
   const int t = (blockIdx.x * blockDim.x + threadIdx.x) * stride;
   const int npm = dyn->npm, c = dyn->cur_main;
   bool ok = false;
@@ -1750,7 +1769,15 @@ template <class T> __global__ void k_collect(const Params<T> P, DevState<T> S, c
     const int i = P.npb + t;
     const int4 code = S.codes[c][i];
     if (code.y == 1 && code.z == RW_MODEL_HYPO_CS) {
-      const T* mp = P.model_par[code.w];
+      T mpa[kMatSize];
+#pragma unroll
+      for (int k = 0; k < kMatSize; ++k) mpa[k] = P.model_par[code.w][k];
+      if (aug.on) {
+        const unsigned long long key = aug.seed * 0x100000001B3ull + (unsigned long long)i;
+        mpa[2] = (T)(aug.phi_lo + (aug.phi_hi - aug.phi_lo) * hash_unit(2 * key));
+        mpa[11] = (T)(aug.e0_lo + (aug.e0_hi - aug.e0_lo) * hash_unit(2 * key + 1));
+      }
+      const T* mp = mpa;
       const S6<T> D = ld6(S.ace_a, S.ace_b, i);
       S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
       HypoPre<T> h;
@@ -1832,9 +1859,13 @@ __global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevSta
         }
       }
     }
-    mlp::store_row<mlp::IN>(sm.x, tid, f);
     float y[mlp::OUT];
-    mlp::forward_tile(sm, 0, phase, y);
+#pragma unroll
+    for (int o = 0; o < mlp::OUT; ++o) y[o] = 0.0f;
+    if (__syncthreads_or(act)) {  // a tile without a trusted particle skips the network
+      mlp::store_row<mlp::IN>(sm.x, tid, f);
+      mlp::forward_tile(sm, 0, phase, y);
+    }
     float used = 0.0f, offered = 0.0f, err = 0.0f;
     if (mine) {
       const T* mp = P.model_par[code.w];

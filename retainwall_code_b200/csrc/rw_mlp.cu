@@ -623,7 +623,8 @@ rw_status rw_mlp_train(rw_mlp* m, int epochs, int batch, float lr, uint64_t seed
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     double lsum_epoch = 0.0;
     long long nb = 0;
-    std::vector<double> lbuf;
+    const long long total = (long long)epochs * (n / batch);
+    long long step = 0;
     for (int ep = 0; ep < epochs; ++ep) {
       long long a;  // multiplier coprime to n: a shuffled order of the samples per epoch
       do {
@@ -637,7 +638,11 @@ rw_status rw_mlp_train(rw_mlp* m, int epochs, int batch, float lr, uint64_t seed
         if (s != RW_OK) return s;
         ++m->adam_t;
         const float bc1 = 1.0f - std::pow(b1, (float)m->adam_t), bc2 = 1.0f - std::pow(b2, (float)m->adam_t);
-        k_adam<<<(NPARAM + 255) / 256, 256, 0, m->st>>>(m->params, m->grad, m->m, m->v, lr, b1, b2, eps, bc1, bc2,
+        // cosine decay from lr to lr / 20 over the call
+        const double frac = total > 1 ? (double)step / (double)(total - 1) : 1.0;
+        const float lr_t = (float)(lr * (0.05 + 0.95 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * frac))));
+        ++step;
+        k_adam<<<(NPARAM + 255) / 256, 256, 0, m->st>>>(m->params, m->grad, m->m, m->v, lr_t, b1, b2, eps, bc1, bc2,
                                                         m->fw, m->bw, m->bias);
         MLP_CU(m, cudaGetLastError());
       }

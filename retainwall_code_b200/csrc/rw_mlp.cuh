@@ -11,7 +11,8 @@
 //     f[6..11] = D / |D|                (|D| = sqrt(D : D), as the reference's norm)
 //     f[12]    = (e - e_min) / (e_c(p) - e_min)   (relative void ratio, fd = f[12]^alpha)
 //     f[13]    = (sin phi_c - SIN_MID) / SIN_HALF (friction angle of the material)
-//     f[14..15] = 0                     (padding to the MMA's K = 16)
+//     f[14]    = f[12]^alpha            (the void-ratio factor fd of the law)
+//     f[15]    = 0                      (padding to the MMA's K = 16)
 // The Jaumann term, the tension cut-off and the cone projection stay exact.
 #pragma once
 #include <cuda_bf16.h>

@@ -39,6 +39,7 @@ def _objective_np(sig, D, rho, mp):
     f[:, 6:12] = D / nD[:, None]
     f[:, 12] = psi
     f[:, 13] = (np.sin(np.float32(phi)) - 0.556) / 0.087
+    f[:, 14] = fd
     return f, R / (p * nD)[:, None] / 1000.0
 
 
@@ -102,7 +103,7 @@ def test_trained_closure_tracks_the_plain_method():
                      steps=60, every=3)
     n = net.sample_count()
     assert n > 100_000
-    loss = net.train(epochs=30, batch=128 * 148, lr=2e-3, seed=1)
+    loss = net.train(epochs=30, batch=4096, lr=2e-3, seed=1)
     c = C.column_collapse(nx=12, ny=12, nz=24, phi_c=31.0, e0=0.68, seed=9, runout=1.0)
     plain = LoquatSph(case=c)
     clo = LoquatSph(case=c)
@@ -115,3 +116,35 @@ def test_trained_closure_tracks_the_plain_method():
     assert rel(clo.get("pos_abs"), plain.get("pos_abs")) < 1e-5
     assert rel(clo.get("str"), plain.get("str")) < 5e-2
     assert clo.info().device_err == 0
+
+
+def test_augmented_samples_follow_the_exact_law():
+    """Augmented samples (material drawn per sample) keep the solver's state and carry the
+    exact target of the drawn material: in normalised variables the HypoCS objective rate
+    is a closed form of the features, R / (p |D|) = -3 C1 d + C2 tr(d) s + C3 tr(s d) / tr(s) s
+    + C4 psi^alpha (s + s_dev), with a = 3 / (sqrt(2) sin phi) recovered from feature 13."""
+    c = C.column_collapse(nx=8, ny=8, nz=16, runout=1.0)
+    s = LoquatSph(case=c)
+    s.step(3)
+    net = Mlp(sample_capacity=100_000)
+    n = net.collect(s, stride=1, augment=(28.0, 40.0, 0.55, 0.80), seed=5)
+    assert n > 0
+    x, t = (a.astype(np.float64) for a in net.samples())
+    mp = np.array([c.params[f"model-0-par-{j}"] for j in range(15)], np.float64)
+    Ei, Vi, pref, alpha = mp[0], mp[1], mp[4], mp[8]
+    sin_phi = x[:, 13] * 0.087 + 0.556
+    assert sin_phi.min() < np.sin(np.radians(29.0)) and sin_phi.max() > np.sin(np.radians(39.0))
+    C1 = -Ei / (3.0 * pref * (1.0 + Vi))
+    a = 3.0 / (np.sqrt(2.0) * sin_phi)
+    C2 = C1 * ((3.0 * Vi + a * np.sqrt(1.0 + Vi * Vi)) / (1.0 - Vi) - a * a / 3.0)
+    C3, C4 = a * a * C1, a * C1
+    sh, d = x[:, 0:6], x[:, 6:12]
+    trs = sh[:, :3].sum(1)
+    trd = d[:, :3].sum(1)
+    trsd = (sh[:, :3] * d[:, :3]).sum(1) + 2.0 * (sh[:, 3:] * d[:, 3:]).sum(1)
+    dev = sh.copy()
+    dev[:, :3] -= (trs / 3.0)[:, None]
+    R = (d * (C1 * trs)[:, None] + sh * (C2 * trd)[:, None] + sh * (C3 * trsd / trs)[:, None]
+         + (sh + dev) * (C4 * x[:, 12] ** alpha)[:, None]) / 1000.0
+    assert rel(t, R) < 2e-5
+    assert rel(x[:, 14], x[:, 12] ** alpha) < 1e-5
