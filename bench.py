@@ -150,15 +150,16 @@ def barrier(ws: int):
         dist.barrier()
 
 
-def interaction_bytes(inf, ncell: int, scalar: int) -> int:
+def interaction_bytes(inf, ncell: int, scalar: int, list_entries: int = 0) -> int:
     """Algorithmic HBM bytes of one interaction launch: every live soil particle's own
     state read once (cell 16, position 4s, velocity 4s, stress 6s, mass 4s, contact
     state 4x4s) and its outputs written once (contact 2x4s, acceleration 4s, strain rate
-    6s, spin 4s), plus each particle's neighbour record (16s) and position (4s) read once,
-    plus the cell ranges (8 B per cell)."""
+    6s, spin 4s), plus each particle's neighbour record (16s, position included) read
+    once, plus the kept candidate lists (4 B per entry) and the cell ranges (8 B per
+    cell)."""
     s = scalar
     per_soil = 16 + (4 + 4 + 6 + 4 + 16) * s + (8 + 4 + 6 + 4) * s
-    return inf.npm * per_soil + inf.np * 20 * s + ncell * 8
+    return inf.npm * per_soil + inf.np * 16 * s + 4 * list_entries + ncell * 8
 
 
 def cpu_sample(case, threads: int, steps: int):
@@ -300,8 +301,10 @@ def run_ours(args, ws, rank, local):
     npm = sim.info().npm
     value = ws * npm * args.steps / (ms * 1e-3)
     inf = sim.info()
+    le, lp = sim.list_stats()
     lists = {"skin_h": 0.02 if args.skin is None else args.skin, "sections_that_sorted": inf.n_sorts,
-             "interactions_on_kept_lists": inf.n_list_reuse, "interactions": 2 * inf.step}
+             "interactions_on_kept_lists": inf.n_list_reuse, "interactions": 2 * inf.step,
+             "mean_list_length": le / max(lp, 1)}
     if inf.device_err:
         raise SystemExit(f"device error word {inf.device_err}")
     if args.no_e2e:
@@ -323,6 +326,7 @@ def run_ours(args, ws, rank, local):
         sim2.wall_force(0)  # D2H of the step's result (3 doubles)
     sim2.synchronize()
     e2e_s = allreduce_max(time.perf_counter() - t0, ws)
+    sim2_lists = sim2.list_stats()
     sim2.close()
     e2e = ws * npm * e2e_steps / e2e_s
     # bytes uploaded by rw_create_from_case: codes, cell, position x2, velocity, id/mass,
@@ -330,7 +334,8 @@ def run_ours(args, ws, rank, local):
     h2d = inf.np * (16 * 6 + 24 * 2) + inf.npb * 16
     # ---- roofline of the dominant kernel ------------------------------------------------
     pk, kind = peaks()
-    ib = interaction_bytes(inf, inf.ncell, 4)
+    list_entries, list_parts = sim2_lists
+    ib = interaction_bytes(inf, inf.ncell, 4, list_entries)
     achieved = ib / (ix_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": "k_interaction", "achieved": achieved, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": kind,
@@ -593,7 +598,7 @@ def main():
     ap.add_argument("--precision-steps", type=int, default=2000)
     ap.add_argument("--batch-cases", type=int, default=64)
     ap.add_argument("--closure-samples", type=int, default=10_000_000)
-    ap.add_argument("--closure-epochs", type=int, default=20)
+    ap.add_argument("--closure-epochs", type=int, default=30)
     ap.add_argument("--closure-run-steps", type=int, default=2000)
     ap.add_argument("--closure-acc-steps", type=int, default=2000)
     args = ap.parse_args()

@@ -249,6 +249,9 @@ rw_status rw_batch_create(rw_ctx* const* ctxs, int n, rw_batch** out);
 rw_status rw_batch_step(rw_batch* b, int nsteps, double* ms);
 rw_status rw_batch_synchronize(rw_batch* b);
 rw_status rw_batch_destroy(rw_batch* b);
+/* Kept candidate lists (RW_OPT_LIST_SKIN) as they stand: out[0] = entries over all soil
+ * particles, out[1] = soil particles holding a list (both 0 when none is kept). */
+rw_status rw_list_stats(rw_ctx* ctx, int64_t* out);
 /* Autotuner: times each interaction kernel (RW_OPT_INTERACTION_KERNEL 0 and 1) on this
  * case for `steps` steps (plus one capture step each; the case advances) and keeps the
  * faster; *chosen receives it. */

@@ -23,6 +23,7 @@ EXPORTS = [
     "rw_mlp_last_error", "rw_mlp_create", "rw_mlp_destroy", "rw_mlp_get_params", "rw_mlp_set_params",
     "rw_mlp_forward", "rw_mlp_grad", "rw_mlp_add_samples", "rw_mlp_samples", "rw_mlp_clear_samples",
     "rw_mlp_train", "rw_mlp_feature_ranges", "rw_mlp_collect", "rw_set_closure", "rw_closure_stats",
+    "rw_list_stats",
 ]
 STAGE_NAMES = ["search_p", "rigid", "adami_p", "corner_p", "interaction_p", "predictor", "search_c", "adami_c",
                "corner_c", "interaction_c", "corrector"]
@@ -90,6 +91,7 @@ def lib() -> ct.CDLL:
     L.rw_mlp_collect.argtypes = [P, P, ct.c_int, ct.c_void_p, ct.c_uint64, ct.POINTER(ct.c_int64)]
     L.rw_set_closure.argtypes = [P, P, ct.c_double]
     L.rw_closure_stats.argtypes = [P, ct.POINTER(ct.c_double)]
+    L.rw_list_stats.argtypes = [P, ct.POINTER(ct.c_int64)]
     _lib = L
     return L
 

@@ -63,6 +63,7 @@ struct EngineBase {
   virtual int set_closure(rw_mlp* net, double margin) = 0;
   virtual void closure_stats(double* out) = 0;
   virtual long long collect(rw_mlp* net, int stride, const Augment& aug) = 0;
+  virtual void list_totals(long long* out) = 0;
 };
 
 static inline unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -524,6 +525,24 @@ template <class T> struct Engine final : EngineBase {
     out[1] = s[1];
     out[2] = s[1] > 0 ? s[2] / s[1] : 0.0;
     out[3] = s[3];
+  }
+  void list_totals(long long* out) override {
+    out[0] = out[1] = 0;
+    if (!S.nbg) return;
+    Dyn<T> d = dyn_host();
+    if (!d.list_ok) return;
+    unsigned long long* tot = nullptr;
+    RW_CU(cudaMallocAsync((void**)&tot, 2 * sizeof(unsigned long long), st));
+    RW_CU(cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), st));
+    k_list_totals<<<2 * nsm, 256, 0, st>>>(S.nbg_cnt, d.npm, tot);
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(tot, st);
+    RW_CU(e);
+    RW_CU(cudaStreamSynchronize(st));
+    out[0] = (long long)h[0];
+    out[1] = (long long)h[1];
   }
   long long collect(rw_mlp* net, int stride, const Augment& aug) override {
     if (mlp::device_of(net) != device) throw Fail(RW_EINVAL, "rw_mlp_collect: the network lives on another device");
@@ -1345,6 +1364,17 @@ rw_status rw_batch_destroy(rw_batch* b) {
   cudaSetDevice(b->b.device);
   delete b;
   return RW_OK;
+}
+
+rw_status rw_list_stats(rw_ctx* ctx, int64_t* out) {
+  if (!out) return RW_EINVAL;
+  return guarded(ctx, [&](rw::EngineBase& e) {
+    long long t[2];
+    e.list_totals(t);
+    out[0] = t[0];
+    out[1] = t[1];
+    return RW_OK;
+  });
 }
 
 rw_status rw_set_closure(rw_ctx* ctx, rw_mlp* net, double margin) {

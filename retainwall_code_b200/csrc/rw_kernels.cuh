@@ -1703,6 +1703,24 @@ static __global__ void k_wall_force_final(double* wsum, int nblocks) {
   for (int k = 0; k < 3; ++k) wsum[3 * nblocks + k] = a[k];
 }
 
+// Totals of the kept candidate lists: out[0] += entries, out[1] += soil particles with a list.
+static __global__ void k_list_totals(const int* cnt, int n, unsigned long long* out) {
+  unsigned long long e = 0, p = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    if (cnt[t] >= 0) {
+      e += (unsigned long long)cnt[t];
+      ++p;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    e += __shfl_xor_sync(0xffffffffu, e, o);
+    p += __shfl_xor_sync(0xffffffffu, p, o);
+  }
+  if ((threadIdx.x & 31) == 0 && p) {
+    atomicAdd(&out[0], e);
+    atomicAdd(&out[1], p);
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // Learned constitutive closure (no counterpart in the reference): samples for its
 // training and its use inside the step.  Features and target as in rw_mlp.cuh.

@@ -148,11 +148,30 @@ __device__ __forceinline__ void wgrad(float* acc, int w0, int b0, const unsigned
   float s[OPT];
 #pragma unroll
   for (int k = 0; k < OPT; ++k) s[k] = 0.0f;
-#pragma unroll 4
-  for (int b = 0; b < TILE; ++b) {
-    const float hv = load_elem<KIN>(hin, b, i);
+  if constexpr (OPT % 8 == 0) {  // whole 16-byte runs of the G row: vector loads
+#pragma unroll 2
+    for (int b = 0; b < TILE; ++b) {
+      const float hv = load_elem<KIN>(hin, b, i);
 #pragma unroll
-    for (int k = 0; k < OPT; ++k) s[k] = fmaf(hv, load_elem<GK>(g, b, o0 + k), s[k]);
+      for (int k8 = 0; k8 < OPT; k8 += 8) {
+        const uint4 q = *reinterpret_cast<const uint4*>(g + tc::kmajor_off(b, o0 + k8, GK));
+        s[k8 + 0] = fmaf(hv, bf16_lo(q.x), s[k8 + 0]);
+        s[k8 + 1] = fmaf(hv, bf16_hi(q.x), s[k8 + 1]);
+        s[k8 + 2] = fmaf(hv, bf16_lo(q.y), s[k8 + 2]);
+        s[k8 + 3] = fmaf(hv, bf16_hi(q.y), s[k8 + 3]);
+        s[k8 + 4] = fmaf(hv, bf16_lo(q.z), s[k8 + 4]);
+        s[k8 + 5] = fmaf(hv, bf16_hi(q.z), s[k8 + 5]);
+        s[k8 + 6] = fmaf(hv, bf16_lo(q.w), s[k8 + 6]);
+        s[k8 + 7] = fmaf(hv, bf16_hi(q.w), s[k8 + 7]);
+      }
+    }
+  } else {
+#pragma unroll 4
+    for (int b = 0; b < TILE; ++b) {
+      const float hv = load_elem<KIN>(hin, b, i);
+#pragma unroll
+      for (int k = 0; k < OPT; ++k) s[k] = fmaf(hv, load_elem<GK>(g, b, o0 + k), s[k]);
+    }
   }
 #pragma unroll
   for (int k = 0; k < OPT; ++k) acc[w0 + i * NOUT + o0 + k] += s[k];
@@ -163,7 +182,7 @@ __device__ __forceinline__ void wgrad(float* acc, int w0, int b0, const unsigned
   }
 }
 
-__global__ void __launch_bounds__(TILE) k_train(Net net, const float* __restrict__ X, const float* __restrict__ Tg,
+__global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restrict__ X, const float* __restrict__ Tg,
                                                 long long n_all, long long first, int n, long long sa, long long sc,
                                                 float inv_count, float* __restrict__ grad, double* __restrict__ loss,
                                                 int* err) {

@@ -65,6 +65,12 @@ class LoquatSph:
         """Use ``net`` (closure.Mlp) for the HypoCS objective stress rate (None: exact)."""
         self._c(lib().rw_set_closure(self._h, net.handle if net is not None else None, margin), "rw_set_closure")
 
+    def list_stats(self):
+        """(entries, soil particles) of the kept candidate lists."""
+        out = (ct.c_int64 * 2)()
+        self._c(lib().rw_list_stats(self._h, out), "rw_list_stats")
+        return out[0], out[1]
+
     def closure_stats(self) -> dict:
         out = (ct.c_double * 4)()
         self._c(lib().rw_closure_stats(self._h, out), "rw_closure_stats")
