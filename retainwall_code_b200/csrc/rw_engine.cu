@@ -410,11 +410,16 @@ template <class T> struct Engine final : EngineBase {
       RW_CU(cudaMemsetAsync(S.near_wall, 0, (size_t)P.ncell_material, st));
       k_mark_near_wall<T><<<nblk(P.npb, 256), 256, 0, st>>>(P, S, d_dyn);
     }
-    if (ncol > 0) {  // column chunks of the interaction
-      k_col_count<T><<<nblk(ncol, 256), 256, 0, st>>>(P, S);
-      k_col_scan<T><<<1, 1024, 0, st>>>(P, S, d_dyn);
-      k_col_fill<T><<<nblk(ncol, 256), 256, 0, st>>>(P, S);
-    }
+    if (ix_kernel == 1) chunk_list();
+    check_launch();
+  }
+  // Column chunks of the chunked interaction kernel (rebuilt after every search while
+  // that kernel is selected).
+  void chunk_list() {
+    if (ncol <= 0) return;
+    k_col_count<T><<<nblk(ncol, 256), 256, 0, st>>>(P, S);
+    k_col_scan<T><<<1, 1024, 0, st>>>(P, S, d_dyn);
+    k_col_fill<T><<<nblk(ncol, 256), 256, 0, st>>>(P, S);
     check_launch();
   }
   void rigid() override {
@@ -621,7 +626,7 @@ template <class T> struct Engine final : EngineBase {
   // Kernels launched by one whole step (launch_step), for launch accounting.
   int kernels_per_step() const {
     // keys, check, sort, ranges, count, permute, flip, contact-wall cells, chunks
-    const int search = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 1 : 0) + (ncol > 0 ? 3 : 0);
+    const int search = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 1 : 0) + (ncol > 0 && ix_kernel == 1 ? 3 : 0);
     const int ix = ix_kernel == 1 ? 1 : 2;             // chunked, or scan + walk
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
@@ -782,7 +787,9 @@ template <class T> struct Engine final : EngineBase {
       strict_fp = v != 0.0;
     } else if (opt == RW_OPT_INTERACTION_KERNEL) {
       if (v != 0.0 && v != 1.0) return RW_EINVAL;
+      const int was = ix_kernel;
       ix_kernel = (int)v;
+      if (ix_kernel == 1 && was != 1) chunk_list();  // chunks of the current ordering
     } else if (opt == RW_OPT_COMPAT_CONTACT) {
       if (v == 0.0) {
         err = "contact state following particles (RW_OPT_COMPAT_CONTACT=0) is not available";
