@@ -28,12 +28,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-updates/s/GPU at 1.92M particles"
-# From the ncu capture of k_interaction on the 0.96M-particle case
-# (profiles/k_interaction_wall2_half.md): DRAM read+write 186.4 + 62.7 MB and 716.1M warp
+# From the ncu capture of the interaction's walk kernel on the 0.96M-particle case
+# (profiles/k_interaction_wall2_half.md): DRAM read+write 461.4 + 65.5 MB and 369.1M warp
 # instructions per launch.  Both grow with the particle count, so they are scaled per
 # soil particle to the benchmarked case.
-IX_DRAM_BYTES_PER_SOIL = (186.42e6 + 62.72e6) / 960000
-IX_WARP_INSTR_PER_SOIL = 716.09e6 / 960000
+IX_DRAM_BYTES_PER_SOIL = (461.38e6 + 65.50e6) / 960000
+IX_WARP_INSTR_PER_SOIL = 369.13e6 / 960000
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
