@@ -42,6 +42,13 @@ template <class T> RWD V3<T> cross(V3<T> a, V3<T> b) {
 
 RWD float f_sqrt(float x) { return sqrtf(x); }
 RWD double f_sqrt(double x) { return sqrt(x); }
+RWD float f_rsqrt(float x) { return rsqrtf(x); }
+RWD double f_rsqrt(double x) { return rsqrt(x); }
+RWD float f_fma(float a, float b, float c) { return fmaf(a, b, c); }
+RWD double f_fma(double a, double b, double c) { return fma(a, b, c); }
+// Quotient through the hardware reciprocal (float) or the correctly rounded divide (double).
+RWD float f_fastdiv(float a, float b) { return __fdividef(a, b); }
+RWD double f_fastdiv(double a, double b) { return a / b; }
 RWD float f_pow(float a, float b) { return powf(a, b); }
 RWD double f_pow(double a, double b) { return pow(a, b); }
 RWD float f_exp(float a) { return expf(a); }

@@ -738,10 +738,18 @@ template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) 
 
 // One pair (i, j) of cuParticleInteractionMaterialLoopSolution
 // (src/particle_interaction.cu:29-114), given dr = (pos_i - pos_j) - offset * 2h.
+// Strict: the reference's expressions, every operation separately rounded (the CPU
+// restatement's order).  Default: the same terms in fewer instructions -- r from the
+// hardware reciprocal square root, the velocity-gradient products with the neighbour
+// volume folded into the kernel gradient, one approximate division in the artificial
+// viscosity -- a few units in the last place from the reference's roundings.
 template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const IState<T>& I, const V3<T> dr,
                                                    const NbVals<T>& nb, Acc<T>& A) {
   using F = Fp<Strict>;
-  T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+  const T r2 = pair_r2(dr.x, dr.y, dr.z);
+  T r;
+  if constexpr (Strict) r = pair_r(r2);
+  else r = r2 > T(0) ? r2 * f_rsqrt(r2) : T(0);
   T q = F::mul(r, P.i_h);
   if (!(q < T(2.0f))) return;
   const T t = T(2.0f) - q;
@@ -751,19 +759,34 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
   const bool contact_j = nb.a.y < T(0);
   V3<T> dvel{I.vel.x - nb.vr.x, I.vel.y - nb.vr.y, I.vel.z - nb.vr.z};
   if (contact_j && I.shift == 1) dvel = V3<T>{T(0), T(0), T(0)};
-  // grad_vel -= (dvel (x) gker) * vol_j
-  A.gv.xx = F::msub(F::mul(dvel.x, gker.x), vol_j, A.gv.xx);
-  A.gv.xy = F::msub(F::mul(dvel.x, gker.y), vol_j, A.gv.xy);
-  A.gv.xz = F::msub(F::mul(dvel.x, gker.z), vol_j, A.gv.xz);
-  A.gv.yx = F::msub(F::mul(dvel.y, gker.x), vol_j, A.gv.yx);
-  A.gv.yy = F::msub(F::mul(dvel.y, gker.y), vol_j, A.gv.yy);
-  A.gv.yz = F::msub(F::mul(dvel.y, gker.z), vol_j, A.gv.yz);
-  A.gv.zx = F::msub(F::mul(dvel.z, gker.x), vol_j, A.gv.zx);
-  A.gv.zy = F::msub(F::mul(dvel.z, gker.y), vol_j, A.gv.zy);
-  A.gv.zz = F::msub(F::mul(dvel.z, gker.z), vol_j, A.gv.zz);
-  if (contact_j) return;
-  const T dvg = F::dot3(dvel.x, dvel.y, dvel.z, gker.x, gker.y, gker.z);
-  A.accden = F::mad(F::mul(I.rho, dvg), vol_j, A.accden);
+  // grad_vel -= (dvel (x) gker) * vol_j;  accden += rho_i (dvel . gker) vol_j
+  if constexpr (Strict) {
+    A.gv.xx = F::msub(F::mul(dvel.x, gker.x), vol_j, A.gv.xx);
+    A.gv.xy = F::msub(F::mul(dvel.x, gker.y), vol_j, A.gv.xy);
+    A.gv.xz = F::msub(F::mul(dvel.x, gker.z), vol_j, A.gv.xz);
+    A.gv.yx = F::msub(F::mul(dvel.y, gker.x), vol_j, A.gv.yx);
+    A.gv.yy = F::msub(F::mul(dvel.y, gker.y), vol_j, A.gv.yy);
+    A.gv.yz = F::msub(F::mul(dvel.y, gker.z), vol_j, A.gv.yz);
+    A.gv.zx = F::msub(F::mul(dvel.z, gker.x), vol_j, A.gv.zx);
+    A.gv.zy = F::msub(F::mul(dvel.z, gker.y), vol_j, A.gv.zy);
+    A.gv.zz = F::msub(F::mul(dvel.z, gker.z), vol_j, A.gv.zz);
+    if (contact_j) return;
+    const T dvg = F::dot3(dvel.x, dvel.y, dvel.z, gker.x, gker.y, gker.z);
+    A.accden = F::mad(F::mul(I.rho, dvg), vol_j, A.accden);
+  } else {
+    const V3<T> gkv{F::mul(gker.x, vol_j), F::mul(gker.y, vol_j), F::mul(gker.z, vol_j)};
+    A.gv.xx = f_fma(-dvel.x, gkv.x, A.gv.xx);
+    A.gv.xy = f_fma(-dvel.x, gkv.y, A.gv.xy);
+    A.gv.xz = f_fma(-dvel.x, gkv.z, A.gv.xz);
+    A.gv.yx = f_fma(-dvel.y, gkv.x, A.gv.yx);
+    A.gv.yy = f_fma(-dvel.y, gkv.y, A.gv.yy);
+    A.gv.yz = f_fma(-dvel.y, gkv.z, A.gv.yz);
+    A.gv.zx = f_fma(-dvel.z, gkv.x, A.gv.zx);
+    A.gv.zy = f_fma(-dvel.z, gkv.y, A.gv.zy);
+    A.gv.zz = f_fma(-dvel.z, gkv.z, A.gv.zz);
+    if (contact_j) return;
+    A.accden = f_fma(I.rho, F::dot3(dvel.x, dvel.y, dvel.z, gkv.x, gkv.y, gkv.z), A.accden);
+  }
   const S6<T> st{I.sor.xx + nb.a.z, I.sor.yy + nb.a.w, I.sor.zz + nb.b.x,
                  I.sor.xy + nb.b.y, I.sor.xz + nb.b.z, I.sor.yz + nb.b.w};
   const T fx = F::dot3(st.xx, st.xy, st.xz, gker.x, gker.y, gker.z);
@@ -779,8 +802,8 @@ template <bool Strict, class T> RWD void pair_eval(const Params<T>& P, const ISt
       if constexpr (Strict) {
         const T phi = F::mul(P.h, visc) / F::mad(r, r, P.eta);
         artv = F::mul(F::mul(P.alpha_m, P.cs_m), phi) / F::mul(T(0.5f), I.rho + rho_j);
-      } else {  // the same quotient with one division
-        artv = F::mul(P.visc_k, visc) / F::mul(F::mad(r, r, P.eta), F::mul(T(0.5f), I.rho + rho_j));
+      } else {  // the same quotient with one approximate division
+        artv = f_fastdiv(F::mul(P.visc_k, visc), F::mul(r2 + P.eta, F::mul(T(0.5f), I.rho + rho_j)));
       }
     }
     const T m = F::mul(mass_j, artv);
