@@ -315,3 +315,48 @@ def test_kept_candidate_lists_reused_and_dropped(cases):
     assert a.info().n_list_reuse == 0
     for key in ("cellpos", "pospres", "velrhop", "str", "contact_var", "accad"):
         np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
+
+
+def test_deletion_matches_oracle():
+    """Soil thrown out through the open +x side of the grid is moved to the deleted cell
+    (cuCheckOutDomain, src/predictor_corrector.cu:183-187; the count bookkeeping of
+    src/loquat_grid.cu:164-190): live and deleted counts, the cell coordinates of every
+    slot and the state of the remaining soil match the oracle step after step."""
+    from retainwall_code_b200 import cases as C
+
+    c = C.column_collapse(nx=8, ny=8, nz=16, runout=0.0)
+    c.velrhop[c.npb:, 0] = 40.0
+    s = LoquatSph(case=c)
+    o = Oracle(c, 4)
+    deleted = []
+    for _ in range(11):
+        s.step(10)
+        o.step(10)
+        a, b = s.info(), o.info()
+        assert (a.npm, a.np_delete_m) == (b.npm, b.np_delete_m)
+        np.testing.assert_array_equal(s.get("cellpos"), o.get("cellpos"))
+        live = slice(a.npb, a.npb + a.npm)
+        assert rel(s.get("pos_abs")[live], o.get("pos_abs")[live]) < 1e-5
+        deleted.append(a.np_delete_m)
+    assert deleted[-1] > 0 and deleted[0] == 0
+    assert s.info().device_err == 0
+
+
+def test_no_boundary_particles_matches_oracle():
+    """A case without boundary particles (npb = 0: soil in free fall)."""
+    from retainwall_code_b200 import cases as C
+
+    b = C._Builder()
+    C._soil(b, 0.05, 0.05, 0.05, 6, 6, 6, 0.005, np.random.default_rng(1), 0.05, 1850.0, -9.81, 0.5)
+    p = C._base_params(0.005, 1.2, 60.0, 0.1, 1850.0, C.hypocs_model(30.0, 0.7, 1850.0))
+    p["domain_size_x"] = p["domain_size_y"] = p["domain_size_z"] = 0.15
+    c = b.case(p, [], "free", 1850.0, C.f32(1850.0 * 0.005 ** 3))
+    assert c.npb == 0
+    s = LoquatSph(case=c)
+    o = Oracle(c, 4)
+    s.step(20)
+    o.step(20)
+    np.testing.assert_array_equal(s.get("cellpos"), o.get("cellpos"))
+    for key in ("pos_abs", "velrhop", "str"):
+        assert rel(s.get(key), o.get(key)) < 1e-5, key
+    assert s.info().device_err == 0
