@@ -883,6 +883,7 @@ RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const ISt
   unsigned ent1 = cnt > 1 ? entry(stride) : 0u;
   int oc = (int)(ent >> 27);
   NbVals<T> nb = load_nb(rec, (int)(ent & 0x7ffffffu));
+#pragma unroll 2  // alternating record registers instead of copying the prefetched one
   for (int e = 0; e < cnt; ++e) {
     const NbVals<T> cur = nb;
     const int occ = oc;
