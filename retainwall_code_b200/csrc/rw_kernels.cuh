@@ -522,7 +522,9 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
       for (int j = rg.x; j < rg.y; ++j) {
         V3<T> dr = pp - ld3(pos, j);
         dr = dr - o;
-        T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+        const T r2 = pair_r2(dr.x, dr.y, dr.z);
+        if (!(r2 < P.r2_prefilter)) continue;  // conservative: q >= 2 beyond it
+        T r = pair_r(r2);
         T q = r * P.i_h;
         if (q < T(2.0f)) {
           T dwdr = kernel_f(P.kgrad, q);
@@ -535,7 +537,9 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
     for (int j = rg.x; j < rg.y; ++j) {
       V3<T> dr = pp - ld3(pos, j);
       dr = dr - o;
-      T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+      const T r2 = pair_r2(dr.x, dr.y, dr.z);
+      if (!(r2 < P.r2_prefilter)) continue;
+      T r = pair_r(r2);
       T q = r * P.i_h;
       if (q < T(2.0f)) {
         T ker = kernel_w(P.knorm, q);
@@ -663,7 +667,9 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
       const V3<T> o = mulI(off, th);
       for (int j = rg.x; j < rg.y; ++j) {
         V3<T> dr = pos_i - ld3(pos, j) - o;
-        T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+        const T r2 = pair_r2(dr.x, dr.y, dr.z);
+        if (!(r2 < P.r2_prefilter)) continue;
+        T r = pair_r(r2);
         T q = r * P.i_h;
         if ((double)q < 2.0) {
           const int codej = S.codes[c][j].x;
@@ -1597,7 +1603,9 @@ template <class T> __global__ void __launch_bounds__(128) k_shepard(const Params
       const V3<T> o = mulI(off, th);
       for (int j = rg.x; j < rg.y; ++j) {
         V3<T> dr = pp - ld3(pos, j) - o;
-        T r = pair_r(pair_r2(dr.x, dr.y, dr.z));
+        const T r2 = pair_r2(dr.x, dr.y, dr.z);
+        if (!(r2 < P.r2_prefilter)) continue;
+        T r = pair_r(r2);
         T q = r * P.i_h;
         if (q < T(2.0f)) {
           T ker = kernel_w(P.knorm, q);
