@@ -277,6 +277,10 @@ template <class T> struct Engine final : EngineBase {
       S.nbg_cnt = dalloc<int>(np - npb);
     }
     S.dacc = dalloc<float>(np);
+    if (npb > 0 && (size_t)IX_CAP * npb < ((size_t)1 << 31)) {  // boundary lists (Adami)
+      S.nbb = dalloc<unsigned>((size_t)IX_CAP * npb);
+      S.nbb_cnt = dalloc<int>(npb);
+    }
     d_clstats = dalloc<double>(4);
     d_count = dalloc<unsigned long long>(1);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

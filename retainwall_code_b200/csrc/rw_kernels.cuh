@@ -87,8 +87,13 @@ template <class T> struct DevState {
   int* nbg_cnt;
   int nbg_stride;
   float* dacc;    // per slot: bound on the distance moved since the lists were built (not permuted)
+  unsigned* nbb;  // boundary particles' kept lists (entry e of particle i at nbb[e * npb + i])
+  int* nbb_cnt;
   unsigned char* near_wall;  // per cell: a contact-wall particle lies in its 27-cell neighbourhood
 };
+
+// Interaction block size; capacity of a kept candidate list (entries per particle).
+constexpr int IX_THREADS = 128, IX_CAP = 96;
 
 template <class T> RWD V3<T> ld3(const V4<T>* p, int i) { V4<T> v = p[i]; return {v.x, v.y, v.z}; }
 template <class T> RWD S6<T> ld6(const V4<T>* a, const V2<T>* b, int i) {
@@ -510,55 +515,72 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
   V4<T> rps{T(0), T(0), T(0), T(0)}, rvr{T(0), T(0), T(0), T(0)};
   V3<T> n_i{T(0), T(0), T(0)};
   const T th = P.two_h;
-  auto scan = [&](const I3 cc, const V3<T> pp) {
-  for (int oc = 0; oc < 27; ++oc) {
-    const I3 off = off_of(oc);
-    const I3 cj{cc.x + off.x, cc.y + off.y, cc.z + off.z};
-    if (!in_grid(P, cj)) continue;
-    const int k = key_of(P, cj);
-    const V3<T> o = mulI(off, th);
-    if (contact) {
-      const int2 rg = S.range[k];
-      for (int j = rg.x; j < rg.y; ++j) {
-        V3<T> dr = pp - ld3(pos, j);
-        dr = dr - o;
-        const T r2 = pair_r2(dr.x, dr.y, dr.z);
-        if (!(r2 < P.r2_prefilter)) continue;  // conservative: q >= 2 beyond it
-        T r = pair_r(r2);
-        T q = r * P.i_h;
-        if (q < T(2.0f)) {
-          T dwdr = kernel_f(P.kgrad, q);
-          V3<T> gker = dr * dwdr;
-          n_i = n_i - gker * P.vol_def;
+  // One neighbour j at dr = (pos_i - pos_j) - offset 2h: boundary j (contact walls
+  // only) feeds the wall normal, material j the extrapolation sums.
+  auto pair = [&](int j, const V3<T> dr, const T r2) {
+    if (!(r2 < P.r2_prefilter)) return;  // conservative: q >= 2 beyond it
+    const T r = pair_r(r2);
+    const T q = r * P.i_h;
+    if (!(q < T(2.0f))) return;
+    if (j < P.npb) {
+      T dwdr = kernel_f(P.kgrad, q);
+      V3<T> gker = dr * dwdr;
+      n_i = n_i - gker * P.vol_def;
+    } else {
+      T ker = kernel_w(P.knorm, q);
+      V4<T> vj = vel[j];
+      T mj = idm[j].y;
+      T vol_j = mj / vj.w;
+      T kv = ker * vol_j;
+      rs = rs + ld6(sa, sb, j) * kv;
+      rps = rps + v4(dr * (ker * mj), kv);
+      rvr = rvr + vj * kv;
+    }
+  };
+  // The 27 cells in the reference's order; with `keep`, the candidates within the list
+  // radius are recorded (same order) for later sections.
+  auto scan = [&](const I3 cc, const V3<T> pp, bool keep) {
+    int cnt = 0;
+    for (int oc = 0; oc < 27; ++oc) {
+      const I3 off = off_of(oc);
+      const I3 cj{cc.x + off.x, cc.y + off.y, cc.z + off.z};
+      if (!in_grid(P, cj)) continue;
+      const int k = key_of(P, cj);
+      const V3<T> o = mulI(off, th);
+      for (int layer = contact ? 0 : 1; layer < 2; ++layer) {
+        const int2 rg = S.range[layer ? k + P.ncell_material : k];
+        for (int j = rg.x; j < rg.y; ++j) {
+          V3<T> dr = pp - ld3(pos, j);
+          dr = dr - o;
+          const T r2 = pair_r2(dr.x, dr.y, dr.z);
+          if (keep && r2 < P.r2_list) {
+            if (cnt < IX_CAP) S.nbb[(size_t)cnt * P.npb + i] = (unsigned)j | ((unsigned)oc << 27);
+            ++cnt;
+          }
+          pair(j, dr, r2);
         }
       }
     }
-    const int2 rg = S.range[k + P.ncell_material];
-    for (int j = rg.x; j < rg.y; ++j) {
-      V3<T> dr = pp - ld3(pos, j);
-      dr = dr - o;
-      const T r2 = pair_r2(dr.x, dr.y, dr.z);
-      if (!(r2 < P.r2_prefilter)) continue;
-      T r = pair_r(r2);
-      T q = r * P.i_h;
-      if (q < T(2.0f)) {
-        T ker = kernel_w(P.knorm, q);
-        V4<T> vj = vel[j];
-        T mj = idm[j].y;
-        T vol_j = mj / vj.w;
-        T kv = ker * vol_j;
-        rs = rs + ld6(sa, sb, j) * kv;
-        rps = rps + v4(dr * (ker * mj), kv);
-        rvr = rvr + vj * kv;
-      }
-    }
-  }
+    if (keep) S.nbb_cnt[i] = cnt <= IX_CAP ? cnt : -1;
   };
-  scan(celli, pos_i);
+  const bool keep = S.nbb && P.keep_lists;
+  const int mode = keep ? dyn->ix_mode : 0;
+  const int kept = mode == 1 ? S.nbb_cnt[i] : -1;
+  if (kept >= 0) {  // walk the kept list
+    for (int e = 0; e < kept; ++e) {
+      const unsigned ent = S.nbb[(size_t)e * P.npb + i];
+      const int j = (int)(ent & 0x7ffffffu);
+      V3<T> dr = pos_i - ld3(pos, j);
+      dr = dr - mulI(off_of((int)(ent >> 27)), th);
+      pair(j, dr, pair_r2(dr.x, dr.y, dr.z));
+    }
+  } else {
+    scan(celli, pos_i, mode == 0 && keep);
+  }
   if (P.periodbound) {
     I3 cpb;
     V3<T> ppb;
-    if (period_image(P, celli, pos_i, true, cpb, ppb)) scan(cpb, ppb);
+    if (period_image(P, celli, pos_i, true, cpb, ppb)) scan(cpb, ppb, false);
   }
   if (enorm(n_i) > T(0)) {
     T nn = enorm(n_i);
@@ -860,7 +882,6 @@ template <bool Strict, class T> RWD void ix_begin(const Params<T>& P, const DevS
   A.gv = F9<T>{T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
 }
 
-constexpr int IX_THREADS = 128, IX_CAP = 96;
 
 // Pair sums of particle i straight from global memory: phase 1 lists candidates in
 // shared memory (my[k * stride]), phase 2 evaluates them in order.
