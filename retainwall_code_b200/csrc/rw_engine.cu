@@ -89,6 +89,7 @@ template <class T> struct Engine final : EngineBase {
   double* d_clstats = nullptr;
   unsigned long long* d_count = nullptr;
   int nsm = 148;
+  size_t near_wall_words = 0;
 
   ~Engine() override {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -269,7 +270,8 @@ template <class T> struct Engine final : EngineBase {
     S.col_len = dalloc<int>(ncol);
     S.col_cnt = dalloc<int>(ncol);
     S.col_off = dalloc<int>(ncol);
-    S.near_wall = dalloc<unsigned char>(P.ncell_material);
+    near_wall_words = ((size_t)P.ncell_material + 3) / 4;
+    S.near_wall = reinterpret_cast<unsigned char*>(dalloc<unsigned>(near_wall_words));
     S.chunks = dalloc<Chunk>(max_chunks);
     S.nbg_stride = (int)(np - npb);
     if ((size_t)IX_CAP * (np - npb) < ((size_t)1 << 31)) {  // list indices stay 32-bit
@@ -338,6 +340,7 @@ template <class T> struct Engine final : EngineBase {
     d.time_f = (T)q.time;
     d.npm = q.npm;
     d.host_dirty = 1;  // soil neighbour records are first written by the corner search
+    d.cells_dirty = 1;
     for (int i = 0; i < P.n_motion; ++i) {
       const rw_motion& m = q.motion[i];
       Table<T>& tb = d.tab[i];
@@ -392,9 +395,12 @@ template <class T> struct Engine final : EngineBase {
     check_launch();
   }
   void neighbor_search(int section) override {
+    // Every kernel of the search returns at once when no particle changed cell since
+    // the last one (Dyn::cells_dirty): keys, order, ranges and counts then stand.
     const int np = P.np;
+    const int* dirty = &d_dyn->cells_dirty;
     k_keys<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
-    if (np > 1) k_check_sorted<<<nblk(np - 1, 256), 256, 0, st>>>(S.keys, np, need_ptr());
+    if (np > 1) k_check_sorted<<<nblk(np - 1, 256), 256, 0, st>>>(S.keys, np, need_ptr(), dirty);
     for (int pass = 0; pass < S.sort_passes; ++pass) {
       const int* ki = (pass & 1) ? S.tk : S.keys;
       const int* vi = (pass & 1) ? S.tv : S.vals;
@@ -405,18 +411,19 @@ template <class T> struct Engine final : EngineBase {
       k_rs_downsweep<<<S.ntiles, RS_THREADS, 0, st>>>(ki, vi, ko, vo, np, 8 * pass, S.hist, S.dtot, S.ntiles,
                                                       need_ptr());
     }
-    RW_CU(cudaMemsetAsync(S.range, 0, (size_t)P.ncell * sizeof(int2), st));
+    k_clear_if<<<2 * nsm, 256, 0, st>>>(reinterpret_cast<unsigned*>(S.range), 2 * (size_t)P.ncell, dirty);
     k_ranges<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
     k_count<T><<<1, 1, 0, st>>>(P, S, d_dyn);
     k_permute<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn, section, compat_contact ? 1 : 0);
-    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
     if (P.npb > 0) {  // cells near contact walls, for the corner search
-      RW_CU(cudaMemsetAsync(S.near_wall, 0, (size_t)P.ncell_material, st));
+      k_clear_if<<<nsm, 256, 0, st>>>(reinterpret_cast<unsigned*>(S.near_wall), near_wall_words, dirty);
       k_mark_near_wall<T><<<nblk(P.npb, 256), 256, 0, st>>>(P, S, d_dyn);
     }
+    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
     if (ix_kernel == 1) chunk_list();
     check_launch();
   }
+
   // Column chunks of the chunked interaction kernel (rebuilt after every search while
   // that kernel is selected).
   void chunk_list() {
@@ -630,7 +637,8 @@ template <class T> struct Engine final : EngineBase {
   // Kernels launched by one whole step (launch_step), for launch accounting.
   int kernels_per_step() const {
     // keys, check, sort, ranges, count, permute, flip, contact-wall cells, chunks
-    const int search = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 1 : 0) + (ncol > 0 && ix_kernel == 1 ? 3 : 0);
+    // keys, check, sort, clear + ranges, count, permute, [clear + near-wall marks], flip, [chunks]
+    const int search = 2 + 3 * S.sort_passes + 5 + (P.npb > 0 ? 2 : 0) + (ncol > 0 && ix_kernel == 1 ? 3 : 0);
     const int ix = ix_kernel == 1 ? 1 : 2;             // chunked, or scan + walk
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
@@ -985,6 +993,7 @@ template <class T> struct Engine final : EngineBase {
     d.list_ok = 0;
     d.ix_mode = 0;
     d.host_dirty = 1;
+    d.cells_dirty = 1;
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     RW_CU(cudaStreamSynchronize(st));
   }
@@ -999,6 +1008,7 @@ template <class T> struct Engine final : EngineBase {
     d.list_ok = 0;
     d.ix_mode = 0;
     d.host_dirty = 1;
+    d.cells_dirty = 1;
     RW_CU(cudaMemcpyAsync(d_dyn, &d, sizeof(d), cudaMemcpyHostToDevice, st));
     RW_CU(cudaStreamSynchronize(st));
   }

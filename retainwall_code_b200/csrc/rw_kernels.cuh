@@ -146,7 +146,7 @@ template <class T> RWD void write_rec(const Params<T>& P, Rec<T>* rec, int i, V4
 template <class T> __global__ void k_keys(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) dyn->need_sort = 0;
-  if (i >= P.np) return;
+  if (i >= P.np || !dyn->cells_dirty) return;  // no cell changed: keys, order and ranges stand
   const int c = dyn->cur_main;
   int4 cp = S.cellpos[c][i];
   int key;
@@ -168,9 +168,16 @@ template <class T> __global__ void k_keys(const Params<T> P, DevState<T> S, Dyn<
   S.vals[i] = i;
 }
 
-static __global__ void k_check_sorted(const int* keys, int n, int* need_sort) {
+static __global__ void k_check_sorted(const int* keys, int n, int* need_sort, const int* dirty = nullptr) {
+  if (dirty && !*dirty) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (i < n && keys[i - 1] > keys[i]) *need_sort = 1;
+}
+
+// Clears n words when the cells changed since the last search.
+static __global__ void k_clear_if(unsigned* p, size_t n, const int* dirty) {
+  if (!*dirty) return;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) p[k] = 0u;
 }
 
 constexpr int RS_THREADS = 256, RS_ITEMS = 8, RS_TILE = RS_THREADS * RS_ITEMS;
@@ -289,7 +296,7 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const int* k
 // cuFindBegEndInCell (src/loquat_grid.cu:185-213): [beg, end) of every occupied cell.
 template <class T> __global__ void k_ranges(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.np) return;
+  if (i >= P.np || !dyn->cells_dirty) return;
   const int* K = dyn->need_sort ? S.skeys : S.keys;
   const int k = K[i];
   int* r = reinterpret_cast<int*>(S.range);
@@ -299,6 +306,7 @@ template <class T> __global__ void k_ranges(const Params<T> P, DevState<T> S, co
 
 // Deleted-particle accounting (src/loquat_grid.cu:234-254), on the device.
 template <class T> __global__ void k_count(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
+  if (!dyn->cells_dirty) return;
   int2 d = S.range[P.ncell_delete_m];
   int cnt = d.y - d.x;
   if (cnt > 0) {
@@ -379,6 +387,7 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
   if (section >= 0) {
     if (dyn->need_sort || dyn->host_dirty) dyn->rec_stale = 1;  // until the next interaction
     dyn->host_dirty = 0;
+    dyn->cells_dirty = 0;  // the search is complete
     const int reuse = (!dyn->need_sort && dyn->list_ok && !dyn->list_kill) ? 1 : 0;
     dyn->ix_mode = reuse;
     dyn->n_reuse += reuse;
@@ -639,7 +648,7 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
 // near_wall is cleared before each search's marking.
 template <class T> __global__ void k_mark_near_wall(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.npb) return;
+  if (i >= P.npb || !dyn->cells_dirty) return;
   const int c = dyn->cur_main;
   if (S.codes[c][i].x < 10) return;
   const int4 cp = S.cellpos[c][i];
@@ -1490,6 +1499,7 @@ template <class T> RWD void list_account(const Params<T>& P, const DevState<T>& 
                                          int cell_moved) {
   const float d = S.dacc[i] + step + P.disp_eps;
   S.dacc[i] = d;
+  if (cell_moved) const_cast<Dyn<T>*>(dyn)->cells_dirty = 1;
   if (cell_moved || d > P.disp_lim) const_cast<Dyn<T>*>(dyn)->list_kill = 1;
 }
 

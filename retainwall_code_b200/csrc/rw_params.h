@@ -83,6 +83,10 @@ template <class T> struct Dyn {
   // them after a permutation or a host write (rec_stale: set by the search, cleared by
   // the interaction that follows).
   int rec_stale, host_dirty;
+  // Some particle changed cell (or the host wrote the state) since the last search:
+  // keys, ranges and counts must be recomputed.  Set by the corrector, cleared at the
+  // end of each search.
+  int cells_dirty, pad2_;
   Motion<T> mv[kMotionMax];
   Table<T> tab[kMotionMax];
 };
