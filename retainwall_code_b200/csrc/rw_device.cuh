@@ -233,8 +233,10 @@ template <class T> RWD void mat_muidp(T dt, V3<T> om, S6<T> D, S6<T>& sigma, con
   sigma = dev + ident6<T>() * sph;
 }
 
-template <class T> struct HypoC { T C1, a, C2, C3, C4; };
-// C1..C4 of src/constitutive_model.h:149-153 and :226-230.
+// Material constants of the hypoplastic update (HypoC, rw_params.h): C1..C4 and a of
+// src/constitutive_model.h:149-153 and :226-230, and the ratios fa, fb, fc and t1 of the
+// cone projection (:276-279).  They depend on the material only, so the step evaluates
+// them once per material on the device (Params::hypo) with these same expressions.
 template <class T> RWD HypoC<T> hypo_coef(T Ei, T Vi, T phi_c, T p_ref) {
   HypoC<T> c;
   c.C1 = (T)(-(double)Ei / (3.0 * (double)p_ref * (double)(T(1) + Vi)));
@@ -243,13 +245,21 @@ template <class T> RWD HypoC<T> hypo_coef(T Ei, T Vi, T phi_c, T p_ref) {
                              (double)(c.a * c.a) / 3.0));
   c.C3 = c.a * c.a * c.C1;
   c.C4 = c.a * c.C1;
+  c.fa = c.C2 / c.C1;
+  c.fb = c.C3 / c.C1;
+  c.fc = c.C4 / c.C1;
+  c.t1 = 1.0 + (double)c.fa + (double)c.fb / 3.0;
   return c;
+}
+template <class T> RWD HypoC<T> hypo_coef(const T* mp, const HypoC<T>* pre) {
+  return pre ? *pre : hypo_coef(mp[0], mp[1], mp[2], mp[4]);
 }
 
 // cuMatModHypo (basic), src/constitutive_model.h:136-202.
-template <class T> RWD void mat_hypo_basic(T dt, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, bool dnorm = false) {
-  T Ei = mp[0], Vi = mp[1], phi_c = mp[2], coh = mp[3], p_ref = mp[4];
-  HypoC<T> c = hypo_coef(Ei, Vi, phi_c, p_ref);
+template <class T> RWD void mat_hypo_basic(T dt, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, bool dnorm = false,
+                                           const HypoC<T>* pre = nullptr) {
+  T coh = mp[3];
+  HypoC<T> c = hypo_coef(mp, pre);
   F9<T> sf = sym2full(sigma);
   if (coh > T(0)) sf = sf - identF<T>() * coh;
   S6<T> jau = jaumann(om, sf);
@@ -291,10 +301,10 @@ template <class T> struct HypoPre {
 
 // false: the zero-stress reset branch (I1 > -4) was taken and sigma is final.
 template <class T> RWD bool hypo_cs_pre(T density, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, T& M_crt, bool dnorm,
-                                        HypoPre<T>& h) {
-  T Ei = mp[0], Vi = mp[1], phi_c = mp[2], coh = mp[3], p_ref = mp[4], void_co = mp[5], lambda = mp[6];
+                                        HypoPre<T>& h, const HypoC<T>* pre = nullptr) {
+  T coh = mp[3], p_ref = mp[4], void_co = mp[5], lambda = mp[6];
   T xi = mp[7], alpha = mp[8], void_min = mp[9], void_max = mp[10], void_0 = mp[11], rho0 = mp[12];
-  h.c = hypo_coef(Ei, Vi, phi_c, p_ref);
+  h.c = hypo_coef(mp, pre);
   h.coh = coh;
   F9<T> sf = sym2full(sigma);
   if (coh > T(0)) sf = sf - identF<T>() * coh;
@@ -341,8 +351,8 @@ template <class T> RWD void hypo_cs_post(T dt, const HypoPre<T>& h, S6<T> rate, 
     return;
   }
   S6<T> dev = str - ident6<T>() * sph;
-  T fa = c.C2 / c.C1, fb = c.C3 / c.C1, fc = c.C4 / c.C1;
-  double t1 = 1.0 + (double)fa + (double)fb / 3.0;
+  const T fa = c.fa, fb = c.fb, fc = c.fc;
+  const double t1 = c.t1;
   T A = (T)((double)(fd * fd * fc * fc) / 3.0 - t1 * t1);
   T B = (T)(2.0 * (double)fd * (double)fd * (double)fc * (double)fc * (t1 * t1 + 2.0 * (double)fa + 3.0) -
             4.0 * (double)fb * ((double)(T(1) + fa) + (double)fb / 3.0));
@@ -359,9 +369,9 @@ template <class T> RWD void hypo_cs_post(T dt, const HypoPre<T>& h, S6<T> rate, 
 }
 
 template <class T> RWD void mat_hypo_cs(T dt, T density, V3<T> om, S6<T> D, S6<T>& sigma, const T* mp, T& M_crt,
-                                        bool dnorm = false) {
+                                        bool dnorm = false, const HypoC<T>* pre = nullptr) {
   HypoPre<T> h;
-  if (!hypo_cs_pre(density, om, D, sigma, mp, M_crt, dnorm, h)) return;
+  if (!hypo_cs_pre(density, om, D, sigma, mp, M_crt, dnorm, h, pre)) return;
   hypo_cs_post(dt, h, hypo_cs_rate(h, D), sigma);
 }
 
@@ -377,11 +387,11 @@ template <class T> RWD T rate_norm(S6<T> D, bool dnorm) {
 // Model dispatch of cuPredictorMaterial / cuCorrectorMaterial
 // (src/predictor_corrector.cu:72-75, :169-172).
 template <class T> RWD void constitutive(int model, const T* mp, T dt, T rho, V3<T> om, S6<T> D, S6<T>& sig,
-                                         bool& yld, T& M_crt, bool dnorm = false) {
+                                         bool& yld, T& M_crt, bool dnorm = false, const HypoC<T>* pre = nullptr) {
   if (model == RW_MODEL_DP) mat_dp(dt, om, D, sig, mp, yld);
   else if (model == RW_MODEL_MUIDP) mat_muidp(dt, om, D, sig, mp);
-  else if (model == RW_MODEL_HYPO_BASIC) mat_hypo_basic(dt, om, D, sig, mp, dnorm);
-  else if (model == RW_MODEL_HYPO_CS) mat_hypo_cs(dt, rho, om, D, sig, mp, M_crt, dnorm);
+  else if (model == RW_MODEL_HYPO_BASIC) mat_hypo_basic(dt, om, D, sig, mp, dnorm, pre);
+  else if (model == RW_MODEL_HYPO_CS) mat_hypo_cs(dt, rho, om, D, sig, mp, M_crt, dnorm, pre);
 }
 
 // Compensated (Kahan) accumulation s += x with running compensation c.  Explicit

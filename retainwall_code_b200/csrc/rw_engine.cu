@@ -283,6 +283,13 @@ template <class T> struct Engine final : EngineBase {
       S.nbb = dalloc<unsigned>((size_t)IX_CAP * npb);
       S.nbb_cnt = dalloc<int>(npb);
     }
+    {  // hypoplastic material constants, evaluated on the device as the kernels would
+      HypoC<T>* tab = dalloc<HypoC<T>>(kModelMax);
+      k_hypo_table<T><<<1, 32, 0, st>>>(P, tab);
+      RW_CU(cudaGetLastError());
+      RW_CU(cudaMemcpyAsync(P.hypo, tab, sizeof(P.hypo), cudaMemcpyDeviceToHost, st));
+      RW_CU(cudaStreamSynchronize(st));
+    }
     d_clstats = dalloc<double>(4);
     d_count = dalloc<unsigned long long>(1);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

@@ -1468,7 +1468,8 @@ template <class T> __global__ void k_predictor(const Params<T> P, DevState<T> S,
   bool yld = false;
   T mcrt = T(0);
   const bool by_closure = P.closure && code.z == RW_MODEL_HYPO_CS;  // k_closure updates the stress
-  if (!by_closure) constitutive(code.z, mp, hdt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
+  const HypoC<T> hc = P.hypo[code.w];
+  if (!by_closure) constitutive(code.z, mp, hdt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0, &hc);
   S.pos[c][i] = ps;
   S.vel[c][i] = vr;
   st6(S.stn_a[c], S.stn_b[c], i, sn);
@@ -1582,7 +1583,8 @@ template <class T> __global__ void k_corrector(const Params<T> P, DevState<T> S,
   bool yld = false;
   T mcrt = T(0);
   const bool by_closure = P.closure && code.z == RW_MODEL_HYPO_CS;  // k_closure updates the stress
-  if (!by_closure) constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0);
+  const HypoC<T> hc = P.hypo[code.w];
+  if (!by_closure) constitutive(code.z, mp, P.dt, vr.w, xyz(S.spin[i]), D, sg, yld, mcrt, P.mixed != 0, &hc);
   if (!yld) id.x = T(100);
   id.w = mcrt;
   if (!in_grid(P, I3{cp.x, cp.y, cp.z})) {
@@ -1767,6 +1769,12 @@ static __global__ void k_wall_force_final(double* wsum, int nblocks) {
 }
 
 // Totals of the kept candidate lists: out[0] += entries, out[1] += soil particles with a list.
+// Per-material constants of the hypoplastic update, once per case (rw_device.cuh).
+template <class T> __global__ void k_hypo_table(const Params<T> P, HypoC<T>* out) {
+  const int m = threadIdx.x;
+  if (m < kModelMax) out[m] = hypo_coef(P.model_par[m][0], P.model_par[m][1], P.model_par[m][2], P.model_par[m][4]);
+}
+
 static __global__ void k_list_totals(const int* cnt, int n, unsigned long long* out) {
   unsigned long long e = 0, p = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
@@ -1929,7 +1937,9 @@ __global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevSta
         S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
         HypoPre<T> h;
         T mcrt;
-        if (hypo_cs_pre(S.vel[c][i].w, V3<T>{T(0), T(0), T(0)}, D, sg, mp, mcrt, P.mixed != 0, h) && h.nD > T(0)) {
+        const HypoC<T> hc = P.hypo[code.w];
+        if (hypo_cs_pre(S.vel[c][i].w, V3<T>{T(0), T(0), T(0)}, D, sg, mp, mcrt, P.mixed != 0, h, &hc) &&
+            h.nD > T(0)) {
           closure_features(h, D, mp, f);
           act = true;
 #pragma unroll
@@ -1955,7 +1965,8 @@ __global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevSta
       S6<T> sg = ld6(S.str_a[c], S.str_b[c], i);
       HypoPre<T> h;
       T mcrt = T(0);
-      if (hypo_cs_pre(S.vel[c][i].w, V3<T>{om4.x, om4.y, om4.z}, D, sg, mp, mcrt, P.mixed != 0, h)) {
+      const HypoC<T> hc = P.hypo[code.w];
+      if (hypo_cs_pre(S.vel[c][i].w, V3<T>{om4.x, om4.y, om4.z}, D, sg, mp, mcrt, P.mixed != 0, h, &hc)) {
         S6<T> rate;
         bool use = act && !sm.err;
 #pragma unroll

@@ -36,6 +36,12 @@ template <class T> struct Table {  // MotionTable (src/types.h:77-97)
   Vec3<T> pos_rp, rotat_vel;
 };
 
+// Per-material constants of the hypoplastic update (see hypo_coef).
+template <class T> struct HypoC {
+  T C1, a, C2, C3, C4, fa, fb, fc;
+  double t1;
+};
+
 template <class T> struct Params {
   int dim, periodbound, n_motion, n_model;
   int np, npb, npm0;        // particle counts at set-up (np, npb never change)
@@ -58,6 +64,7 @@ template <class T> struct Params {
   float disp_eps;            // rounding allowance added per position update
   int keep_lists;            // 0: every interaction scans the cells
   int closure;               // 1: HypoCS stress updates by the learned closure (k_closure)
+  HypoC<T> hypo[kModelMax];  // per-material constants, evaluated once on the device
   int mixed;                 // precision form: compensated integration, FP64 strain-rate norm
   int pad_m;
 };
