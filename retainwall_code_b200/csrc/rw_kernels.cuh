@@ -132,7 +132,17 @@ template <class T> RWD void write_rec(const Params<T>& P, Rec<T>* rec, int i, V4
   r.vr = vr;
   r.a = V4<T>{mass, contact ? -vol : vol, sor.xx, sor.yy};
   r.b = V4<T>{sor.zz, sor.xy, sor.xz, sor.yz};
-  rec[i] = r;
+  if constexpr (sizeof(T) == 4) {  // two 256-bit stores (sm_100)
+    float* q = reinterpret_cast<float*>(rec + i);
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(q), "f"(r.p.x), "f"(r.p.y), "f"(r.p.z),
+                 "f"(r.p.w), "f"(r.vr.x), "f"(r.vr.y), "f"(r.vr.z), "f"(r.vr.w)
+                 : "memory");
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(q + 8), "f"(r.a.x), "f"(r.a.y),
+                 "f"(r.a.z), "f"(r.a.w), "f"(r.b.x), "f"(r.b.y), "f"(r.b.z), "f"(r.b.w)
+                 : "memory");
+  } else {
+    rec[i] = r;
+  }
 }
 
 // ---------------------------------------------------------------------------------
@@ -770,6 +780,21 @@ template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) 
   v.vr = rec[j].vr;
   v.a = rec[j].a;
   v.b = rec[j].b;
+  return v;
+}
+// Float records: two 256-bit loads (sm_100) instead of four 128-bit ones.  Half the load
+// instructions and L1 requests per neighbour; the walk kernel's L1 request rate is what
+// bounds it.  Records are 64 bytes from a 256-byte aligned cudaMalloc base.
+static_assert(sizeof(Rec<float>) == 64, "float records are one 64-byte line");
+template <> RWD NbVals<float> load_nb<float>(const Rec<float>* __restrict__ rec, int j) {
+  NbVals<float> v;
+  const float* q = reinterpret_cast<const float*>(rec + j);
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(v.p.x), "=f"(v.p.y), "=f"(v.p.z), "=f"(v.p.w), "=f"(v.vr.x), "=f"(v.vr.y), "=f"(v.vr.z), "=f"(v.vr.w)
+      : "l"(q));
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(v.a.x), "=f"(v.a.y), "=f"(v.a.z), "=f"(v.a.w), "=f"(v.b.x), "=f"(v.b.y), "=f"(v.b.z), "=f"(v.b.w)
+      : "l"(q + 8));
   return v;
 }
 
