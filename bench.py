@@ -29,11 +29,19 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-updates/s/GPU at 1.92M particles"
 # From the ncu capture of the interaction's walk kernel on the 0.96M-particle case
-# (profiles/k_interaction_wall2_half.md): DRAM read+write 461.4 + 65.5 MB and 369.1M warp
+# (profiles/k_interaction_wall2_half.md): DRAM read+write 461.4 + 64.6 MB and 331.1M warp
 # instructions per launch.  Both grow with the particle count, so they are scaled per
 # soil particle to the benchmarked case.
-IX_DRAM_BYTES_PER_SOIL = (461.38e6 + 65.50e6) / 960000
-IX_WARP_INSTR_PER_SOIL = 369.13e6 / 960000
+IX_DRAM_BYTES_PER_SOIL = (461.39e6 + 64.64e6) / 960000
+IX_WARP_INSTR_PER_SOIL = 331.09e6 / 960000
+# L1 data-stage wavefronts the walk kernel cannot avoid: each listed neighbour's 64-byte
+# record is two 32-byte sectors read by one lane (records of a warp's lanes are distinct),
+# each list entry an eighth of a sector (a warp's 32 entries are one coalesced 128-byte
+# load), each particle's own state and outputs about 240 B.  The L1 data stage retires one
+# wavefront per cycle per SM, and scattered sectors cost one wavefront each (ncu: 122.5M
+# sectors requested, 134M wavefronts with the shared-memory ones, 87% of peak).
+IX_L1_SECTORS_PER_ENTRY = 2 + 1 / 8
+IX_L1_SECTORS_PER_SOIL = 240 / 32
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
@@ -345,7 +353,7 @@ def run_ours(args, ws, rank, local):
     roof = {"bound": "hbm", "kernel": "k_interaction", "achieved": achieved, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": kind,
             "traffic": IX_DRAM_BYTES_PER_SOIL * npm, "algorithmic_bytes_per_launch": ib, "launch_ms": ix_ms,
-            "note": "not HBM-bound: gather latency and pair arithmetic; see the issue entry"}
+            "note": "not HBM-bound: bound by the L1 data stage (record gathers), see roofline_l1"}
     # whole step against the compulsory traffic of the algorithm: FP32 compact state of
     # 104 B per soil particle moved through two sections (bin, sort, permute, contact
     # preparation, interaction + integration) = 1276 B per soil particle, 644 B per
@@ -362,6 +370,12 @@ def run_ours(args, ws, rank, local):
     issue = {"bound": "instruction issue", "kernel": "k_interaction", "achieved": issue_ach, "peak": issue_peak,
              "unit": "warp-instructions/s", "frac": issue_ach / issue_peak,
              "note": "instructions per launch from the ncu capture, scaled per soil particle"}
+    l1_sectors = IX_L1_SECTORS_PER_ENTRY * list_entries + IX_L1_SECTORS_PER_SOIL * npm
+    l1_peak = 148 * mhz * 1e6  # one L1 data-stage wavefront per cycle per SM
+    roof_l1 = {"bound": "L1 data stage", "kernel": "k_interaction", "achieved": l1_sectors / (ix_ms * 1e-3),
+               "peak": l1_peak, "unit": "sectors/s", "frac": l1_sectors / (ix_ms * 1e-3) / l1_peak,
+               "sectors_per_launch": l1_sectors,
+               "note": "2 sectors per listed neighbour (64-B record) + 1/8 per list entry + 7.5 per particle"}
     line = {
         "metric": METRIC, "value": value, "unit": "particle-updates/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -371,6 +385,7 @@ def run_ours(args, ws, rank, local):
         "e2e": {"value": e2e, "unit": "particle-updates/s", "h2d_bytes_per_step": int(h2d / e2e_steps),
                 "d2h_bytes_per_step": 24, "note": "case upload from host + per-step rw_step + wall-force read"},
         "roofline": roof,
+        "roofline_l1": roof_l1,
         "roofline_issue": issue,
         "roofline_step": roof_step,
         "stage_ms": stages,

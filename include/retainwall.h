@@ -123,7 +123,10 @@ typedef struct rw_info {
   int32_t cell_num[3], n_motion;
   double time, dt, h, dr;
   int32_t n_sorts;       /* neighbour-search sections whose sort permuted the particles     */
-  int32_t n_list_reuse;  /* corrector-section interactions that walked the predictor's lists */
+  int32_t n_list_reuse;  /* interactions that walked kept candidate lists                    */
+  int32_t n_search_skipped; /* captured-step searches skipped whole (no particle changed cell)  */
+  int32_t n_scan_skipped;   /* captured-step interactions whose scan launch was skipped (every
+                               particle walked a kept list)                                      */
 } rw_info;
 
 typedef struct rw_ctx rw_ctx;

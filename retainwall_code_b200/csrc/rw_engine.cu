@@ -90,12 +90,16 @@ template <class T> struct Engine final : EngineBase {
   unsigned long long* d_count = nullptr;
   int nsm = 148;
   size_t near_wall_words = 0;
+  // Step graphs captured with conditional nodes (gated()); st_body captures their bodies.
+  bool allow_cond = false;
+  cudaStream_t st_body = nullptr;
 
   ~Engine() override {
     if (gexec) cudaGraphExecDestroy(gexec);
     if (st) cudaStreamSynchronize(st);
     for (void* p : allocs) cudaFree(p);
     if (st) cudaStreamDestroy(st);
+    if (st_body) cudaStreamDestroy(st_body);
   }
 
   template <class X> X* dalloc(size_t n) {
@@ -122,6 +126,52 @@ template <class T> struct Engine final : EngineBase {
     return d;
   }
   void check_launch() { RW_CU(cudaGetLastError()); }
+
+  // Work that often has nothing to do.  While a step graph is being captured (with
+  // conditional nodes allowed), body() goes into the body of an IF node and gate(h)
+  // launches the one-thread kernel that sets its condition on the device, so a skipped
+  // body costs one small launch instead of a launch per kernel.  Otherwise body() is
+  // launched as it is and its kernels return at once on their own.
+  template <class Gate, class Body> void gated(Gate gate, Body body) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    RW_CU(cudaStreamIsCapturing(st, &cs));
+    if (!allow_cond || cs != cudaStreamCaptureStatusActive) {
+      body();
+      return;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    RW_CU(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    RW_CU(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    gate(h);
+    check_launch();
+    RW_CU(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    RW_CU(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    if (!st_body) RW_CU(cudaStreamCreateWithFlags(&st_body, cudaStreamNonBlocking));
+    RW_CU(cudaStreamBeginCaptureToGraph(st_body, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+    std::swap(st, st_body);  // the body's launches go to the body graph
+    try {
+      body();
+    } catch (...) {
+      std::swap(st, st_body);
+      cudaGraph_t bg = nullptr;
+      cudaStreamEndCapture(st_body, &bg);
+      throw;
+    }
+    std::swap(st, st_body);
+    cudaGraph_t bg = nullptr;
+    RW_CU(cudaStreamEndCapture(st_body, &bg));  // the body graph belongs to the node
+    RW_CU(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  }
 
   // ------------------------------------------------------------------------------
   // Set-up: InitializeParameters (src/loquat.cu:130-190), AllocateGpuMemory,
@@ -296,50 +346,43 @@ template <class T> struct Engine final : EngineBase {
     RW_CU(cudaMemsetAsync(S.dacc, 0, np * sizeof(float), st));
     d_dyn = dalloc<Dyn<T>>(1);
 
-    // Host-side conversion to structure-of-arrays, with the reference's
-    // absolute -> in-cell position arithmetic (src/loquat_grid.cu:322-330).
-    std::vector<int4> h_codes(np), h_cell(np);
-    std::vector<V4<T>> h_pos(np), h_ori(np), h_vel(np), h_idm(np), h_nrm(npb);
-    std::vector<V4<T>> h_sa(np), h_na(np);
-    std::vector<V2<T>> h_sb(np), h_nb(np);
-    const T half_ih = (T)(0.5 * (double)P.i_h);
-    for (size_t i = 0; i < np; ++i) {
-      const int32_t* cc = c->codes + 4 * i;
-      h_codes[i] = int4{cc[0], cc[1], cc[2], cc[3]};
-      const double* a = c->pospres + 4 * i;
-      V4<T> pa{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
-      h_ori[i] = pa;
-      T sx = pa.x * half_ih, sy = pa.y * half_ih, sz = pa.z * half_ih;
-      int cx = (int)sx, cy = (int)sy, cz = (int)sz;
-      h_cell[i] = int4{cx, cy, cz, 0};
-      T ox = (T)cx * P.two_h, oy = (T)cy * P.two_h, oz = (T)cz * P.two_h;
-      h_pos[i] = V4<T>{pa.x - ox, pa.y - oy, pa.z - oz, pa.w};
-      a = c->velrhop + 4 * i;
-      h_vel[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
-      a = c->idmassidx + 4 * i;
-      h_idm[i] = V4<T>{(T)a[0], (T)a[1], (T)i, (T)a[3]};
-      a = c->stress + 6 * i;
-      h_sa[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
-      h_sb[i] = V2<T>{(T)a[4], (T)a[5]};
-      a = c->strain + 6 * i;
-      h_na[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
-      h_nb[i] = V2<T>{(T)a[4], (T)a[5]};
+    // The case arrays are uploaded as the caller holds them and converted on the device
+    // (k_ingest).  The staging area is the candidate-list buffer, unused until the first
+    // interaction builds the lists, or a temporary allocation when that is too small.
+    {
+      const size_t b_codes = np * 16, b4 = np * 4 * sizeof(double), b6 = np * 6 * sizeof(double);
+      const size_t b_nrm = npb * 4 * sizeof(double);
+      const size_t raw = b_codes + 3 * b4 + 2 * b6 + b_nrm;
+      unsigned char* stage = nullptr;
+      bool temp = false;
+      if (S.nbg && (size_t)IX_CAP * (np - npb) * sizeof(unsigned) >= raw) {
+        stage = reinterpret_cast<unsigned char*>(S.nbg);
+      } else {
+        RW_CU(cudaMalloc(reinterpret_cast<void**>(&stage), raw));
+        temp = true;
+      }
+      size_t off = 0;
+      auto put = [&](const void* h, size_t n) -> const void* {
+        unsigned char* d = stage + off;
+        if (n) RW_CU(cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, st));
+        off += n;
+        return d;
+      };
+      RawCase R;
+      R.codes = static_cast<const int4*>(put(c->codes, b_codes));
+      R.pospres = static_cast<const double*>(put(c->pospres, b4));
+      R.velrhop = static_cast<const double*>(put(c->velrhop, b4));
+      R.idmassidx = static_cast<const double*>(put(c->idmassidx, b4));
+      R.stress = static_cast<const double*>(put(c->stress, b6));
+      R.strain = static_cast<const double*>(put(c->strain, b6));
+      R.normal = static_cast<const double*>(put(npb ? c->normal : nullptr, b_nrm));
+      k_ingest<T><<<nblk((long)np, 256), 256, 0, st>>>(P, S, R, (T)(0.5 * (double)P.i_h));
+      RW_CU(cudaGetLastError());
+      if (temp) {
+        RW_CU(cudaStreamSynchronize(st));
+        RW_CU(cudaFree(stage));
+      }
     }
-    for (size_t i = 0; i < npb; ++i) {
-      const double* a = c->normal + 4 * i;
-      h_nrm[i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
-    }
-    up(S.codes[0], h_codes);
-    up(S.cellpos[0], h_cell);
-    up(S.pos[0], h_pos);
-    up(S.pos_ori[0], h_ori);
-    up(S.vel[0], h_vel);
-    up(S.idm[0], h_idm);
-    up(S.str_a[0], h_sa);
-    up(S.str_b[0], h_sb);
-    up(S.stn_a[0], h_na);
-    up(S.stn_b[0], h_nb);
-    up(S.normal[0], h_nrm);
 
     Dyn<T> d;
     std::memset(&d, 0, sizeof(d));
@@ -404,28 +447,31 @@ template <class T> struct Engine final : EngineBase {
   void neighbor_search(int section) override {
     // Every kernel of the search returns at once when no particle changed cell since
     // the last one (Dyn::cells_dirty): keys, order, ranges and counts then stand.
-    const int np = P.np;
-    const int* dirty = &d_dyn->cells_dirty;
-    k_keys<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
-    if (np > 1) k_check_sorted<<<nblk(np - 1, 256), 256, 0, st>>>(S.keys, np, need_ptr(), dirty);
-    for (int pass = 0; pass < S.sort_passes; ++pass) {
-      const int* ki = (pass & 1) ? S.tk : S.keys;
-      const int* vi = (pass & 1) ? S.tv : S.vals;
-      int* ko = (pass & 1) ? S.keys : S.tk;
-      int* vo = (pass & 1) ? S.vals : S.tv;
-      k_rs_upsweep<<<S.ntiles, RS_THREADS, 0, st>>>(ki, np, 8 * pass, S.hist, S.ntiles, need_ptr());
-      k_rs_scan<<<256, RS_THREADS, 0, st>>>(S.hist, S.ntiles, S.dtot, need_ptr());
-      k_rs_downsweep<<<S.ntiles, RS_THREADS, 0, st>>>(ki, vi, ko, vo, np, 8 * pass, S.hist, S.dtot, S.ntiles,
-                                                      need_ptr());
-    }
-    k_clear_if<<<2 * nsm, 256, 0, st>>>(reinterpret_cast<unsigned*>(S.range), 2 * (size_t)P.ncell, dirty);
-    k_ranges<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
-    k_count<T><<<1, 1, 0, st>>>(P, S, d_dyn);
-    k_permute<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn, section, compat_contact ? 1 : 0);
-    if (P.npb > 0) {  // cells near contact walls, for the corner search
-      k_clear_if<<<nsm, 256, 0, st>>>(reinterpret_cast<unsigned*>(S.near_wall), near_wall_words, dirty);
-      k_mark_near_wall<T><<<nblk(P.npb, 256), 256, 0, st>>>(P, S, d_dyn);
-    }
+    gated([&](cudaGraphConditionalHandle h) { k_search_gate<T><<<1, 1, 0, st>>>(d_dyn, h); },
+          [&] {
+            const int np = P.np;
+            const int* dirty = &d_dyn->cells_dirty;
+            k_keys<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
+            if (np > 1) k_check_sorted<<<nblk(np - 1, 256), 256, 0, st>>>(S.keys, np, need_ptr(), dirty);
+            for (int pass = 0; pass < S.sort_passes; ++pass) {
+              const int* ki = (pass & 1) ? S.tk : S.keys;
+              const int* vi = (pass & 1) ? S.tv : S.vals;
+              int* ko = (pass & 1) ? S.keys : S.tk;
+              int* vo = (pass & 1) ? S.vals : S.tv;
+              k_rs_upsweep<<<S.ntiles, RS_THREADS, 0, st>>>(ki, np, 8 * pass, S.hist, S.ntiles, need_ptr());
+              k_rs_scan<<<256, RS_THREADS, 0, st>>>(S.hist, S.ntiles, S.dtot, need_ptr());
+              k_rs_downsweep<<<S.ntiles, RS_THREADS, 0, st>>>(ki, vi, ko, vo, np, 8 * pass, S.hist, S.dtot, S.ntiles,
+                                                              need_ptr());
+            }
+            k_clear_if<<<2 * nsm, 256, 0, st>>>(reinterpret_cast<unsigned*>(S.range), 2 * (size_t)P.ncell, dirty);
+            k_ranges<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn);
+            k_count<T><<<1, 1, 0, st>>>(P, S, d_dyn);
+            k_permute<T><<<nblk(np, 256), 256, 0, st>>>(P, S, d_dyn, section, compat_contact ? 1 : 0);
+            if (P.npb > 0) {  // cells near contact walls, for the corner search
+              k_clear_if<<<nsm, 256, 0, st>>>(reinterpret_cast<unsigned*>(S.near_wall), near_wall_words, dirty);
+              k_mark_near_wall<T><<<nblk(P.npb, 256), 256, 0, st>>>(P, S, d_dyn);
+            }
+          });
     k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
     if (ix_kernel == 1) chunk_list();
     check_launch();
@@ -472,13 +518,14 @@ template <class T> struct Engine final : EngineBase {
         else k_interaction2<T, false><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
       } else {
         const unsigned g = nblk(n, IX_THREADS);
-        if (strict_fp) {
-          k_interaction<T, true, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
-          k_interaction<T, true, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
-        } else {
-          k_interaction<T, false, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
-          k_interaction<T, false, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
-        }
+        // the scan launch, skipped in a captured step when every particle walks a kept list
+        gated([&](cudaGraphConditionalHandle h) { k_scan_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
+              [&] {
+                if (strict_fp) k_interaction<T, true, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
+                else k_interaction<T, false, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
+              });
+        if (strict_fp) k_interaction<T, true, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
+        else k_interaction<T, false, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
       }
       check_launch();
     }
@@ -610,18 +657,23 @@ template <class T> struct Engine final : EngineBase {
   }
 
   // One whole step captured as a graph (not instantiated); the caller owns it.
-  cudaGraph_t capture_step() {
+  // cond: gate the search and the scan launch with conditional nodes (gated()).  The
+  // batched sweep nests step graphs as child graphs and captures them without.
+  cudaGraph_t capture_step(bool cond = false) {
     cudaGraph_t g = nullptr;
     const int c0 = cpar;
     RW_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    allow_cond = cond;
     try {
       launch_step();
     } catch (...) {
+      allow_cond = false;
       cudaStreamEndCapture(st, &g);
       if (g) cudaGraphDestroy(g);
       cpar = c0;
       throw;
     }
+    allow_cond = false;
     RW_CU(cudaStreamEndCapture(st, &g));
     cpar = c0;  // the step runs two interactions: parity is back where it started
     return g;
@@ -633,9 +685,15 @@ template <class T> struct Engine final : EngineBase {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
       }
-      cudaGraph_t g = capture_step();
+      cudaGraph_t g = capture_step(true);
       cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
       cudaGraphDestroy(g);
+      if (e != cudaSuccess) {  // a driver without conditional nodes: plain step graph
+        cudaGetLastError();
+        g = capture_step(false);
+        e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+      }
       RW_CU(e);
       g_cpar = cpar;
     }

@@ -145,6 +145,78 @@ template <class T> RWD void write_rec(const Params<T>& P, Rec<T>* rec, int i, V4
   }
 }
 
+// The neighbour-side values one pair term needs.
+template <class T> struct NbVals {
+  V4<T> p, vr, a, b;
+};
+template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) {
+  NbVals<T> v;
+  v.p = rec[j].p;
+  v.vr = rec[j].vr;
+  v.a = rec[j].a;
+  v.b = rec[j].b;
+  return v;
+}
+// Float records: two 256-bit loads (sm_100) instead of four 128-bit ones.  Half the load
+// instructions and L1 requests per neighbour; the walk kernel's L1 request rate is what
+// bounds it.  Records are 64 bytes from a 256-byte aligned cudaMalloc base.
+static_assert(sizeof(Rec<float>) == 64, "float records are one 64-byte line");
+template <> RWD NbVals<float> load_nb<float>(const Rec<float>* __restrict__ rec, int j) {
+  NbVals<float> v;
+  const float* q = reinterpret_cast<const float*>(rec + j);
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(v.p.x), "=f"(v.p.y), "=f"(v.p.z), "=f"(v.p.w), "=f"(v.vr.x), "=f"(v.vr.y), "=f"(v.vr.z), "=f"(v.vr.w)
+      : "l"(q));
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(v.a.x), "=f"(v.a.y), "=f"(v.a.z), "=f"(v.a.w), "=f"(v.b.x), "=f"(v.b.y), "=f"(v.b.z), "=f"(v.b.w)
+      : "l"(q + 8));
+  return v;
+}
+
+// ---------------------------------------------------------------------------------
+// Case ingest: the caller's arrays (array of structures, double) -> the device layout.
+// ---------------------------------------------------------------------------------
+struct RawCase {
+  const int4* codes;
+  const double* pospres;
+  const double* velrhop;
+  const double* idmassidx;
+  const double* stress;
+  const double* strain;
+  const double* normal;
+};
+
+// One particle of LoadParticles' conversion with the absolute -> in-cell split of
+// src/loquat_grid.cu:322-330: cell = trunc(x / 2h), in-cell position = x - cell * 2h.
+// Every product and difference is rounded on its own (no contraction), so the result
+// is the host arithmetic of the reference's loader, bit for bit.
+template <class T> __global__ void k_ingest(const Params<T> P, DevState<T> S, RawCase R, T half_ih) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)P.np) return;
+  S.codes[0][i] = R.codes[i];
+  const double* a = R.pospres + 4 * i;
+  const V4<T> pa{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+  S.pos_ori[0][i] = pa;
+  const int cx = (int)rmul(pa.x, half_ih), cy = (int)rmul(pa.y, half_ih), cz = (int)rmul(pa.z, half_ih);
+  S.cellpos[0][i] = int4{cx, cy, cz, 0};
+  S.pos[0][i] = V4<T>{add_rn(pa.x, -rmul((T)cx, P.two_h)), add_rn(pa.y, -rmul((T)cy, P.two_h)),
+                      add_rn(pa.z, -rmul((T)cz, P.two_h)), pa.w};
+  a = R.velrhop + 4 * i;
+  S.vel[0][i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+  a = R.idmassidx + 4 * i;
+  S.idm[0][i] = V4<T>{(T)a[0], (T)a[1], (T)i, (T)a[3]};
+  a = R.stress + 6 * i;
+  S.str_a[0][i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+  S.str_b[0][i] = V2<T>{(T)a[4], (T)a[5]};
+  a = R.strain + 6 * i;
+  S.stn_a[0][i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+  S.stn_b[0][i] = V2<T>{(T)a[4], (T)a[5]};
+  if (i < (size_t)P.npb) {
+    a = R.normal + 4 * i;
+    S.normal[0][i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // Cell list: keys, stable radix sort, ranges, gather-permute
 // (src/loquat_grid.cu:140-320, src/loquat.cu:254-287).
@@ -405,6 +477,7 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
       dyn->list_ok = 0;
       dyn->list_kill = 0;
       dyn->build_kill = section;
+      dyn->n_spill = 0;
     }
   }
   if (!rigid) return;
@@ -446,6 +519,31 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
       }
     }
   }
+}
+
+// Gates of a captured step graph: one-thread kernels that set the condition of the IF
+// node holding work that would otherwise launch only to return at once.
+// Search: keys, sort, ranges, counts, permutation and contact-wall cells have nothing to
+// do when no particle changed cell (what k_keys does then is clear need_sort).
+template <class T> __global__ void k_search_gate(Dyn<T>* dyn, cudaGraphConditionalHandle h) {
+  const int d = dyn->cells_dirty;
+  if (!d) {
+    dyn->need_sort = 0;
+    dyn->n_search_skipped += 1;
+  }
+  cudaGraphSetConditional(h, d ? 1u : 0u);
+}
+// Interaction scan launch: needed when the lists are being rebuilt, when some list of
+// the last build overflowed, or for deleted slots (their contact state is carried).
+template <class T>
+__global__ void k_scan_gate(const Params<T> P, DevState<T> S, Dyn<T>* dyn, cudaGraphConditionalHandle h) {
+  const int mode = (S.nbg && P.keep_lists) ? dyn->ix_mode : 0;
+  const bool run = mode != 1 || dyn->n_spill > 0 || dyn->npm < P.np - P.npb;
+  if (!run) {
+    dyn->rec_stale = 0;  // what the scan launch does first
+    dyn->n_scan_skipped += 1;
+  }
+  cudaGraphSetConditional(h, run ? 1u : 0u);
 }
 
 template <class T> __global__ void k_begin(Dyn<T>* dyn) { dyn->time_f = (T)dyn->time_d; }
@@ -699,42 +797,74 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
   V4<T> ny = S.cny[i];
   V4<T> vz = S.cvz[i];
   const T th = P.two_h;
-  {
+  // One boundary candidate j at in-cell position pj, in the cell at offset off (the body
+  // of the reference's scan).  contact(): j belongs to a contact wall; vel_of(): its
+  // velocity.
+  auto visit = [&](int j, const I3 off, const V3<T> pj, auto&& contact, auto&& vel_of) {
+    V3<T> dr = pos_i - pj - mulI(off, th);
+    const T r2 = pair_r2(dr.x, dr.y, dr.z);
+    if (!(r2 < P.r2_prefilter)) return;
+    T r = pair_r(r2);
+    T q = r * P.i_h;
+    if (!((double)q < 2.0)) return;
+    if (!contact()) return;
+    T dwdr = kernel_f(P.kgrad, q);
+    V3<T> gker = dr * dwdr;
+    if (r < d_ij && r > T(0)) {
+      const V4<T> na4 = S.cny[j];
+      const V3<T> n_ad{na4.x, na4.y, na4.z};
+      const V3<T> n_mat = dr / r;
+      d_ij = r;
+      cv.y = f_abs(dot(dr, n_ad));
+      cv.w = (T)S.codes[c][j].x;
+      const V4<T> vj = vel_of();
+      vz = V4<T>{vj.x, vj.y, vj.z, T(0)};
+      const T cos_c = T(0.866f);
+      const T cos_n = f_abs(dot(n_mat, n_ad));
+      if (cos_n < cos_c) ny = V4<T>{n_mat.x, n_mat.y, n_mat.z, T(0)};
+      else ny = V4<T>{n_ad.x, n_ad.y, n_ad.z, T(0)};
+    }
+    cv.x += f_abs((ny.x * gker.x + ny.y * gker.y + ny.z * gker.z) * P.vol_def);
+  };
+  // When this section's interaction walks the kept lists, they hold every boundary
+  // particle within 2h of i in the scan's order (per cell offset, the boundary range
+  // first, ascending index): walking their boundary entries visits the same candidates
+  // that pass the q < 2 test, in the same order, without the boundary cells' full ranges.
+  // The boundary neighbour records (written by the Adami kernel earlier in the section)
+  // carry j's position, velocity and contact flag in one 64-byte line; entries are read
+  // four at a time and their records together, so a near-wall thread waits for two
+  // loads per four entries instead of a chain of loads per entry.
+  const int kept = (S.nbg && P.keep_lists && dyn->ix_mode == 1) ? S.nbg_cnt[t] : -1;
+  if (kept >= 0) {
+    const Rec<T>* __restrict__ rec = S.rec;
+    const unsigned* __restrict__ lst = S.nbg + t;
+    const size_t stride = (size_t)S.nbg_stride;
+    constexpr unsigned kNone = 0x7ffffffu;  // index of no particle (np < 2^27)
+    for (int e0 = 0; e0 < kept; e0 += 4) {
+      unsigned ent[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) ent[k] = e0 + k < kept ? __ldcs(lst + (size_t)(e0 + k) * stride) : kNone;
+      NbVals<T> nb[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if ((int)(ent[k] & kNone) < P.npb) nb[k] = load_nb(rec, (int)(ent[k] & kNone));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int j = (int)(ent[k] & kNone);
+        if (j >= P.npb) continue;
+        const NbVals<T>& b = nb[k];
+        visit(j, off_of((int)(ent[k] >> 27)), V3<T>{b.p.x, b.p.y, b.p.z}, [&] { return b.a.y < T(0); },
+              [&] { return b.vr; });
+      }
+    }
+  } else {
     for (int oc = 0; oc < 27; ++oc) {
       const I3 off = off_of(oc);
       const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
       if (!in_grid(P, cj)) continue;
       const int2 rg = S.range[key_of(P, cj)];
-      const V3<T> o = mulI(off, th);
-      for (int j = rg.x; j < rg.y; ++j) {
-        V3<T> dr = pos_i - ld3(pos, j) - o;
-        const T r2 = pair_r2(dr.x, dr.y, dr.z);
-        if (!(r2 < P.r2_prefilter)) continue;
-        T r = pair_r(r2);
-        T q = r * P.i_h;
-        if ((double)q < 2.0) {
-          const int codej = S.codes[c][j].x;
-          if (codej >= 10) {
-            T dwdr = kernel_f(P.kgrad, q);
-            V3<T> gker = dr * dwdr;
-            if (r < d_ij && r > T(0)) {
-              const V4<T> na4 = S.cny[j];
-              const V3<T> n_ad{na4.x, na4.y, na4.z};
-              const V3<T> n_mat = dr / r;
-              d_ij = r;
-              cv.y = f_abs(dot(dr, n_ad));
-              cv.w = (T)codej;
-              const V4<T> vj = S.vel[c][j];
-              vz = V4<T>{vj.x, vj.y, vj.z, T(0)};
-              const T cos_c = T(0.866f);
-              const T cos_n = f_abs(dot(n_mat, n_ad));
-              if (cos_n < cos_c) ny = V4<T>{n_mat.x, n_mat.y, n_mat.z, T(0)};
-              else ny = V4<T>{n_ad.x, n_ad.y, n_ad.z, T(0)};
-            }
-            cv.x += f_abs((ny.x * gker.x + ny.y * gker.y + ny.z * gker.z) * P.vol_def);
-          }
-        }
-      }
+      for (int j = rg.x; j < rg.y; ++j)
+        visit(j, off, ld3(pos, j), [&] { return S.codes[c][j].x >= 10; }, [&] { return S.vel[c][j]; });
     }
   }
   S.cv[cpar][i] = cv;
@@ -770,33 +900,6 @@ template <class T> struct IState {
   int shift;
 };
 
-// The neighbour-side values one pair term needs.
-template <class T> struct NbVals {
-  V4<T> p, vr, a, b;
-};
-template <class T> RWD NbVals<T> load_nb(const Rec<T>* __restrict__ rec, int j) {
-  NbVals<T> v;
-  v.p = rec[j].p;
-  v.vr = rec[j].vr;
-  v.a = rec[j].a;
-  v.b = rec[j].b;
-  return v;
-}
-// Float records: two 256-bit loads (sm_100) instead of four 128-bit ones.  Half the load
-// instructions and L1 requests per neighbour; the walk kernel's L1 request rate is what
-// bounds it.  Records are 64 bytes from a 256-byte aligned cudaMalloc base.
-static_assert(sizeof(Rec<float>) == 64, "float records are one 64-byte line");
-template <> RWD NbVals<float> load_nb<float>(const Rec<float>* __restrict__ rec, int j) {
-  NbVals<float> v;
-  const float* q = reinterpret_cast<const float*>(rec + j);
-  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-      : "=f"(v.p.x), "=f"(v.p.y), "=f"(v.p.z), "=f"(v.p.w), "=f"(v.vr.x), "=f"(v.vr.y), "=f"(v.vr.z), "=f"(v.vr.w)
-      : "l"(q));
-  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-      : "=f"(v.a.x), "=f"(v.a.y), "=f"(v.a.z), "=f"(v.a.w), "=f"(v.b.x), "=f"(v.b.y), "=f"(v.b.z), "=f"(v.b.w)
-      : "l"(q + 8));
-  return v;
-}
 
 // One pair (i, j) of cuParticleInteractionMaterialLoopSolution
 // (src/particle_interaction.cu:29-114), given dr = (pos_i - pos_j) - offset * 2h.
@@ -917,19 +1020,18 @@ template <bool Strict, class T> RWD void ix_begin(const Params<T>& P, const DevS
 }
 
 
-// Pair sums of particle i straight from global memory: phase 1 lists candidates in
-// shared memory (my[k * stride]), phase 2 evaluates them in order.
-// otab[oc] = cell offset oc times 2h (a shared-memory table: no per-pair decode).
-template <class T> RWD void fill_offsets(V4<T>* otab, T th) {
-  if (threadIdx.x < 27) {
-    const I3 f = off_of((int)threadIdx.x);
-    otab[threadIdx.x] = V4<T>{(T)f.x * th, (T)f.y * th, (T)f.z * th, T(0)};
-  }
+// Exact float of a small integer (|v| < 2^22) without a conversion instruction.
+template <class T> RWD T small_float(int v) {
+  if constexpr (sizeof(T) == 4) return __int_as_float(0x4B400000 + v) - 12582912.0f;
+  else return (T)v;
 }
 
+// Evaluates the listed candidates of particle i (entry k at my[k * stride]: index j |
+// cell offset << 27) in list order.  The cell offset is decoded arithmetically (no
+// table lookup, which would compete with the record gathers for the L1 data stage).
 template <bool Strict, class T, bool Kept = false>
 RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const IState<T>& I, const unsigned* my,
-                      int stride, int cnt, const V4<T>* otab, Acc<T>& A) {
+                      int stride, int cnt, Acc<T>& A) {
   const Rec<T>* __restrict__ rec = S.rec;
   if (cnt <= 0) return;
   // Kept lists (global memory) are read once per interaction: streaming loads, so they
@@ -953,8 +1055,17 @@ RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const ISt
       nb = load_nb(rec, (int)(ent1 & 0x7ffffffu));
       if (e + 2 < cnt) ent1 = entry((e + 2) * stride);
     }
-    const V4<T> o = otab[occ];
-    pair_eval<Strict>(P, I, V3<T>{I.pos.x - cur.p.x - o.x, I.pos.y - cur.p.y - o.y, I.pos.z - cur.p.z - o.z}, cur, A);
+    // cell offset digits of occ = dx + 3 dy + 9 dz (each 0..2), without a table
+    const int dz = (occ * 57) >> 9;
+    const int rr = occ - 9 * dz;
+    const int dy = (rr * 11) >> 5;
+    const int dx = rr - 3 * dy;
+    const T th = P.two_h;
+    // (pos_i - p_j) - (d - 1) 2h with one rounding after the exact product: the same
+    // value as subtracting the tabulated offset
+    pair_eval<Strict>(P, I, V3<T>{f_fma(small_float<T>(1 - dx), th, I.pos.x - cur.p.x),
+                                  f_fma(small_float<T>(1 - dy), th, I.pos.y - cur.p.y),
+                                  f_fma(small_float<T>(1 - dz), th, I.pos.z - cur.p.z)}, cur, A);
   }
 }
 
@@ -963,7 +1074,7 @@ RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const ISt
 // up is evaluated and emptied, and the scan resumes (order preserved).
 template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
                                                         const IState<T>& I, unsigned* my, int stride, int cap,
-                                                        const V4<T>* otab, Acc<T>& A, int keep_slot = -1) {
+                                                        Acc<T>& A, int keep_slot = -1) {
   const V4<T>* __restrict__ pos = S.pos[c];
   const T th = P.two_h;
   const T r2max = keep_slot >= 0 ? P.r2_list : P.r2_prefilter;
@@ -984,7 +1095,7 @@ template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, cons
         const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
         if (dx * dx + dy * dy + dz * dz < r2max) {
           if (cnt == cap) {
-            ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, otab, A);
+            ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
             cnt = 0;
             spilled = true;
           }
@@ -999,7 +1110,7 @@ template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, cons
       for (int e = 0; e < cnt; ++e) S.nbg[(size_t)e * S.nbg_stride + keep_slot] = my[e * stride];
     S.nbg_cnt[keep_slot] = spilled ? -1 : cnt;
   }
-  ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, otab, A);
+  ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
 }
 
 // Second pass of a particle within 2h of a periodic plane, over the neighbours of its
@@ -1132,8 +1243,6 @@ template <class T, bool Strict, bool Walk>
 __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
     k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, int cpar) {
   extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread (scan only)
-  __shared__ V4<T> otab[27];
-  fill_offsets(otab, P.two_h);
   __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!Walk && t == 0) const_cast<Dyn<T>*>(dyn)->rec_stale = 0;  // the corner search has refreshed the records
@@ -1167,10 +1276,12 @@ __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
   IState<T> I;
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
-  if (Walk) ix_list_eval<Strict, T, true>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, otab, A);
-  else
-    ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, otab, A,
+  if (Walk) ix_list_eval<Strict, T, true>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, A);
+  else {
+    ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A,
                            (mode == 0 && keep) ? t : -1);
+    if (mode == 0 && keep && S.nbg_cnt[t] < 0) atomicAdd(&const_cast<Dyn<T>*>(dyn)->n_spill, 1);
+  }
   if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }
@@ -1282,8 +1393,6 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
                                                                                        const Dyn<T>* dyn, int cpar) {
   extern __shared__ __align__(16) unsigned char smraw[];
   Ix2Smem<T>& sm = *reinterpret_cast<Ix2Smem<T>*>(smraw);
-  __shared__ V4<T> otab[27];
-  fill_offsets(otab, P.two_h);
   const int tid = threadIdx.x;
   if (blockIdx.x == 0 && tid == 0) const_cast<Dyn<T>*>(dyn)->rec_stale = 0;  // records refreshed by the corner search
   // Deleted slots keep their contact state (the chunk list covers live particles only).
@@ -1377,7 +1486,7 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
   if (fallback) {
     // Too big for the tile: same arithmetic from global memory, list in the round buffer.
     ix_sums_global<Strict>(P, S, c, celli, I, reinterpret_cast<unsigned*>(&sm.list[0][0]) + tid, IX2_TB,
-                           IX2_CAP / 2, otab, A);
+                           IX2_CAP / 2, A);
     if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
     ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
     return;

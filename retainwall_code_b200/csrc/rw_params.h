@@ -93,7 +93,11 @@ template <class T> struct Dyn {
   // Some particle changed cell (or the host wrote the state) since the last search:
   // keys, ranges and counts must be recomputed.  Set by the corrector, cleared at the
   // end of each search.
-  int cells_dirty, pad2_;
+  int cells_dirty;
+  int n_spill;  // kept lists of the last build that overflowed (those particles scan)
+  // Work skipped by the gates of a captured step graph (conditional nodes): searches
+  // with no cell change, scan launches with every particle on a kept list.
+  int n_search_skipped, n_scan_skipped;
   Motion<T> mv[kMotionMax];
   Table<T> tab[kMotionMax];
 };
