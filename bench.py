@@ -163,6 +163,22 @@ def barrier(ws: int):
         dist.barrier()
 
 
+def timed_steps(sim, steps: int, device: int):
+    """Times `steps` graph replays with CUDA events, sampling clocks meanwhile; returns
+    (ms, kernels launched, clock sampler).  The launch count is the graph's kernels minus
+    the gated bodies the device skipped (searches with no cell change, scan launches
+    with every particle on a kept list), read from the context's counters."""
+    i0 = sim.info()
+    with ClockSampler(device) as clk:
+        ms = sim.step_timed(steps)
+    sim.synchronize()
+    i1 = sim.info()
+    launched = (steps * i1.graph_kernels
+                - (i1.n_search_skipped - i0.n_search_skipped) * i1.search_body_kernels
+                - (i1.n_scan_skipped - i0.n_scan_skipped))
+    return ms, launched, clk
+
+
 def interaction_bytes(inf, ncell: int, scalar: int, list_entries: int = 0) -> int:
     """Algorithmic HBM bytes of one interaction launch: every live soil particle's own
     state read once (cell 16, position 4s, velocity 4s, stress 6s, mass 4s, contact
@@ -306,9 +322,7 @@ def run_ours(args, ws, rank, local):
     sim.step(args.warmup)
     sim.synchronize()
     barrier(ws)
-    with ClockSampler(local) as clk:
-        ms = sim.step_timed(args.steps)
-    sim.synchronize()
+    ms, launched, clk = timed_steps(sim, args.steps, local)
     ms = allreduce_max(ms, ws)
     barrier(ws)
     npm = sim.info().npm
@@ -390,7 +404,7 @@ def run_ours(args, ws, rank, local):
         "roofline_step": roof_step,
         "stage_ms": stages,
         "candidate_lists": lists,
-        "gpu_launches": kps * args.steps,
+        "gpu_launches": launched,
         "clocks": clocks,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -559,11 +573,11 @@ def run_closure(args, ws, rank, local):
         sim.step(args.warmup)
         sim.synchronize()
         barrier(ws)
-        with ClockSampler(local) as clk:
-            ms = sim.step_timed(args.steps)
+        ms, launched, clk = timed_steps(sim, args.steps, local)
         ms = allreduce_max(ms, ws)
         stages, kps = sim.profile(3)
-        res[mode] = {"ms": ms, "npm": sim.info().npm, "stages": stages, "kps": kps, "clocks": clk.summary(),
+        res[mode] = {"ms": ms, "npm": sim.info().npm, "stages": stages, "launched": launched,
+                     "clocks": clk.summary(),
                      "wall_force_N": float(sim.wall_force(0)[0]), "stats": sim.closure_stats(),
                      "err": sim.info().device_err}
         sim.close()
@@ -597,7 +611,7 @@ def run_closure(args, ws, rank, local):
             "training": {"samples": n_samples, "runs": runs, "collect_s": collect_s, "epochs": args.closure_epochs,
                          "train_s": train_s, "samples_per_s": n_samples * args.closure_epochs / train_s,
                          "final_mse": loss},
-            "stage_ms": res["closure"]["stages"], "gpu_launches": res["closure"]["kps"] * args.steps,
+            "stage_ms": res["closure"]["stages"], "gpu_launches": res["closure"]["launched"],
             "clocks": res["closure"]["clocks"], "device_err": res["closure"]["err"],
         }), flush=True)
 

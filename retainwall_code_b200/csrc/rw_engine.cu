@@ -92,6 +92,7 @@ template <class T> struct Engine final : EngineBase {
   size_t near_wall_words = 0;
   // Step graphs captured with conditional nodes (gated()); st_body captures their bodies.
   bool allow_cond = false;
+  bool graph_cond = false;  // the instantiated step graph has the gates
   cudaStream_t st_body = nullptr;
 
   ~Engine() override {
@@ -688,6 +689,7 @@ template <class T> struct Engine final : EngineBase {
       cudaGraph_t g = capture_step(true);
       cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
       cudaGraphDestroy(g);
+      graph_cond = e == cudaSuccess;
       if (e != cudaSuccess) {  // a driver without conditional nodes: plain step graph
         cudaGetLastError();
         g = capture_step(false);
@@ -829,6 +831,13 @@ template <class T> struct Engine final : EngineBase {
     o->dr = (double)P.dr;
     o->n_sorts = d.n_sorts;
     o->n_list_reuse = d.n_reuse;
+    o->n_search_skipped = d.n_search_skipped;
+    o->n_scan_skipped = d.n_scan_skipped;
+    // kernels of the captured step graph when every gated body runs: the plain step
+    // plus one gate per search and per scan launch
+    const bool scan_gate = ix_kernel == 0 && P.np > P.npb;
+    o->graph_kernels = kernels_per_step() + (graph_cond ? 2 + (scan_gate ? 2 : 0) : 0);
+    o->search_body_kernels = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 2 : 0);
   }
 
   // Kept candidate lists: radius 2h + skin; dropped once any particle may have moved
