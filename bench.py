@@ -29,17 +29,17 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-updates/s/GPU at 1.92M particles"
 # From the ncu capture of the interaction's walk kernel on the 0.96M-particle case
-# (profiles/k_interaction_wall2_half.md): DRAM read+write 461.4 + 64.6 MB and 331.1M warp
+# (profiles/k_interaction_wall2_half.md): DRAM read+write 461.4 + 63.4 MB and 337.2M warp
 # instructions per launch.  Both grow with the particle count, so they are scaled per
 # soil particle to the benchmarked case.
-IX_DRAM_BYTES_PER_SOIL = (461.39e6 + 64.64e6) / 960000
-IX_WARP_INSTR_PER_SOIL = 331.09e6 / 960000
+IX_DRAM_BYTES_PER_SOIL = (461.41e6 + 63.44e6) / 960000
+IX_WARP_INSTR_PER_SOIL = 337.22e6 / 960000
 # L1 data-stage wavefronts the walk kernel cannot avoid: each listed neighbour's 64-byte
 # record is two 32-byte sectors read by one lane (records of a warp's lanes are distinct),
 # each list entry an eighth of a sector (a warp's 32 entries are one coalesced 128-byte
 # load), each particle's own state and outputs about 240 B.  The L1 data stage retires one
 # wavefront per cycle per SM, and scattered sectors cost one wavefront each (ncu: 122.5M
-# sectors requested, 134M wavefronts with the shared-memory ones, 87% of peak).
+# sectors requested per launch on the 0.96M case, 84% of the stage's peak).
 IX_L1_SECTORS_PER_ENTRY = 2 + 1 / 8
 IX_L1_SECTORS_PER_SOIL = 240 / 32
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
@@ -318,6 +318,8 @@ def run_ours(args, ws, rank, local):
         sim.set_option(_abi.OPT_STRICT_FP, 1)
     if args.skin is not None:
         sim.set_option(_abi.OPT_LIST_SKIN, args.skin)
+    if args.no_gates:
+        sim.set_option(_abi.OPT_GRAPH_GATES, 0)
     inf = sim.info()
     sim.step(args.warmup)
     sim.synchronize()
@@ -628,6 +630,8 @@ def main():
     ap.add_argument("--ix-kernel", type=int, default=None, help="interaction kernel: 0 global (default), 1 chunked")
     ap.add_argument("--skin", type=float, default=None, help="kept candidate-list skin in units of h (0: scan cells)")
     ap.add_argument("--strict", action="store_true", help="separately rounded interaction arithmetic")
+    ap.add_argument("--no-gates", action="store_true",
+                    help="plain step graph without conditional nodes (for ncu, which replays single graph kernels)")
     ap.add_argument("--precision-report", action="store_true", help="precision form vs FP64 (configs 1 and 3)")
     ap.add_argument("--precision-steps", type=int, default=2000)
     ap.add_argument("--batch-cases", type=int, default=64)

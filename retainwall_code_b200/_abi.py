@@ -12,6 +12,7 @@ STATUS_NAMES = {0: "RW_OK", 1: "RW_EINVAL", 2: "RW_ENOENT", 3: "RW_EIO", 4: "RW_
 MODEL_MAX, MATERIAL_SIZE, MOTION_MAX, TABLE_MAX = 10, 15, 10, 10
 OPT_WALL_FRICTION, OPT_COMPAT_CONTACT, OPT_INTERACTION_KERNEL, OPT_STRICT_FP, OPT_MIXED_PRECISION = 0, 1, 2, 3, 4
 OPT_LIST_SKIN = 5
+OPT_GRAPH_GATES = 6
 
 # rw_array ids and their row shapes (columns, integer?)
 ARRAYS: Dict[str, int] = {

@@ -92,6 +92,7 @@ template <class T> struct Engine final : EngineBase {
   size_t near_wall_words = 0;
   // Step graphs captured with conditional nodes (gated()); st_body captures their bodies.
   bool allow_cond = false;
+  bool graph_gates = true;  // RW_OPT_GRAPH_GATES
   bool graph_cond = false;  // the instantiated step graph has the gates
   cudaStream_t st_body = nullptr;
 
@@ -686,10 +687,10 @@ template <class T> struct Engine final : EngineBase {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
       }
-      cudaGraph_t g = capture_step(true);
+      cudaGraph_t g = capture_step(graph_gates);
       cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
       cudaGraphDestroy(g);
-      graph_cond = e == cudaSuccess;
+      graph_cond = graph_gates && e == cudaSuccess;
       if (e != cudaSuccess) {  // a driver without conditional nodes: plain step graph
         cudaGetLastError();
         g = capture_step(false);
@@ -871,6 +872,8 @@ template <class T> struct Engine final : EngineBase {
       P.mixed = v != 0.0 ? 1 : 0;
     } else if (opt == RW_OPT_STRICT_FP) {
       strict_fp = v != 0.0;
+    } else if (opt == RW_OPT_GRAPH_GATES) {
+      graph_gates = v != 0.0;
     } else if (opt == RW_OPT_INTERACTION_KERNEL) {
       if (v != 0.0 && v != 1.0) return RW_EINVAL;
       const int was = ix_kernel;

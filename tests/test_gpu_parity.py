@@ -317,6 +317,33 @@ def test_kept_candidate_lists_reused_and_dropped(cases):
         np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
 
 
+def test_graph_gates_skip_idle_work_only(cases):
+    """The step graph's conditional nodes skip a search in which no particle changed
+    cell and the scan launch of an interaction that walks every kept list; the device
+    counts what it skipped.  Results equal a plain graph (every kernel launched) bit for
+    bit, in a quasi-static case (searches skipped) and in a fast one (none skipped)."""
+    from retainwall_code_b200 import _abi
+
+    fast = mini_cases()["wall_mini"]
+    fast.velrhop[fast.npb:, 0] = 40.0
+    for c, quiet in ((cases["wall_mini"], True), (fast, False)):
+        g = LoquatSph(case=c)
+        p = LoquatSph(case=c)
+        p.set_option(_abi.OPT_GRAPH_GATES, 0)
+        g.step(6)
+        p.step(6)
+        for key in ("cellpos", "pospres", "velrhop", "str", "contact_var", "accad"):
+            np.testing.assert_array_equal(g.get(key), p.get(key), err_msg=key)
+        gi, pi = g.info(), p.info()
+        assert pi.n_search_skipped == 0 and pi.n_scan_skipped == 0
+        assert pi.graph_kernels - gi.graph_kernels == -4  # two search gates, two scan gates
+        if quiet:
+            assert gi.n_search_skipped > 0 and gi.n_scan_skipped > 0
+        else:
+            assert gi.n_scan_skipped == 0
+        assert gi.device_err == 0
+
+
 def test_deletion_matches_oracle():
     """Soil thrown out through the open +x side of the grid is moved to the deleted cell
     (cuCheckOutDomain, src/predictor_corrector.cu:183-187; the count bookkeeping of
