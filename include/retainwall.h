@@ -258,6 +258,10 @@ rw_status rw_batch_create(rw_ctx* const* ctxs, int n, rw_batch** out);
 rw_status rw_batch_step(rw_batch* b, int nsteps, double* ms);
 rw_status rw_batch_synchronize(rw_batch* b);
 rw_status rw_batch_destroy(rw_batch* b);
+/* rw_wall_force of every context of the batch (same mode, wall_id and strip), after the
+ * batch's steps: out_xyz receives 3 doubles per context, in creation order, with one
+ * copy back and one wait for all of them. */
+rw_status rw_batch_wall_force(rw_batch* b, int mode, int wall_id, const double* strip, double* out_xyz);
 /* Kept candidate lists (RW_OPT_LIST_SKIN) as they stand: out[0] = entries over all soil
  * particles, out[1] = soil particles holding a list (both 0 when none is kept). */
 rw_status rw_list_stats(rw_ctx* ctx, int64_t* out);

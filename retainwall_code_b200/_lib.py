@@ -19,7 +19,7 @@ EXPORTS = [
     "rw_particle_interaction", "rw_predictor", "rw_corrector", "rw_end_step", "rw_step", "rw_synchronize",
     "rw_wall_force", "rw_save", "rw_get_info", "rw_set_option", "rw_get_array", "rw_set_array", "rw_set_counters",
     "rw_profile", "rw_step_timed", "rw_cell_sort_noalloc", "rw_batch_create", "rw_batch_step",
-    "rw_batch_synchronize", "rw_batch_destroy", "rw_autotune", "rw_wall_profile",
+    "rw_batch_synchronize", "rw_batch_destroy", "rw_batch_wall_force", "rw_autotune", "rw_wall_profile",
     "rw_mlp_last_error", "rw_mlp_create", "rw_mlp_destroy", "rw_mlp_get_params", "rw_mlp_set_params",
     "rw_mlp_forward", "rw_mlp_grad", "rw_mlp_add_samples", "rw_mlp_samples", "rw_mlp_clear_samples",
     "rw_mlp_train", "rw_mlp_feature_ranges", "rw_mlp_collect", "rw_set_closure", "rw_closure_stats",
@@ -63,6 +63,7 @@ def lib() -> ct.CDLL:
     L.rw_batch_step.argtypes = [P, ct.c_int, ct.POINTER(ct.c_double)]
     L.rw_batch_synchronize.argtypes = [P]
     L.rw_batch_destroy.argtypes = [P]
+    L.rw_batch_wall_force.argtypes = [P, ct.c_int, ct.c_int, ct.c_void_p, ct.POINTER(ct.c_double)]
     L.rw_autotune.argtypes = [P, ct.c_int, ct.POINTER(ct.c_int)]
     L.rw_wall_profile.argtypes = [P, ct.c_double, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(ct.c_double)]
     L.rw_cell_sort_noalloc.argtypes = [ct.c_void_p, ct.c_int32, ct.c_int32, ct.c_void_p, ct.c_void_p, ct.c_void_p]

@@ -57,7 +57,9 @@ struct EngineBase {
   virtual void profile(int nsteps, double* ms, int n, int* kps) = 0;
   virtual void wall_profile(double x_wall, double z_top, double dz, int nbins, double* out) = 0;
   virtual double step_timed(int n) = 0;
-  virtual cudaGraph_t step_graph() = 0;
+  virtual cudaGraph_t step_graph(bool gates) = 0;
+  // Wall resultant computed on stream s into the device array d_out (3 doubles).
+  virtual void wall_force_enqueue(cudaStream_t s, int mode, int wall_id, const double* strip, double* d_out) = 0;
   virtual cudaStream_t stream() const = 0;
   virtual int soil_count() = 0;
   virtual int set_closure(rw_mlp* net, double margin) = 0;
@@ -104,11 +106,27 @@ template <class T> struct Engine final : EngineBase {
     if (st_body) cudaStreamDestroy(st_body);
   }
 
+  // Zeroed device buffers.  create() sizes everything it allocates in a measuring pass
+  // and takes it from one arena (one cudaMalloc instead of about seventy), each buffer
+  // 256-byte aligned; later allocations get their own cudaMalloc.
+  char* arena = nullptr;
+  size_t arena_cap = 0, arena_used = 0;
+  bool measuring = false;
   template <class X> X* dalloc(size_t n) {
+    const size_t bytes = (std::max<size_t>(n, 1) * sizeof(X) + 255) & ~(size_t)255;
+    if (measuring) {
+      arena_used += bytes;
+      return nullptr;
+    }
+    if (arena && arena_used + bytes <= arena_cap) {
+      X* p = reinterpret_cast<X*>(arena + arena_used);
+      arena_used += bytes;
+      return p;
+    }
     void* p = nullptr;
-    RW_CU(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(X)));
+    RW_CU(cudaMalloc(&p, bytes));
     allocs.push_back(p);
-    RW_CU(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(X), st));
+    RW_CU(cudaMemsetAsync(p, 0, bytes, st));
     return (X*)p;
   }
   template <class X> void up(X* d, const std::vector<X>& h) {
@@ -268,85 +286,97 @@ template <class T> struct Engine final : EngineBase {
     P.dt = P.cfl * (P.h / P.cs_m);  // StepCalculation (src/loquat.cu:368-369)
 
     const size_t np = P.np, npb = P.npb;
-    for (int b = 0; b < 2; ++b) {
-      S.codes[b] = dalloc<int4>(np);
-      S.cellpos[b] = dalloc<int4>(np);
-      S.pos[b] = dalloc<V4<T>>(np);
-      S.pos_ori[b] = dalloc<V4<T>>(np);
-      S.vel[b] = dalloc<V4<T>>(np);
-      S.idm[b] = dalloc<V4<T>>(np);
-      S.str_a[b] = dalloc<V4<T>>(np);
-      S.str_b[b] = dalloc<V2<T>>(np);
-      S.stn_a[b] = dalloc<V4<T>>(np);
-      S.stn_b[b] = dalloc<V2<T>>(np);
-      S.normal[b] = dalloc<V4<T>>(npb);
-      S.pos_ini[b] = dalloc<V4<T>>(np);
-      S.vel_ini[b] = dalloc<V4<T>>(np);
-      S.stri_a[b] = dalloc<V4<T>>(np);
-      S.stri_b[b] = dalloc<V2<T>>(np);
-      S.stni_a[b] = dalloc<V4<T>>(np);
-      S.stni_b[b] = dalloc<V2<T>>(np);
-      S.cv[b] = dalloc<V4<T>>(np);
-      S.cf[b] = dalloc<V4<T>>(np);
-      S.cmp_p[b] = dalloc<V4<T>>(np);
-      S.cmp_v[b] = dalloc<V4<T>>(np);
-      S.cmp_pi[b] = dalloc<V4<T>>(np);
-      S.cmp_vi[b] = dalloc<V4<T>>(np);
-    }
-    S.accad = dalloc<V4<T>>(np);
-    S.spin = dalloc<V4<T>>(np);
-    S.ace_a = dalloc<V4<T>>(np);
-    S.ace_b = dalloc<V2<T>>(np);
-    S.cny = dalloc<V4<T>>(np);
-    S.cvz = dalloc<V4<T>>(np);
-    S.rec = dalloc<Rec<T>>(np);
-    S.tc_a = dalloc<V4<T>>(np);
-    S.tc_b = dalloc<V2<T>>(np);
-    S.keys = dalloc<int>(np);
-    S.vals = dalloc<int>(np);
-    S.tk = dalloc<int>(np);
-    S.tv = dalloc<int>(np);
-    S.range = dalloc<int2>(P.ncell);
-    S.ntiles = (int)nblk((long)np, RS_TILE);
-    S.hist = dalloc<int>(256 * (size_t)S.ntiles);
-    S.dtot = dalloc<int>(256);
-    int bits = 1;
-    while ((1L << bits) <= P.ncell_delete_m) ++bits;
-    S.sort_passes = (bits + 7) / 8;
-    S.skeys = (S.sort_passes & 1) ? S.tk : S.keys;
-    S.sperm = (S.sort_passes & 1) ? S.tv : S.vals;
-    S.wsum = dalloc<double>(3 * (WF_BLOCKS + 1));
-    ncol = P.cell_num[0] * P.cell_num[1];
-    max_chunks = P.npm0 / IX2_TB + ncol + 1;
-    S.col_beg = dalloc<int>(ncol);
-    S.col_len = dalloc<int>(ncol);
-    S.col_cnt = dalloc<int>(ncol);
-    S.col_off = dalloc<int>(ncol);
-    near_wall_words = ((size_t)P.ncell_material + 3) / 4;
-    S.near_wall = reinterpret_cast<unsigned char*>(dalloc<unsigned>(near_wall_words));
-    S.chunks = dalloc<Chunk>(max_chunks);
-    S.nbg_stride = (int)(np - npb);
-    if ((size_t)IX_CAP * (np - npb) < ((size_t)1 << 31)) {  // list indices stay 32-bit
-      S.nbg = dalloc<unsigned>((size_t)IX_CAP * (np - npb));
-      S.nbg_cnt = dalloc<int>(np - npb);
-    }
-    S.dacc = dalloc<float>(np);
-    if (npb > 0 && (size_t)IX_CAP * npb < ((size_t)1 << 31)) {  // boundary lists (Adami)
-      S.nbb = dalloc<unsigned>((size_t)IX_CAP * npb);
-      S.nbb_cnt = dalloc<int>(npb);
-    }
+    HypoC<T>* tab = nullptr;
+    auto allocate = [&] {
+      for (int b = 0; b < 2; ++b) {
+        S.codes[b] = dalloc<int4>(np);
+        S.cellpos[b] = dalloc<int4>(np);
+        S.pos[b] = dalloc<V4<T>>(np);
+        S.pos_ori[b] = dalloc<V4<T>>(np);
+        S.vel[b] = dalloc<V4<T>>(np);
+        S.idm[b] = dalloc<V4<T>>(np);
+        S.str_a[b] = dalloc<V4<T>>(np);
+        S.str_b[b] = dalloc<V2<T>>(np);
+        S.stn_a[b] = dalloc<V4<T>>(np);
+        S.stn_b[b] = dalloc<V2<T>>(np);
+        S.normal[b] = dalloc<V4<T>>(npb);
+        S.pos_ini[b] = dalloc<V4<T>>(np);
+        S.vel_ini[b] = dalloc<V4<T>>(np);
+        S.stri_a[b] = dalloc<V4<T>>(np);
+        S.stri_b[b] = dalloc<V2<T>>(np);
+        S.stni_a[b] = dalloc<V4<T>>(np);
+        S.stni_b[b] = dalloc<V2<T>>(np);
+        S.cv[b] = dalloc<V4<T>>(np);
+        S.cf[b] = dalloc<V4<T>>(np);
+        S.cmp_p[b] = dalloc<V4<T>>(np);
+        S.cmp_v[b] = dalloc<V4<T>>(np);
+        S.cmp_pi[b] = dalloc<V4<T>>(np);
+        S.cmp_vi[b] = dalloc<V4<T>>(np);
+      }
+      S.accad = dalloc<V4<T>>(np);
+      S.spin = dalloc<V4<T>>(np);
+      S.ace_a = dalloc<V4<T>>(np);
+      S.ace_b = dalloc<V2<T>>(np);
+      S.cny = dalloc<V4<T>>(np);
+      S.cvz = dalloc<V4<T>>(np);
+      S.rec = dalloc<Rec<T>>(np);
+      S.tc_a = dalloc<V4<T>>(np);
+      S.tc_b = dalloc<V2<T>>(np);
+      S.keys = dalloc<int>(np);
+      S.vals = dalloc<int>(np);
+      S.tk = dalloc<int>(np);
+      S.tv = dalloc<int>(np);
+      S.range = dalloc<int2>(P.ncell);
+      S.ntiles = (int)nblk((long)np, RS_TILE);
+      S.hist = dalloc<int>(256 * (size_t)S.ntiles);
+      S.dtot = dalloc<int>(256);
+      int bits = 1;
+      while ((1L << bits) <= P.ncell_delete_m) ++bits;
+      S.sort_passes = (bits + 7) / 8;
+      S.skeys = (S.sort_passes & 1) ? S.tk : S.keys;
+      S.sperm = (S.sort_passes & 1) ? S.tv : S.vals;
+      S.wsum = dalloc<double>(3 * (WF_BLOCKS + 1));
+      ncol = P.cell_num[0] * P.cell_num[1];
+      max_chunks = P.npm0 / IX2_TB + ncol + 1;
+      S.col_beg = dalloc<int>(ncol);
+      S.col_len = dalloc<int>(ncol);
+      S.col_cnt = dalloc<int>(ncol);
+      S.col_off = dalloc<int>(ncol);
+      near_wall_words = ((size_t)P.ncell_material + 3) / 4;
+      S.near_wall = reinterpret_cast<unsigned char*>(dalloc<unsigned>(near_wall_words));
+      S.chunks = dalloc<Chunk>(max_chunks);
+      S.nbg_stride = (int)(np - npb);
+      if ((size_t)IX_CAP * (np - npb) < ((size_t)1 << 31)) {  // list indices stay 32-bit
+        S.nbg = dalloc<unsigned>((size_t)IX_CAP * (np - npb));
+        S.nbg_cnt = dalloc<int>(np - npb);
+      }
+      S.dacc = dalloc<float>(np);
+      if (npb > 0 && (size_t)IX_CAP * npb < ((size_t)1 << 31)) {  // boundary lists (Adami)
+        S.nbb = dalloc<unsigned>((size_t)IX_CAP * npb);
+        S.nbb_cnt = dalloc<int>(npb);
+      }
+      tab = dalloc<HypoC<T>>(kModelMax);
+      d_clstats = dalloc<double>(4);
+      d_count = dalloc<unsigned long long>(1);
+      d_dyn = dalloc<Dyn<T>>(1);
+    };
+    measuring = true;
+    arena_used = 0;
+    allocate();
+    measuring = false;
+    arena_cap = arena_used;
+    arena_used = 0;
+    RW_CU(cudaMalloc(reinterpret_cast<void**>(&arena), arena_cap));
+    allocs.push_back(arena);
+    RW_CU(cudaMemsetAsync(arena, 0, arena_cap, st));
+    allocate();
     {  // hypoplastic material constants, evaluated on the device as the kernels would
-      HypoC<T>* tab = dalloc<HypoC<T>>(kModelMax);
       k_hypo_table<T><<<1, 32, 0, st>>>(P, tab);
       RW_CU(cudaGetLastError());
       RW_CU(cudaMemcpyAsync(P.hypo, tab, sizeof(P.hypo), cudaMemcpyDeviceToHost, st));
       RW_CU(cudaStreamSynchronize(st));
     }
-    d_clstats = dalloc<double>(4);
-    d_count = dalloc<unsigned long long>(1);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    RW_CU(cudaMemsetAsync(S.dacc, 0, np * sizeof(float), st));
-    d_dyn = dalloc<Dyn<T>>(1);
 
     // The case arrays are uploaded as the caller holds them and converted on the device
     // (k_ingest).  The staging area is the candidate-list buffer, unused until the first
@@ -775,7 +805,7 @@ template <class T> struct Engine final : EngineBase {
     return (double)ms;
   }
 
-  cudaGraph_t step_graph() override { return capture_step(); }
+  cudaGraph_t step_graph(bool gates) override { return capture_step(gates && graph_gates); }
 
   // Defaults of the reference's profile (src/utilities.cu:284-292,336): wall face at
   // 0.04 + bound_thickness - 0.005 t, top at 0.04 + 1.0 + bound_thickness, bins of dr,
@@ -1091,6 +1121,15 @@ template <class T> struct Engine final : EngineBase {
   }
 
   void wall_force(int mode, int wall_id, const double* strip, double* out) override {
+    wall_force_kernels(st, mode, wall_id, strip);
+    RW_CU(cudaMemcpyAsync(out, S.wsum + 3 * WF_BLOCKS, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaStreamSynchronize(st));
+  }
+  void wall_force_enqueue(cudaStream_t s, int mode, int wall_id, const double* strip, double* d_out) override {
+    wall_force_kernels(s, mode, wall_id, strip);
+    RW_CU(cudaMemcpyAsync(d_out, S.wsum + 3 * WF_BLOCKS, 3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  }
+  void wall_force_kernels(cudaStream_t s, int mode, int wall_id, const double* strip) {
     double xmax, zmin, zmax;
     if (strip) {
       xmax = strip[0];
@@ -1101,11 +1140,9 @@ template <class T> struct Engine final : EngineBase {
       zmin = (double)(P.bound_thickness + T(0.04f));
       zmax = (double)(P.bound_thickness + T(0.04f) + T(1.0f));
     }
-    k_wall_force<T><<<WF_BLOCKS, WF_THREADS, 0, st>>>(P, S, d_dyn, cpar, mode, wall_id, xmax, zmin, zmax);
-    k_wall_force_final<<<1, 32, 0, st>>>(S.wsum, WF_BLOCKS);
+    k_wall_force<T><<<WF_BLOCKS, WF_THREADS, 0, s>>>(P, S, d_dyn, cpar, mode, wall_id, xmax, zmin, zmax);
+    k_wall_force_final<<<1, 32, 0, s>>>(S.wsum, WF_BLOCKS);
     check_launch();
-    RW_CU(cudaMemcpyAsync(out, S.wsum + 3 * WF_BLOCKS, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    RW_CU(cudaStreamSynchronize(st));
   }
 
   // Saving (src/loquat.cu:439-482): output_N.xml + particles with the Shepard-smoothed
@@ -1195,6 +1232,9 @@ struct Batch {
   int device = 0;
   cudaStream_t st = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  bool gated = false;      // the children carry their search / scan gates
+  double* d_wf = nullptr;  // wall resultants of every context (3 each), device and pinned host
+  double* h_wf = nullptr;
   std::string err;
   ~Batch() {
     if (gexec) cudaGraphExecDestroy(gexec);
@@ -1202,26 +1242,52 @@ struct Batch {
       cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
     }
+    if (d_wf) cudaFree(d_wf);
+    if (h_wf) cudaFreeHost(h_wf);
   }
   // Parent graph with every context's step as an independent child graph: the branches
-  // have no dependencies on each other, so the executor runs them concurrently.
+  // have no dependencies on each other, so the executor runs them concurrently.  The
+  // children keep their conditional gates where the driver accepts them in child
+  // graphs; otherwise they are plain step graphs.
   void build() {
-    cudaGraph_t parent = nullptr;
-    RW_CU(cudaGraphCreate(&parent, 0));
-    try {
-      for (EngineBase* e : engines) {
-        cudaGraph_t child = e->step_graph();
-        cudaGraphNode_t node;
-        cudaError_t rc = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
-        cudaGraphDestroy(child);
-        RW_CU(rc);
+    for (int attempt = 0; attempt < 2 && !gexec; ++attempt) {
+      const bool gates = attempt == 0;
+      cudaGraph_t parent = nullptr;
+      RW_CU(cudaGraphCreate(&parent, 0));
+      cudaError_t rc = cudaSuccess;
+      try {
+        for (EngineBase* e : engines) {
+          cudaGraph_t child = e->step_graph(gates);
+          cudaGraphNode_t node;
+          rc = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, child);
+          cudaGraphDestroy(child);
+          if (rc != cudaSuccess) break;
+        }
+        if (rc == cudaSuccess) rc = cudaGraphInstantiate(&gexec, parent, 0);
+      } catch (...) {
+        cudaGraphDestroy(parent);
+        throw;
       }
-      RW_CU(cudaGraphInstantiate(&gexec, parent, 0));
-    } catch (...) {
       cudaGraphDestroy(parent);
-      throw;
+      if (rc != cudaSuccess) {
+        gexec = nullptr;
+        cudaGetLastError();
+        if (!gates) RW_CU(rc);
+      }
+      gated = gates && gexec;
     }
-    cudaGraphDestroy(parent);
+  }
+  // Every context's wall resultant with one copy back and one wait.
+  void wall_force(int mode, int wall_id, const double* strip, double* out) {
+    const size_t n = engines.size();
+    if (!d_wf) {
+      RW_CU(cudaMalloc(reinterpret_cast<void**>(&d_wf), 3 * n * sizeof(double)));
+      RW_CU(cudaMallocHost(reinterpret_cast<void**>(&h_wf), 3 * n * sizeof(double)));
+    }
+    for (size_t k = 0; k < n; ++k) engines[k]->wall_force_enqueue(st, mode, wall_id, strip, d_wf + 3 * k);
+    RW_CU(cudaMemcpyAsync(h_wf, d_wf, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RW_CU(cudaStreamSynchronize(st));
+    std::memcpy(out, h_wf, 3 * n * sizeof(double));
   }
 };
 
@@ -1421,6 +1487,18 @@ rw_status rw_batch_create(rw_ctx* const* ctxs, int n, rw_batch** out) {
     return RW_EINVAL;
   }
   *out = bt.release();
+  return RW_OK;
+}
+
+rw_status rw_batch_wall_force(rw_batch* b, int mode, int wall_id, const double* strip, double* out_xyz) {
+  if (!b || !out_xyz || (mode != 0 && mode != 1)) return RW_EINVAL;
+  try {
+    RW_CU(cudaSetDevice(b->b.device));
+    b->b.wall_force(mode, wall_id, strip, out_xyz);
+  } catch (const Fail& f) {
+    b->b.err = f.what();
+    return f.code;
+  }
   return RW_OK;
 }
 

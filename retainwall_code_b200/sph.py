@@ -251,6 +251,16 @@ class Batch:
     def synchronize(self) -> None:
         check(lib().rw_batch_synchronize(self._h), "rw_batch_synchronize", None)
 
+    def wall_force(self, mode: int = 0, wall_id: int = 10, strip: Optional[Sequence[float]] = None) -> np.ndarray:
+        """LoquatSph.wall_force of every case (rows in the batch's order), one copy back."""
+        out = (ct.c_double * (3 * len(self.sims)))()
+        sp = None
+        if strip is not None:
+            sa = (ct.c_double * 3)(*strip)
+            sp = ct.cast(sa, ct.c_void_p)
+        check(lib().rw_batch_wall_force(self._h, mode, wall_id, sp, out), "rw_batch_wall_force", None)
+        return np.array(out[:]).reshape(len(self.sims), 3)
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib().rw_batch_destroy(self._h)

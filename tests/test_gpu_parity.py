@@ -244,12 +244,15 @@ def test_batch_equals_individual_runs():
     b = Batch(together)
     b.step(6)
     b.synchronize()
-    for c, t in zip(cs, together):
+    forces = b.wall_force(0)
+    assert forces.shape == (3, 3)
+    for k, (c, t) in enumerate(zip(cs, together)):
         alone = LoquatSph(case=c)
         alone.step(6)
         for key in ("cellpos", "pospres", "velrhop", "str", "contact_mag"):
             np.testing.assert_array_equal(t.get(key), alone.get(key), err_msg=key)
         assert t.info().step == 6
+        np.testing.assert_array_equal(forces[k], alone.wall_force(0))
     b.close()
 
 
