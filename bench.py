@@ -264,6 +264,10 @@ def run_batch(args, ws, rank, local):
     ms = allreduce_max(ms, ws)
     total_npm = sum(s["nx"] * s["ny"] * s["nz"] for s in specs)
     value = total_npm * args.steps / (ms * 1e-3)
+    infos = [sim.info() for sim in sims]
+    lists = {"sections_that_sorted": sum(i.n_sorts for i in infos),
+             "interactions_on_kept_lists": sum(i.n_list_reuse for i in infos),
+             "interactions": sum(2 * i.step for i in infos)}
     for sim in sims:
         if sim.info().device_err:
             raise SystemExit("device error word set")
@@ -295,6 +299,7 @@ def run_batch(args, ws, rank, local):
                 "h2d_bytes_per_step": int(sum(c.np_ * 144 + c.npb * 16 for c in host_cases) / args.steps),
                 "d2h_bytes_per_step": 24 * len(mine),
                 "note": "upload of every case + batched steps + per-case wall-force reads (rank 0)"},
+        "candidate_lists_rank0": lists,
         "clocks": clk.summary(),
     }
     if rank == 0:

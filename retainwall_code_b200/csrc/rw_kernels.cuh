@@ -1589,11 +1589,12 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
 // Predictor (src/predictor_corrector.cu:52-103): saves the step-start state into the
 // *_ini buffers (the reference's four D2D copies) and advances material half a step.
 // ---------------------------------------------------------------------------------
-// Both integrators are held to three 256-thread blocks per SM (80 registers, a few
-// spilled bytes): they stream about 300 B per particle, and at the two blocks their
-// natural 94 registers allow they wait on memory (measured 19% faster at three).
+// Both integrators are held to four 256-thread blocks per SM (64 registers, about
+// 100 spilled bytes): they stream about 300 B per particle, and at the two blocks
+// their natural 94 registers allow they wait on memory (measured 19% faster at
+// three blocks, another 5% at four).
 template <class T>
-__global__ void __launch_bounds__(256, 3) k_predictor(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+__global__ void __launch_bounds__(256, 4) k_predictor(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.np) return;
   const int c = dyn->cur_main, ci = dyn->cur_ini;
@@ -1681,7 +1682,7 @@ template <class T> RWD void list_account(const Params<T>& P, const DevState<T>& 
 }
 
 template <class T>
-__global__ void __launch_bounds__(256, 3) k_corrector(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+__global__ void __launch_bounds__(256, 4) k_corrector(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int npm = dyn->npm;
   if (i >= P.npb + npm) return;
