@@ -167,7 +167,8 @@ def timed_steps(sim, steps: int, device: int):
     """Times `steps` graph replays with CUDA events, sampling clocks meanwhile; returns
     (ms, kernels launched, clock sampler).  The launch count is the graph's kernels minus
     the gated bodies the device skipped (searches with no cell change, scan launches
-    with every particle on a kept list), read from the context's counters."""
+    with every particle on a list, list builds while the kept lists stand), read from
+    the context's counters."""
     i0 = sim.info()
     with ClockSampler(device) as clk:
         ms = sim.step_timed(steps)
@@ -175,7 +176,8 @@ def timed_steps(sim, steps: int, device: int):
     i1 = sim.info()
     launched = (steps * i1.graph_kernels
                 - (i1.n_search_skipped - i0.n_search_skipped) * i1.search_body_kernels
-                - (i1.n_scan_skipped - i0.n_scan_skipped))
+                - (i1.n_scan_skipped - i0.n_scan_skipped)
+                - (i1.n_build_skipped - i0.n_build_skipped))
     return ms, launched, clk
 
 

@@ -127,6 +127,8 @@ typedef struct rw_info {
   int32_t n_search_skipped; /* captured-step searches skipped whole (no particle changed cell)  */
   int32_t n_scan_skipped;   /* captured-step interactions whose scan launch was skipped (every
                                particle walked a kept list)                                      */
+  int32_t n_build_skipped;     /* captured-step interactions whose list build was skipped (the
+                                  kept lists stood)                                              */
   int32_t graph_kernels;       /* kernels of one captured step when no gated body is skipped     */
   int32_t search_body_kernels; /* kernels a skipped search does not launch                       */
 } rw_info;

@@ -88,7 +88,7 @@ class Info(ct.Structure):
         ("cell_num", ct.c_int32 * 3), ("n_motion", ct.c_int32),
         ("time", ct.c_double), ("dt", ct.c_double), ("h", ct.c_double), ("dr", ct.c_double),
         ("n_sorts", ct.c_int32), ("n_list_reuse", ct.c_int32),
-        ("n_search_skipped", ct.c_int32), ("n_scan_skipped", ct.c_int32),
+        ("n_search_skipped", ct.c_int32), ("n_scan_skipped", ct.c_int32), ("n_build_skipped", ct.c_int32),
         ("graph_kernels", ct.c_int32), ("search_body_kernels", ct.c_int32),
     ]
 

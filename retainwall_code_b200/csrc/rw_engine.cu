@@ -550,7 +550,10 @@ template <class T> struct Engine final : EngineBase {
         else k_interaction2<T, false><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
       } else {
         const unsigned g = nblk(n, IX_THREADS);
-        // the scan launch, skipped in a captured step when every particle walks a kept list
+        // the list build (only when the lists are to be rebuilt), the scan launch (only
+        // for particles without a list, and deleted slots), then the walk
+        gated([&](cudaGraphConditionalHandle h) { k_build_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
+              [&] { k_build_lists<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn); });
         gated([&](cudaGraphConditionalHandle h) { k_scan_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
               [&] {
                 if (strict_fp) k_interaction<T, true, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
@@ -737,7 +740,7 @@ template <class T> struct Engine final : EngineBase {
     // keys, check, sort, ranges, count, permute, flip, contact-wall cells, chunks
     // keys, check, sort, clear + ranges, count, permute, [clear + near-wall marks], flip, [chunks]
     const int search = 2 + 3 * S.sort_passes + 5 + (P.npb > 0 ? 2 : 0) + (ncol > 0 && ix_kernel == 1 ? 3 : 0);
-    const int ix = ix_kernel == 1 ? 1 : 2;             // chunked, or scan + walk
+    const int ix = ix_kernel == 1 ? 1 : 3;             // chunked, or list build + scan + walk
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
     if (P.stress_shepard_filter != 0) k += 2;
@@ -864,10 +867,11 @@ template <class T> struct Engine final : EngineBase {
     o->n_list_reuse = d.n_reuse;
     o->n_search_skipped = d.n_search_skipped;
     o->n_scan_skipped = d.n_scan_skipped;
+    o->n_build_skipped = d.n_build_skipped;
     // kernels of the captured step graph when every gated body runs: the plain step
-    // plus one gate per search and per scan launch
-    const bool scan_gate = ix_kernel == 0 && P.np > P.npb;
-    o->graph_kernels = kernels_per_step() + (graph_cond ? 2 + (scan_gate ? 2 : 0) : 0);
+    // plus one gate per search and two per interaction (list build, scan launch)
+    const bool ix_gates = ix_kernel == 0 && P.np > P.npb;
+    o->graph_kernels = kernels_per_step() + (graph_cond ? 2 + (ix_gates ? 4 : 0) : 0);
     o->search_body_kernels = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 2 : 0);
   }
 

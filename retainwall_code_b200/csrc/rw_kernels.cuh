@@ -533,12 +533,18 @@ template <class T> __global__ void k_search_gate(Dyn<T>* dyn, cudaGraphCondition
   }
   cudaGraphSetConditional(h, d ? 1u : 0u);
 }
-// Interaction scan launch: needed when the lists are being rebuilt, when some list of
-// the last build overflowed, or for deleted slots (their contact state is carried).
+// List build: needed when the lists are to be rebuilt (mode 0 with lists on).
+template <class T>
+__global__ void k_build_gate(const Params<T> P, DevState<T> S, Dyn<T>* dyn, cudaGraphConditionalHandle h) {
+  const bool run = S.nbg && P.keep_lists && dyn->ix_mode == 0;
+  if (!run) dyn->n_build_skipped += 1;
+  cudaGraphSetConditional(h, run ? 1u : 0u);
+}
+// Interaction scan launch: needed with lists off, when some list of the last build
+// overflowed, or for deleted slots (their contact state is carried).
 template <class T>
 __global__ void k_scan_gate(const Params<T> P, DevState<T> S, Dyn<T>* dyn, cudaGraphConditionalHandle h) {
-  const int mode = (S.nbg && P.keep_lists) ? dyn->ix_mode : 0;
-  const bool run = mode != 1 || dyn->n_spill > 0 || dyn->npm < P.np - P.npb;
+  const bool run = !(S.nbg && P.keep_lists) || dyn->n_spill > 0 || dyn->npm < P.np - P.npb;
   if (!run) {
     dyn->rec_stale = 0;  // what the scan launch does first
     dyn->n_scan_skipped += 1;
@@ -1112,12 +1118,11 @@ RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const ISt
 // up is evaluated and emptied, and the scan resumes (order preserved).
 template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, const DevState<T>& S, int c, const I3 celli,
                                                         const IState<T>& I, unsigned* my, int stride, int cap,
-                                                        Acc<T>& A, int keep_slot = -1) {
+                                                        Acc<T>& A) {
   const V4<T>* __restrict__ pos = S.pos[c];
   const T th = P.two_h;
-  const T r2max = keep_slot >= 0 ? P.r2_list : P.r2_prefilter;
+  const T r2max = P.r2_prefilter;
   int cnt = 0;
-  bool spilled = false;
   for (int oc = 0; oc < 27; ++oc) {
     const I3 off = off_of(oc);
     const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
@@ -1135,18 +1140,12 @@ template <bool Strict, class T> RWD void ix_sums_global(const Params<T>& P, cons
           if (cnt == cap) {
             ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
             cnt = 0;
-            spilled = true;
           }
           my[cnt * stride] = (unsigned)j | ((unsigned)oc << 27);
           ++cnt;
         }
       }
     }
-  }
-  if (keep_slot >= 0) {  // keep the list for the corrector section (unless it spilled)
-    if (!spilled)
-      for (int e = 0; e < cnt; ++e) S.nbg[(size_t)e * S.nbg_stride + keep_slot] = my[e * stride];
-    S.nbg_cnt[keep_slot] = spilled ? -1 : cnt;
   }
   ix_list_eval<Strict>(P, S, c, I, my, stride, cnt, A);
 }
@@ -1268,12 +1267,67 @@ template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const Dev
   S.spin[i] = v4(skewpart(A.gv), T(0.f));
 }
 
+// Candidate lists of every live soil particle (mode 0 with lists on): the 27 cells in
+// the scan's order (cz, cy, cx; boundary range before material range; ascending j),
+// every candidate within the list radius, written column-major to HBM.  A list longer
+// than IX_CAP is marked -1 and counted (n_spill): the scan launch then takes that
+// particle.  Also starts the lists' displacement bounds.  Light (no pair arithmetic,
+// no shared-memory list), so it runs at full occupancy; the walk kernel then evaluates
+// the new lists as it does kept ones, with the same pairs in the same order as a scan.
+template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!S.nbg || !P.keep_lists || dyn->ix_mode != 0) return;
+  if (t == 0) {
+    dyn->list_ok = 1;
+    dyn->list_kill = dyn->build_kill;
+  }
+  if (t >= dyn->npm) return;
+  const int i = P.npb + t;
+  S.dacc[i] = 0.0f;
+  const int c = dyn->cur_main;
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  const V3<T> pos_i = ld3(pos, i);
+  const T th = P.two_h;
+  unsigned* __restrict__ out = S.nbg + t;
+  const size_t stride = (size_t)S.nbg_stride;
+  int cnt = 0;
+  for (int oc = 0; oc < 27; ++oc) {
+    const I3 off = off_of(oc);
+    const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+    if (!in_grid(P, cj)) continue;
+    const int k = key_of(P, cj);
+    const V3<T> pmo = pos_i - mulI(off, th);  // conservative pre-test only
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      const int2 rg = S.range[pass ? k + P.ncell_material : k];
+#pragma unroll 4
+      for (int j = rg.x; j < rg.y; ++j) {
+        const V4<T> pj = pos[j];
+        const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
+        if (dx * dx + dy * dy + dz * dz < P.r2_list) {
+          if (cnt < IX_CAP) __stcs(out + (size_t)cnt * stride, (unsigned)j | ((unsigned)oc << 27));
+          ++cnt;
+        }
+      }
+    }
+  }
+  if (cnt > IX_CAP) {
+    S.nbg_cnt[t] = -1;
+    atomicAdd(&dyn->n_spill, 1);
+  } else {
+    S.nbg_cnt[t] = cnt;
+  }
+}
+
 // Interaction, one thread per soil particle, neighbours read from global memory, as
 // two launches that split the particles between them:
-//  - scan (Walk = false): scans the 27 cells (keeping the candidate lists when the
-//    step's mode is 0), and handles deleted slots and particles without a kept list;
-//  - walk (Walk = true): in mode 1, walks the kept lists of the other particles.  It
-//    carries no scan state, so it runs with fewer registers.
+//  - walk (Walk = true): walks the candidate lists, kept from an earlier section or
+//    just built by k_build_lists.  It carries no scan state, so it runs with fewer
+//    registers;
+//  - scan (Walk = false): scans the 27 cells for the particles without a list (lists
+//    off, or a list that overflowed) and carries the contact state of deleted slots.
 #ifndef RW_WALK_MIN_BLOCKS
 #define RW_WALK_MIN_BLOCKS 0  // resident blocks per SM the walk kernel's register budget aims at (0: none)
 #endif
@@ -1281,7 +1335,6 @@ template <class T, bool Strict, bool Walk>
 __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
     k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, int cpar) {
   extern __shared__ unsigned nbl[];  // IX_CAP x blockDim, column per thread (scan only)
-  __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!Walk && t == 0) const_cast<Dyn<T>*>(dyn)->rec_stale = 0;  // the corner search has refreshed the records
   const int total = P.np - P.npb;
@@ -1289,25 +1342,16 @@ __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
   const int i = P.npb + t;
   const int npm = dyn->npm;
   const bool keep = S.nbg && P.keep_lists;
-  const int mode = keep ? dyn->ix_mode : 0;
   if (Walk) {
-    if (mode != 1 || t >= npm) return;
+    if (!keep || t >= npm) return;
   } else if (t >= npm) {  // deleted slots keep their contact state
     S.cv[cpar ^ 1][i] = S.cv[cpar][i];
     S.cf[cpar ^ 1][i] = S.cf[cpar][i];
     return;
   }
-  const int kept = mode == 1 ? S.nbg_cnt[t] : -1;
+  const int kept = keep ? S.nbg_cnt[t] : -1;
   if (Walk != (kept >= 0)) return;  // the other launch takes this particle
   const int c = dyn->cur_main;
-  if (!Walk) {
-    if (mode == 0 && t == 0 && keep) {
-      Dyn<T>* d = const_cast<Dyn<T>*>(dyn);
-      d->list_ok = 1;
-      d->list_kill = d->build_kill;
-    }
-    if (mode == 0) S.dacc[i] = 0.0f;
-  }
   const int4 cp = S.cellpos[c][i];
   const I3 celli{cp.x, cp.y, cp.z};
   const V4<T> cv = S.cv[cpar][i];
@@ -1315,11 +1359,7 @@ __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
   if (Walk) ix_list_eval<Strict, T, true>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, A);
-  else {
-    ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A,
-                           (mode == 0 && keep) ? t : -1);
-    if (mode == 0 && keep && S.nbg_cnt[t] < 0) atomicAdd(&const_cast<Dyn<T>*>(dyn)->n_spill, 1);
-  }
+  else ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A);
   if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
 }

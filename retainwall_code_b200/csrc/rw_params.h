@@ -96,8 +96,9 @@ template <class T> struct Dyn {
   int cells_dirty;
   int n_spill;  // kept lists of the last build that overflowed (those particles scan)
   // Work skipped by the gates of a captured step graph (conditional nodes): searches
-  // with no cell change, scan launches with every particle on a kept list.
-  int n_search_skipped, n_scan_skipped;
+  // with no cell change, scan launches with every particle on a list, list builds
+  // while the kept lists stand.
+  int n_search_skipped, n_scan_skipped, n_build_skipped;
   Motion<T> mv[kMotionMax];
   Table<T> tab[kMotionMax];
 };

@@ -338,12 +338,12 @@ def test_graph_gates_skip_idle_work_only(cases):
         for key in ("cellpos", "pospres", "velrhop", "str", "contact_var", "accad"):
             np.testing.assert_array_equal(g.get(key), p.get(key), err_msg=key)
         gi, pi = g.info(), p.info()
-        assert pi.n_search_skipped == 0 and pi.n_scan_skipped == 0
-        assert pi.graph_kernels - gi.graph_kernels == -4  # two search gates, two scan gates
-        if quiet:
-            assert gi.n_search_skipped > 0 and gi.n_scan_skipped > 0
+        assert pi.n_search_skipped == 0 and pi.n_scan_skipped == 0 and pi.n_build_skipped == 0
+        assert gi.graph_kernels - pi.graph_kernels == 6  # gates: 2 searches, 2 list builds, 2 scans
+        if quiet:  # every interaction walks a list; lists rebuilt once
+            assert gi.n_scan_skipped == 12 and gi.n_build_skipped == 11 and gi.n_search_skipped > 0
         else:
-            assert gi.n_scan_skipped == 0
+            assert gi.n_build_skipped == 0
         assert gi.device_err == 0
 
 
