@@ -701,13 +701,17 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
   const int kept = mode == 1 ? S.nbb_cnt[i] : -1;
   if (kept >= 0) {
     // Walk the kept list four entries at a time, each batch's neighbour data loaded
-    // together: a thread next to the soil waits for two loads per four entries instead
-    // of a chain of loads per entry.
+    // together and the next batch's entries loaded while it is in flight: a thread next
+    // to the soil waits for about one load per four entries instead of a chain of loads
+    // per entry.
     constexpr unsigned kNone = 0x7ffffffu;  // index of no particle (np < 2^27)
-    for (int e0 = 0; e0 < kept; e0 += 4) {
-      unsigned ent[4];
+    auto entries = [&](int e0, unsigned* ent) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) ent[k] = e0 + k < kept ? __ldcs(S.nbb + (size_t)(e0 + k) * P.npb + i) : kNone;
+    };
+    unsigned ent[4], nxt[4];
+    entries(0, ent);
+    for (int e0 = 0; e0 < kept; e0 += 4) {
       V4<T> pj[4], vj[4];
       T mj[4];
       S6<T> sj[4];
@@ -722,6 +726,7 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
           sj[k] = ld6(sa, sb, j);
         }
       }
+      entries(e0 + 4, nxt);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int j = (int)(ent[k] & kNone);
@@ -734,6 +739,8 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
           s6 = sj[k];
         });
       }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) ent[k] = nxt[k];
     }
   } else {
     scan(celli, pos_i, mode == 0 && keep);
@@ -884,14 +891,18 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
     const unsigned* __restrict__ lst = S.nbg + t;
     const size_t stride = (size_t)S.nbg_stride;
     constexpr unsigned kNone = 0x7ffffffu;  // index of no particle (np < 2^27)
-    for (int e0 = 0; e0 < kept; e0 += 4) {
-      unsigned ent[4];
+    auto entries = [&](int e0, unsigned* ent) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) ent[k] = e0 + k < kept ? __ldcs(lst + (size_t)(e0 + k) * stride) : kNone;
+    };
+    unsigned ent[4], nxt[4];
+    entries(0, ent);
+    for (int e0 = 0; e0 < kept; e0 += 4) {
       NbVals<T> nb[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k)
         if ((int)(ent[k] & kNone) < P.npb) nb[k] = load_nb(rec, (int)(ent[k] & kNone));
+      entries(e0 + 4, nxt);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int j = (int)(ent[k] & kNone);
@@ -900,6 +911,8 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
         visit(j, off_of((int)(ent[k] >> 27)), V3<T>{b.p.x, b.p.y, b.p.z}, [&] { return b.a.y < T(0); },
               [&] { return b.vr; });
       }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) ent[k] = nxt[k];
     }
   } else {
     for (int oc = 0; oc < 27; ++oc) {

@@ -90,3 +90,34 @@ def test_cli_runs_project(tmp_path):
     assert "output_0.xml" in files and "output_1.xml" in files and "time_history.txt" in files
     th = np.loadtxt(os.path.join(proj, "time_history.txt")).reshape(-1, 2)
     assert th.shape[0] >= 2
+
+
+def test_case_ingest_matches_host_conversion():
+    """rw_create_from_case copies the caller's double arrays as they are and converts them
+    on the device (LoadParticles' absolute -> in-cell split, src/loquat_grid.cu:322-330).
+    The state after creation equals the same conversion done on the host in float32,
+    bit for bit, row by row (rows are matched through the original index that the
+    loader keeps in idmassidx[:, 2], since creation also sorts by cell)."""
+    c = C.retaining_wall(nx=24, ny=12, nz=16, dx=0.004, name="ingest")
+    s = LoquatSph(case=c)
+    f32 = np.float32
+    h = f32(c.params["dr"]) * f32(c.params["hdr"])
+    half_ih = f32(0.5 * float(f32(1.0) / h))
+    two_h = f32(2.0 * float(h))
+    pa = c.pospres.astype(f32)
+    cell = (pa[:, :3] * half_ih).astype(np.int32)  # truncation toward zero
+    pos = pa.copy()
+    pos[:, :3] = pa[:, :3] - cell.astype(f32) * two_h
+    idx = s.get("idmassidx")[:, 2].astype(np.int64)
+    assert np.array_equal(np.sort(idx), np.arange(c.np_))
+    np.testing.assert_array_equal(s.get("pospres"), pos[idx].astype(np.float64))
+    np.testing.assert_array_equal(s.get("cellpos")[:, :3], cell[idx])
+    np.testing.assert_array_equal(s.get("codes"), c.codes[idx])
+    np.testing.assert_array_equal(s.get("velrhop"), c.velrhop.astype(f32)[idx].astype(np.float64))
+    np.testing.assert_array_equal(s.get("str"), c.stress.astype(f32)[idx].astype(np.float64))
+    np.testing.assert_array_equal(s.get("stn"), c.strain.astype(f32)[idx].astype(np.float64))
+    m = s.get("idmassidx")
+    np.testing.assert_array_equal(m[:, 1], c.idmassidx[:, 1].astype(f32)[idx].astype(np.float64))
+    assert np.all(idx[:c.npb] < c.npb)  # boundary rows stay in front
+    np.testing.assert_array_equal(s.get("normal_m"), c.normal.astype(f32)[idx[:c.npb]].astype(np.float64))
+    assert s.info().device_err == 0
