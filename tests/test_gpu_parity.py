@@ -347,6 +347,27 @@ def test_graph_gates_skip_idle_work_only(cases):
         assert gi.device_err == 0
 
 
+def test_overflowing_lists_fall_back_to_the_scan(cases):
+    """With a skin wide enough that some candidate lists exceed their 96 entries, the
+    list build marks those lists and counts them; the scan launch takes exactly those
+    particles while the walk takes the rest.  The result equals scanning every
+    particle (skin 0), bit for bit."""
+    from retainwall_code_b200 import _abi
+
+    c = cases["wall_mini"]
+    a = LoquatSph(case=c)
+    a.set_option(_abi.OPT_LIST_SKIN, 0.45)
+    b = LoquatSph(case=c)
+    b.set_option(_abi.OPT_LIST_SKIN, 0.0)
+    a.step(4)
+    b.step(4)
+    ent, parts = a.list_stats()
+    assert 0 < parts < a.info().npm  # some lists kept, some overflowed
+    for key in ("cellpos", "pospres", "velrhop", "str", "contact_var", "accad"):
+        np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
+    assert a.info().device_err == 0
+
+
 def test_deletion_matches_oracle():
     """Soil thrown out through the open +x side of the grid is moved to the deleted cell
     (cuCheckOutDomain, src/predictor_corrector.cu:183-187; the count bookkeeping of
