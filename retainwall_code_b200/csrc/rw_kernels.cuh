@@ -464,7 +464,7 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
   }
   // Candidate lists: an interaction walks the kept lists when nothing was permuted and
   // no particle changed cell or moved more than the skin allows since they were built
-  // (the integrators raise list_kill); otherwise it scans the cells and keeps new lists.
+  // (the integrators raise list_kill); otherwise k_build_lists builds new ones first.
   // Lists built in the corrector section, from mid-step positions, are not kept.
   if (section >= 0) {
     if (dyn->need_sort || dyn->host_dirty) dyn->rec_stale = 1;  // until the next interaction

@@ -80,8 +80,8 @@ template <class T> struct Dyn {
   unsigned err;              // RW_DERR_* bits
   int step;
   int nchunks;               // live entries of the interaction chunk list
-  // Candidate lists kept across sections and steps: ix_mode 0 = scan the cells (and
-  // keep the lists), 1 = walk the kept lists.  list_kill: some particle changed cell or
+  // Candidate lists kept across sections and steps: ix_mode 0 = build new lists (then
+  // walk them), 1 = walk the kept lists.  list_kill: some particle changed cell or
   // moved too far since the lists were built; build_kill: lists built in this section
   // are not to be kept (a corrector-section rebuild).
   int ix_mode, list_ok, list_kill, build_kill;
