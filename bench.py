@@ -43,6 +43,10 @@ IX_WARP_INSTR_PER_SOIL = 337.22e6 / 960000
 IX_L1_SECTORS_PER_ENTRY = 2 + 1 / 8
 IX_L1_SECTORS_PER_SOIL = 240 / 32
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# Host bytes rw_create_from_case copies per particle (int32 x4 codes, double x4 position,
+# velocity and id/mass, double x6 stress and strain) and per boundary normal (double x4).
+H2D_PER_PARTICLE = 16 + 3 * 32 + 2 * 48
+H2D_PER_BOUNDARY = 32
 
 
 def peaks():
@@ -325,7 +329,8 @@ def run_batch(args, ws, rank, local):
                    "interaction_kernel_choice_rank0": {"0": kinds.count(0), "1": kinds.count(1)},
                    "parallelism": f"cases sharded over {ws} GPU(s), largest first"},
         "e2e": {"value": total_npm * args.steps / e2e_s, "unit": "particle-updates/s",
-                "h2d_bytes_per_step": int(sum(c.np_ * 144 + c.npb * 16 for c in host_cases) / args.steps),
+                "h2d_bytes_per_step": int(sum(c.np_ * H2D_PER_PARTICLE + c.npb * H2D_PER_BOUNDARY
+                                              for c in host_cases) / args.steps),
                 "d2h_bytes_per_step": 24 * len(mine),
                 "note": "upload of every case from pinned host arrays + batched steps + one wall-force read per step (rank 0)"},
         "candidate_lists_rank0": lists,
@@ -391,9 +396,10 @@ def run_ours(args, ws, rank, local):
     sim2_lists = sim2.list_stats()
     sim2.close()
     e2e = ws * npm * e2e_steps / e2e_s
-    # bytes uploaded by rw_create_from_case: codes, cell, position x2, velocity, id/mass,
-    # stress, strain (float32 structure of arrays) + boundary normals
-    h2d = inf.np * (16 * 6 + 24 * 2) + inf.npb * 16
+    # bytes uploaded by rw_create_from_case: the caller's arrays as they are (codes 16 B,
+    # position, velocity, id/mass 32 B each, stress and strain 48 B each; normals 32 B
+    # per boundary particle), converted on the device
+    h2d = inf.np * H2D_PER_PARTICLE + inf.npb * H2D_PER_BOUNDARY
     # ---- roofline of the dominant kernel ------------------------------------------------
     pk, kind = peaks()
     list_entries, list_parts = sim2_lists
