@@ -720,13 +720,21 @@ template <class T> struct Engine final : EngineBase {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
       }
-      cudaGraph_t g = capture_step(graph_gates);
-      cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
-      cudaGraphDestroy(g);
-      graph_cond = graph_gates && e == cudaSuccess;
-      if (e != cudaSuccess) {  // a driver without conditional nodes: plain step graph
+      cudaError_t e = cudaErrorNotSupported;
+      if (graph_gates) {
+        try {
+          cudaGraph_t g = capture_step(true);
+          e = cudaGraphInstantiate(&gexec, g, 0);
+          cudaGraphDestroy(g);
+        } catch (const Fail&) {  // capture with conditional nodes refused
+          e = cudaErrorNotSupported;
+        }
+      }
+      graph_cond = e == cudaSuccess;
+      if (e != cudaSuccess) {  // gates off, or a driver without conditional nodes: plain step graph
         cudaGetLastError();
-        g = capture_step(false);
+        gexec = nullptr;
+        cudaGraph_t g = capture_step(false);
         e = cudaGraphInstantiate(&gexec, g, 0);
         cudaGraphDestroy(g);
       }
@@ -1268,11 +1276,16 @@ struct Batch {
           if (rc != cudaSuccess) break;
         }
         if (rc == cudaSuccess) rc = cudaGraphInstantiate(&gexec, parent, 0);
+      } catch (const Fail&) {
+        cudaGraphDestroy(parent);
+        if (!gates) throw;
+        rc = cudaErrorNotSupported;  // capture with conditional nodes refused: plain children
+        parent = nullptr;
       } catch (...) {
         cudaGraphDestroy(parent);
         throw;
       }
-      cudaGraphDestroy(parent);
+      if (parent) cudaGraphDestroy(parent);
       if (rc != cudaSuccess) {
         gexec = nullptr;
         cudaGetLastError();
