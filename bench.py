@@ -6,7 +6,13 @@ inputs from retainwall_code_b200.cases.retaining_wall.  A step is one whole
 StepCalculation + PredictorSection + CorrectorSection (src/loquat.cu:548-561), replayed
 from a captured CUDA graph; the state (~1.6 GB) is larger than L2, so no flush is needed.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload wall2|col1]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload wall2|wall2_half|col1|batch64|batch64_forms|closure] [--precision-report]
+
+Workloads besides the default: batch64 (the 64-case sweep in one graph launch per step),
+batch64_forms (the same with the precision form and the learned closure, against plain
+FP32), closure (the learned closure on the 1.92M wall), --precision-report (the
+precision form against FP64).
 
 --gpus N under torchrun: N independent replicas of the case, one per GPU (the single
 case does not shard); value = N x npm x K / max-over-ranks device time.
@@ -340,6 +346,87 @@ def run_batch(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_batch_forms(args, ws, rank, local):
+    """The three forms together on the batched sweep: the 64 cases advanced in one graph
+    launch per step with the precision form (compensated integration, FP64 norms) and the
+    learned closure (trained as in the closure workload), against the same batch in plain
+    FP32.  value = aggregate particle-updates/s of the combined form; each case's wall
+    resultant after the timed steps is compared with its plain run."""
+    import numpy as np
+
+    from retainwall_code_b200 import Batch, LoquatSph, _abi, cases as C
+
+    specs = C.batch_sweep(n_cases=args.batch_cases)
+    owner, loads = shard_cases(specs, ws)
+    mine = [s for k, s in enumerate(specs) if owner[k] == rank]
+    cases = [C.retaining_wall(nx=s["nx"], ny=s["ny"], nz=s["nz"], dx=s["dx"], phi_c=s["phi_c"], e0=s["e0"],
+                              mode=s["mode"], seed=s["seed"], name=s["name"]) for s in mine]
+    net, training = train_closure(args, local) if args.batch_forms != "precision" else (None, None)
+    res = {}
+    for form in ("plain", "forms"):
+        sims = []
+        for c in cases:
+            sim = LoquatSph(case=c, device=local, precision=4)
+            if form == "forms":
+                if args.batch_forms in ("both", "precision"):
+                    sim.set_option(_abi.OPT_MIXED_PRECISION, 1)
+                if args.batch_forms in ("both", "closure"):
+                    sim.set_closure(net, margin=0.05)
+            sims.append(sim)
+        b = Batch(sims)
+        b.step(args.warmup)
+        b.synchronize()
+        barrier(ws)
+        with ClockSampler(local) as clk:
+            ms = b.step_timed(args.steps)
+        ms = allreduce_max(ms, ws)
+        # the lateral resultant averaged over 50 further steps: one step's contact force
+        # flickers with single contacts opening and closing
+        navg = 50
+        forces = np.zeros(len(sims))
+        for _ in range(navg):
+            b.step(1)
+            forces += b.wall_force(0)[:, 0] / navg
+        stats = [sim.closure_stats() for sim in sims] if form == "forms" and net is not None else []
+        errs = [sim.info().device_err for sim in sims]
+        res[form] = {"ms": ms, "forces": forces, "stats": stats, "clocks": clk.summary(), "err": max(errs)}
+        b.close()
+        for sim in sims:
+            sim.close()
+    total_npm = sum(s["nx"] * s["ny"] * s["nz"] for s in specs)
+    value = total_npm * args.steps / (res["forms"]["ms"] * 1e-3)
+    plain = total_npm * args.steps / (res["plain"]["ms"] * 1e-3)
+    fp, ff = res["plain"]["forces"], res["forms"]["forces"]
+    scale = np.maximum(np.abs(fp), 1e-9)
+    rel = np.abs(ff - fp) / scale
+    offered = sum(st["offered"] for st in res["forms"]["stats"])
+    used = sum(st["used"] for st in res["forms"]["stats"])
+    judged = [st["mean_rel_err"] for st in res["forms"]["stats"] if st["used"] > 0]
+    line = {
+        "metric": "aggregate particle-updates/s, batched sweep of 64 retaining-wall cases, precision form + learned closure",
+        "value": value, "unit": "particle-updates/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["forms"]["ms"] / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32+bf16", "data": "synthetic (seeded generator, config-5 sweep)",
+        "config": {"workload": "batched sweep, combined forms", "forms": args.batch_forms, "cases": len(specs),
+                   "soil_particles_total": total_npm,
+                   "cases_on_rank0": len(mine), "parallelism": f"cases sharded over {ws} GPU(s), largest first"},
+        "plain_batch": {"value": plain, "ms_per_step": res["plain"]["ms"] / args.steps},
+        "forms_over_plain_batch": value / plain,
+        "wall_force_vs_plain_fp32": {"averaged_over_steps": 50,
+                                     "max_rel": float(rel.max()), "median_rel": float(np.median(rel)),
+                                     "cases_within_1pct": int((rel <= 0.01).sum()), "cases": int(len(rel)),
+                                     "per_case": [[s["mode"], s["nx"] * s["ny"] * s["nz"], float(a), float(b)]
+                                                  for s, a, b in zip(mine, fp, ff)]},
+        "closure": {"offered": offered, "used": used, "used_share": used / max(offered, 1),
+                    "mean_judged_rel_err_over_cases": float(np.mean(judged)) if judged else None},
+        "training": training,
+        "clocks": res["forms"]["clocks"],
+        "device_err": max(res["forms"]["err"], res["plain"]["err"]),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
 
@@ -569,18 +656,14 @@ def closure_accuracy(net, steps, device):
     return out
 
 
-def run_closure(args, ws, rank, local):
-    """The learned-closure form: a network trained on plain runs of the column collapse
-    and retaining-wall configurations (phi_c 28-40 deg, e0 0.55-0.80), then the 1.92M
-    retaining wall stepped with and without it.  value = particle-updates/s with the
-    closure; the plain throughput, the closure's judged error, its fallback share and the
-    wall force against the plain run are reported beside it."""
-    import numpy as np
-
-    from retainwall_code_b200 import LoquatSph, cases as C
+def train_closure(args, device):
+    """The closure network trained on plain runs of the column collapse and of retaining
+    walls of the batched sweep's kind (phi_c 28-40 deg, e0 0.55-0.80, three wall modes,
+    per-sample material augmentation); returns (network, training record)."""
+    from retainwall_code_b200 import cases as C
     from retainwall_code_b200.closure import Mlp, training_run
 
-    net = Mlp(device=local, seed=1, sample_capacity=args.closure_samples)
+    net = Mlp(device=device, seed=1, sample_capacity=args.closure_samples)
     t0 = time.perf_counter()
     runs = 0
     while net.sample_count() < args.closure_samples:
@@ -596,14 +679,29 @@ def run_closure(args, ws, rank, local):
             case = C.retaining_wall(nx=80, ny=32, nz=40, dx=0.004, phi_c=phi, e0=e0, mode=mode, seed=100 + runs)
             stride = 16
         training_run(net, case, steps=args.closure_run_steps, every=max(4, args.closure_run_steps // 100),
-                     stride=stride, device=local, seed=runs)
+                     stride=stride, device=device, seed=runs)
         runs += 1
     collect_s = time.perf_counter() - t0
     n_samples = net.sample_count()
     t0 = time.perf_counter()
     loss = net.train(epochs=args.closure_epochs, batch=8192, lr=2e-3, seed=1)
     train_s = time.perf_counter() - t0
+    return net, {"samples": n_samples, "runs": runs, "collect_s": collect_s, "epochs": args.closure_epochs,
+                 "train_s": train_s, "samples_per_s": n_samples * args.closure_epochs / train_s,
+                 "final_mse": loss}
 
+
+def run_closure(args, ws, rank, local):
+    """The learned-closure form: a network trained on plain runs of the column collapse
+    and retaining-wall configurations (phi_c 28-40 deg, e0 0.55-0.80), then the 1.92M
+    retaining wall stepped with and without it.  value = particle-updates/s with the
+    closure; the plain throughput, the closure's judged error, its fallback share and the
+    wall force against the plain run are reported beside it."""
+    import numpy as np
+
+    from retainwall_code_b200 import LoquatSph, cases as C
+
+    net, training = train_closure(args, local)
     acc = closure_accuracy(net, args.closure_acc_steps, local)
     case, cfg = make_case("wall2")
     res = {}
@@ -649,9 +747,7 @@ def run_closure(args, ws, rank, local):
                                             "unit": "TFLOP/s", "frac": tflops / pk["bf16_tflops"],
                                             "note": "two launches per step; MACs of the padded 16-64-64-64-64-16 net"}},
             "accuracy_vs_fp64": acc,
-            "training": {"samples": n_samples, "runs": runs, "collect_s": collect_s, "epochs": args.closure_epochs,
-                         "train_s": train_s, "samples_per_s": n_samples * args.closure_epochs / train_s,
-                         "final_mse": loss},
+            "training": training,
             "stage_ms": res["closure"]["stages"], "gpu_launches": res["closure"]["launched"],
             "clocks": res["closure"]["clocks"], "device_err": res["closure"]["err"],
         }), flush=True)
@@ -674,6 +770,8 @@ def main():
     ap.add_argument("--precision-report", action="store_true", help="precision form vs FP64 (configs 1 and 3)")
     ap.add_argument("--precision-steps", type=int, default=2000)
     ap.add_argument("--batch-cases", type=int, default=64)
+    ap.add_argument("--batch-forms", choices=["both", "closure", "precision"], default="both",
+                    help="forms applied in the batch64_forms workload")
     ap.add_argument("--closure-samples", type=int, default=10_000_000)
     ap.add_argument("--closure-epochs", type=int, default=30)
     ap.add_argument("--closure-run-steps", type=int, default=2000)
@@ -691,6 +789,8 @@ def main():
     try:
         if args.workload == "batch64":
             run_batch(args, ws, rank, local)
+        elif args.workload == "batch64_forms":
+            run_batch_forms(args, ws, rank, local)
         elif args.workload == "closure":
             run_closure(args, ws, rank, local)
         else:

@@ -155,10 +155,13 @@ enum {
                                    candidates within 2h + skin and walks them instead of the 27 cells until
                                    a sort permutes, a particle changes cell, or a particle may have moved
                                    0.45 skin; results do not depend on it. */
-  RW_OPT_GRAPH_GATES = 6        /* 1 (default): the captured step graph skips a search with no cell change
+  RW_OPT_GRAPH_GATES = 6,       /* 1 (default): the captured step graph skips a search with no cell change
                                    and an idle scan launch behind conditional nodes; 0: plain graph, every
                                    kernel launched (profilers that replay single graph kernels need it).
                                    Results do not depend on it. */
+  RW_OPT_CLOSURE_MAX_ERR = 7    /* learned closure: a particle keeps the network's objective rate only while
+                                   its judged relative error against the exact rate is at most this
+                                   (default 0.02; 0: no bound, the trust region alone decides) */
 };
 
 const char* rw_status_string(rw_status s);
@@ -335,8 +338,9 @@ rw_status rw_mlp_collect(rw_mlp* m, rw_ctx* ctx, int stride, const double* augme
 /* Uses the network for the objective stress rate of this context's HypoCS particles
  * (NULL: exact updates again).  A particle uses it only when all its features lie within
  * the ranges of the network's stored samples, each widened by `margin` times its width,
- * and every output within (1 + margin) times the largest stored |target|; otherwise, and
- * for the zero-stress reset, the exact update runs.  The Jaumann term, the tension
+ * and every output within (1 + margin) times the largest stored |target|, and the
+ * network's rate is within RW_OPT_CLOSURE_MAX_ERR of the exact one (which is computed
+ * anyway to judge it); otherwise, and for the zero-stress reset, the exact update runs.  The Jaumann term, the tension
  * cut-off and the cone projection stay exact.  Ranges are taken at this call; the
  * weights are read at every step. */
 rw_status rw_set_closure(rw_ctx* ctx, rw_mlp* m, double margin);

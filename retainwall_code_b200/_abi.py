@@ -13,6 +13,7 @@ MODEL_MAX, MATERIAL_SIZE, MOTION_MAX, TABLE_MAX = 10, 15, 10, 10
 OPT_WALL_FRICTION, OPT_COMPAT_CONTACT, OPT_INTERACTION_KERNEL, OPT_STRICT_FP, OPT_MIXED_PRECISION = 0, 1, 2, 3, 4
 OPT_LIST_SKIN = 5
 OPT_GRAPH_GATES = 6
+OPT_CLOSURE_MAX_ERR = 7
 
 # rw_array ids and their row shapes (columns, integer?)
 ARRAYS: Dict[str, int] = {

@@ -88,6 +88,7 @@ template <class T> struct Engine final : EngineBase {
   int saves = 0;  // the first save is RunSimulation's initial output
   rw_mlp* cl_net = nullptr;  // learned closure (P.closure), its trust region and statistics
   ClosureTrust cl_trust{};
+  double cl_err_max = 0.02;  // RW_OPT_CLOSURE_MAX_ERR
   double* d_clstats = nullptr;
   unsigned long long* d_count = nullptr;
   int nsm = 148;
@@ -613,6 +614,7 @@ template <class T> struct Engine final : EngineBase {
       cl_trust.hi[k] = hi[k] + (float)margin * w;
     }
     cl_trust.out_max = tmax * (1.0f + (float)margin);
+    cl_trust.err_max = (float)cl_err_max;
     RW_CU(cudaSetDevice(device));
     RW_CU(cudaFuncSetAttribute(k_closure<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(mlp::FwdSmem)));
@@ -916,6 +918,13 @@ template <class T> struct Engine final : EngineBase {
       strict_fp = v != 0.0;
     } else if (opt == RW_OPT_GRAPH_GATES) {
       graph_gates = v != 0.0;
+    } else if (opt == RW_OPT_CLOSURE_MAX_ERR) {
+      if (!(v >= 0.0)) {
+        err = "closure error bound must be >= 0";
+        return RW_EINVAL;
+      }
+      cl_err_max = v;
+      cl_trust.err_max = (float)v;
     } else if (opt == RW_OPT_INTERACTION_KERNEL) {
       if (v != 0.0 && v != 1.0) return RW_EINVAL;
       const int was = ix_kernel;

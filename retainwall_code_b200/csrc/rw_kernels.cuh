@@ -2030,6 +2030,7 @@ static __global__ void k_list_totals(const int* cnt, int n, unsigned long long* 
 struct ClosureTrust {
   float lo[mlp::IN], hi[mlp::IN];  // accepted feature ranges
   float out_max;                   // accepted |output|
+  float err_max;                   // accepted judged relative error of the rate (<= 0: no bound)
 };
 
 template <class T> RWD void closure_features(const HypoPre<T>& h, const S6<T>& D, const T* mp, float* f) {
@@ -2203,15 +2204,19 @@ __global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevSta
 #pragma unroll
         for (int o = 0; o < mlp::OUT; ++o) use = use && fabsf(y[o]) <= tr.out_max;
         if (h.nD > T(0)) offered = 1.0f;
-        if (use) {
+        if (use) {  // judged against the exact objective rate; kept within the error bound
           const S6<T> Rm = closure_scale_out(h, y);
           const S6<T> Rx = hypo_cs_objective(h, D);
           const S6<T> d = Rm - Rx;
           const T nx = f_sqrt(trace2(Rx, Rx)), nd = f_sqrt(trace2(d, d));
           err = (float)(nd / (nx + T(1e-30)));
+          use = !(tr.err_max > 0.0f) || err <= tr.err_max;
+        }
+        if (use) {
           used = 1.0f;
-          rate = h.jau + Rm;
+          rate = h.jau + closure_scale_out(h, y);
         } else {
+          err = 0.0f;
           rate = hypo_cs_rate(h, D);
         }
         hypo_cs_post(dt, h, rate, sg);

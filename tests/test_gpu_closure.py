@@ -148,3 +148,41 @@ def test_augmented_samples_follow_the_exact_law():
          + (sh + dev) * (C4 * x[:, 12] ** alpha)[:, None]) / 1000.0
     assert rel(t, R) < 2e-5
     assert rel(x[:, 14], x[:, 12] ** alpha) < 1e-5
+
+
+def test_judged_error_bound():
+    """Every update that uses the network is judged against the exact objective rate;
+    RW_OPT_CLOSURE_MAX_ERR keeps the network's rate only within that relative error.
+    With a bound of 1e-9 no update keeps it and the step follows the plain method; with
+    a bound at the unbounded run's mean judged error, fewer updates keep it and none of
+    those is judged worse than the bound."""
+    from retainwall_code_b200 import _abi
+
+    c = C.column_collapse(nx=8, ny=8, nz=16, runout=1.0)
+    net = Mlp(seed=5, sample_capacity=200_000)
+    training_run(net, c, steps=20, every=2)
+    net.train(epochs=10, batch=2048, lr=2e-3, seed=2)
+    plain = LoquatSph(case=c)
+    tight = LoquatSph(case=c)
+    tight.set_closure(net, margin=0.05)
+    tight.set_option(_abi.OPT_CLOSURE_MAX_ERR, 1e-9)
+    free = LoquatSph(case=c)
+    free.set_closure(net, margin=0.05)
+    free.set_option(_abi.OPT_CLOSURE_MAX_ERR, 0.0)
+    for s in (plain, tight, free):
+        s.step(10)
+    st = tight.closure_stats()
+    assert st["offered"] > 0 and st["used"] == 0
+    for key in ("pospres", "velrhop", "str"):
+        assert rel(tight.get(key), plain.get(key)) < 1e-6, key
+    sf = free.closure_stats()
+    assert sf["used"] > 0 and sf["max_rel_err"] > sf["mean_rel_err"] > 0
+    bound = LoquatSph(case=c)
+    bound.set_closure(net, margin=0.05)
+    bound.set_option(_abi.OPT_CLOSURE_MAX_ERR, sf["mean_rel_err"])
+    bound.step(10)
+    sb = bound.closure_stats()
+    assert 0 < sb["used"] < sf["used"]
+    assert sb["max_rel_err"] <= sf["mean_rel_err"] * (1 + 1e-6)
+    for s in (tight, free, bound):
+        assert s.info().device_err == 0
