@@ -305,7 +305,8 @@ def run_batch(args, ws, rank, local):
     infos = [sim.info() for sim in sims]
     lists = {"sections_that_sorted": sum(i.n_sorts for i in infos),
              "interactions_on_kept_lists": sum(i.n_list_reuse for i in infos),
-             "interactions": sum(2 * i.step for i in infos)}
+             "interactions": sum(2 * i.step for i in infos),
+             "searches_skipped_by_graph_gates": sum(i.n_search_skipped for i in infos)}
     for sim in sims:
         if sim.info().device_err:
             raise SystemExit("device error word set")

@@ -58,6 +58,9 @@ struct EngineBase {
   virtual void wall_profile(double x_wall, double z_top, double dz, int nbins, double* out) = 0;
   virtual double step_timed(int n) = 0;
   virtual cudaGraph_t step_graph(bool gates) = 0;
+  // Launches one whole step on this context's stream while that stream takes part in a
+  // capture begun elsewhere (the batch's fork/join capture).
+  virtual void launch_into_capture(bool gates) = 0;
   // Wall resultant computed on stream s into the device array d_out (3 doubles).
   virtual void wall_force_enqueue(cudaStream_t s, int mode, int wall_id, const double* strip, double* d_out) = 0;
   virtual cudaStream_t stream() const = 0;
@@ -819,6 +822,19 @@ template <class T> struct Engine final : EngineBase {
   }
 
   cudaGraph_t step_graph(bool gates) override { return capture_step(gates && graph_gates); }
+  void launch_into_capture(bool gates) override {
+    const int c0 = cpar;
+    allow_cond = gates && graph_gates;
+    try {
+      launch_step();
+    } catch (...) {
+      allow_cond = false;
+      cpar = c0;
+      throw;
+    }
+    allow_cond = false;
+    cpar = c0;  // the step runs two interactions: parity is back where it started
+  }
 
   // Defaults of the reference's profile (src/utilities.cu:284-292,336): wall face at
   // 0.04 + bound_thickness - 0.005 t, top at 0.04 + 1.0 + bound_thickness, bins of dr,
@@ -1266,11 +1282,43 @@ struct Batch {
     if (d_wf) cudaFree(d_wf);
     if (h_wf) cudaFreeHost(h_wf);
   }
-  // Parent graph with every context's step as an independent child graph: the branches
-  // have no dependencies on each other, so the executor runs them concurrently.  The
-  // children keep their conditional gates where the driver accepts them in child
-  // graphs; otherwise they are plain step graphs.
+  // One graph holding every context's step as an independent branch, so the executor
+  // runs them concurrently.  First choice: a single capture forked from the batch's
+  // stream onto each context's stream and joined back, which keeps each step's
+  // conditional gates.  Otherwise a parent graph of per-context child graphs, gated
+  // where the driver accepts conditional nodes in child graphs, plain if not.
+  bool build_forked() {
+    std::vector<cudaEvent_t> ev(engines.size() + 1, nullptr);
+    for (auto& e : ev) RW_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaGraph_t g = nullptr;
+    bool ok = false;
+    RW_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      RW_CU(cudaEventRecord(ev[0], st));
+      for (size_t k = 0; k < engines.size(); ++k) {
+        cudaStream_t es = engines[k]->stream();
+        RW_CU(cudaStreamWaitEvent(es, ev[0], 0));
+        engines[k]->launch_into_capture(true);
+        RW_CU(cudaEventRecord(ev[k + 1], es));
+        RW_CU(cudaStreamWaitEvent(st, ev[k + 1], 0));
+      }
+      RW_CU(cudaStreamEndCapture(st, &g));
+      ok = cudaGraphInstantiate(&gexec, g, 0) == cudaSuccess;
+    } catch (const Fail&) {
+      cudaStreamEndCapture(st, &g);  // ends the capture on every joined stream
+      ok = false;
+    }
+    if (g) cudaGraphDestroy(g);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (!ok) {
+      gexec = nullptr;
+      cudaGetLastError();
+    }
+    gated = ok;
+    return ok;
+  }
   void build() {
+    if (build_forked()) return;
     for (int attempt = 0; attempt < 2 && !gexec; ++attempt) {
       const bool gates = attempt == 0;
       cudaGraph_t parent = nullptr;

@@ -246,6 +246,8 @@ def test_batch_equals_individual_runs():
     b.synchronize()
     forces = b.wall_force(0)
     assert forces.shape == (3, 3)
+    # the batch graph keeps each step's gates: quiet sections skip their search
+    assert sum(t.info().n_search_skipped for t in together) > 0
     for k, (c, t) in enumerate(zip(cs, together)):
         alone = LoquatSph(case=c)
         alone.step(6)
