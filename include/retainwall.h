@@ -253,8 +253,8 @@ rw_status rw_profile(rw_ctx* ctx, int nsteps, double* ms_per_stage, int n_stages
 
 /* Batched cases (no reference counterpart; the reference runs one case per process).
  * Contexts on one device are advanced together: each context's whole step becomes an
- * independent child graph of one parent graph, so one graph launch per step runs every
- * case and the executor overlaps their kernels.  rw_batch_step is asynchronous unless
+ * independent branch of one graph (captured forked onto the contexts' streams), so one
+ * graph launch per step runs every case and the executor overlaps their kernels.  rw_batch_step is asynchronous unless
  * ms is non-NULL (then it waits and returns the device time of the nsteps launches);
  * call rw_batch_synchronize before reading any context.  The contexts must outlive the
  * batch and must not be stepped individually while it is in use. */

@@ -697,8 +697,8 @@ template <class T> struct Engine final : EngineBase {
   }
 
   // One whole step captured as a graph (not instantiated); the caller owns it.
-  // cond: gate the search and the scan launch with conditional nodes (gated()).  The
-  // batched sweep nests step graphs as child graphs and captures them without.
+  // cond: gate the search, the list build and the scan launch with conditional nodes
+  // (gated()).  The batch's fallback nests step graphs as child graphs, without.
   cudaGraph_t capture_step(bool cond = false) {
     cudaGraph_t g = nullptr;
     const int c0 = cpar;
