@@ -373,6 +373,7 @@ def run_batch_forms(args, ws, rank, local):
                     sim.set_option(_abi.OPT_MIXED_PRECISION, 1)
                 if args.batch_forms in ("both", "closure"):
                     sim.set_closure(net, margin=0.05)
+                    sim.set_option(_abi.OPT_CLOSURE_MAX_ERR, args.closure_max_err)
             sims.append(sim)
         b = Batch(sims)
         b.step(args.warmup)
@@ -610,13 +611,13 @@ def precision_report(args):
     print(json.dumps(out), flush=True)
 
 
-def closure_accuracy(net, steps, device):
+def closure_accuracy(net, steps, device, max_err=0.02):
     """FP64 runs against plain FP32 and FP32 with the learned closure, same seeds: the
     column collapse (config 1's case) for positions and stress invariants, a 41k
     retaining wall for the wall resultant (largest deviation over the run)."""
     import numpy as np
 
-    from retainwall_code_b200 import LoquatSph, cases as C
+    from retainwall_code_b200 import LoquatSph, _abi, cases as C
 
     def rel(a, b):
         return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-300))
@@ -629,6 +630,7 @@ def closure_accuracy(net, steps, device):
             sim = LoquatSph(case=case, precision=8 if mode == "f64" else 4, device=device)
             if mode == "closure":
                 sim.set_closure(net, margin=0.05)
+                sim.set_option(_abi.OPT_CLOSURE_MAX_ERR, max_err)
             x0 = sim.get("pos_abs")[:, :3].astype(np.float64)
             wf, done, chunk = [], 0, max(1, steps // 20)
             while done < steps:
@@ -700,16 +702,17 @@ def run_closure(args, ws, rank, local):
     wall force against the plain run are reported beside it."""
     import numpy as np
 
-    from retainwall_code_b200 import LoquatSph, cases as C
+    from retainwall_code_b200 import LoquatSph, _abi, cases as C
 
     net, training = train_closure(args, local)
-    acc = closure_accuracy(net, args.closure_acc_steps, local)
+    acc = closure_accuracy(net, args.closure_acc_steps, local, args.closure_max_err)
     case, cfg = make_case("wall2")
     res = {}
     for mode in ("plain", "closure"):
         sim = LoquatSph(case=case, device=local)
         if mode == "closure":
             sim.set_closure(net, margin=0.05)
+            sim.set_option(_abi.OPT_CLOSURE_MAX_ERR, args.closure_max_err)
         sim.step(args.warmup)
         sim.synchronize()
         barrier(ws)
@@ -777,6 +780,8 @@ def main():
     ap.add_argument("--closure-epochs", type=int, default=30)
     ap.add_argument("--closure-run-steps", type=int, default=2000)
     ap.add_argument("--closure-acc-steps", type=int, default=2000)
+    ap.add_argument("--closure-max-err", type=float, default=0.02,
+                    help="judged-error bound of the closure (RW_OPT_CLOSURE_MAX_ERR)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.precision_report:
