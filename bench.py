@@ -229,12 +229,13 @@ def interaction_bytes(inf, ncell: int, scalar: int, list_entries: int = 0) -> in
     return inf.npm * per_soil + inf.np * 16 * s + 4 * list_entries + ncell * 8
 
 
-def cpu_sample(case, threads: int, steps: int):
-    """The reference step on host cores: the CPU restatement, full case, `steps` steps."""
+def cpu_sample(case, threads: int, steps: int, precision: int = 4):
+    """The reference step on host cores: the CPU restatement, full case, `steps` steps
+    (precision 4: float, as the reference's default build; 8: double)."""
     from oracle.oracle import Oracle
 
     t0 = time.perf_counter()
-    o = Oracle(case, 4, threads)
+    o = Oracle(case, precision, threads)
     t_init = time.perf_counter() - t0
     o.step(1)  # warm-up step
     t0 = time.perf_counter()
@@ -542,6 +543,9 @@ def run_ours(args, ws, rank, local):
         ups, dt, _ = cpu_sample(case, threads, 2)
         line["cpu_baseline"] = {"value": ups, "unit": "particle-updates/s", "cores": threads, "kind": "port",
                                 "sample": f"2 whole steps of the full {npm}-particle case (+1 warm-up)"}
+        ups64, _, _ = cpu_sample(case, threads, 1, precision=8)
+        line["cpu_baseline_f64"] = {"value": ups64, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+                                    "sample": f"1 whole FP64 step of the full {npm}-particle case (+1 warm-up)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
