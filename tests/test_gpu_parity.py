@@ -349,6 +349,32 @@ def test_graph_gates_skip_idle_work_only(cases):
         assert gi.device_err == 0
 
 
+def test_options_changed_between_steps_keep_the_state(cases):
+    """Options that rebuild the step graph (gates, list skin, interaction kernel) can be
+    changed between steps; the state carries over and the run equals one that kept the
+    defaults, bit for bit."""
+    from retainwall_code_b200 import _abi
+
+    c = cases["wall_mini"]
+    ref = LoquatSph(case=c)
+    ref.step(8)
+    s = LoquatSph(case=c)
+    s.step(2)
+    s.set_option(_abi.OPT_GRAPH_GATES, 0)
+    s.step(2)
+    s.set_option(_abi.OPT_LIST_SKIN, 0.0)
+    s.step(2)
+    s.set_option(_abi.OPT_GRAPH_GATES, 1)
+    s.set_option(_abi.OPT_LIST_SKIN, 0.02)
+    s.set_option(_abi.OPT_INTERACTION_KERNEL, 1)
+    s.step(1)
+    s.set_option(_abi.OPT_INTERACTION_KERNEL, 0)
+    s.step(1)
+    for key in ("cellpos", "pospres", "velrhop", "str", "contact_var", "accad"):
+        np.testing.assert_array_equal(s.get(key), ref.get(key), err_msg=key)
+    assert s.info().step == 8 and s.info().device_err == 0
+
+
 def test_overflowing_lists_fall_back_to_the_scan(cases):
     """With a skin wide enough that some candidate lists exceed their 96 entries, the
     list build marks those lists and counts them; the scan launch takes exactly those
