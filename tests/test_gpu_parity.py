@@ -245,7 +245,8 @@ def test_batch_equals_individual_runs():
     b.step(6)
     b.synchronize()
     forces = b.wall_force(0)
-    assert forces.shape == (3, 3)
+    strips = b.wall_force(1)
+    assert forces.shape == (3, 3) and strips.shape == (3, 3)
     # the batch graph keeps each step's gates: quiet sections skip their search
     assert sum(t.info().n_search_skipped for t in together) > 0
     for k, (c, t) in enumerate(zip(cs, together)):
@@ -255,6 +256,7 @@ def test_batch_equals_individual_runs():
             np.testing.assert_array_equal(t.get(key), alone.get(key), err_msg=key)
         assert t.info().step == 6
         np.testing.assert_array_equal(forces[k], alone.wall_force(0))
+        np.testing.assert_array_equal(strips[k], alone.wall_force(1))
     b.close()
 
 
