@@ -321,7 +321,12 @@ def run_batch(args, ws, rank, local):
     b.close()
     barrier(ws)
     t0 = time.perf_counter()
-    sims2 = [LoquatSph(case=c, device=local, precision=4) for c in host_cases]
+    # contexts are independent: a host creates them from several threads (each call
+    # holds no Python lock while the library uploads and converts its case)
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        sims2 = list(ex.map(lambda c: LoquatSph(case=c, device=local, precision=4), host_cases))
     b2 = Batch(sims2)
     for _ in range(args.steps):
         b2.step(1)
