@@ -18,6 +18,11 @@ precision form against FP64).
 case does not shard); value = N x npm x K / max-over-ranks device time.
 --impl reference: the reference step on the host cores (the CPU restatement of the
 reference's kernels, all threads), rank 0 only, a bounded sample of steps.
+
+Beside the headline the default line carries: `amortized` (the same case over 2000 steps
+from step 0, sorts and candidate-list rebuilds included), `reference_cuda` (the
+reference's own CUDA build on the same case files and GPU, timed by its driver) and the
+CPU baselines.
 """
 from __future__ import annotations
 
@@ -244,6 +249,36 @@ def cpu_sample(case, threads: int, steps: int, precision: int = 4):
     npm = o.info().npm
     o.close()
     return npm * steps / dt, dt, t_init
+
+
+def reference_cuda_sample(case, steps: int, warmup: int, device: int):
+    """The reference's own CUDA build (oracle/_ref/ref_driver_f32, built from the reference's
+    sources) on the same case files and the same GPU: its step loop timed with CUDA events
+    by the driver, clocks sampled meanwhile.  The reference hard-codes the wall friction
+    (0.58108); the step's work does not depend on its value."""
+    import tempfile
+
+    from retainwall_code_b200 import cases as C
+
+    drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver_f32")
+    if not os.path.exists(drv):
+        return {"unavailable": "oracle/_ref/ref_driver_f32 not built (needs the reference sources)"}
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    gpu = vis.split(",")[device] if vis else str(device)  # the driver runs on its device 0
+    with tempfile.TemporaryDirectory() as d:
+        proj = os.path.join(d, "wall")
+        C.write_case(case, proj)
+        with ClockSampler(device) as clk:
+            r = subprocess.run([drv, proj, "--steps", str(steps), "--warmup", str(warmup), "--time"],
+                               capture_output=True, text=True, timeout=1200,
+                               env=dict(os.environ, CUDA_VISIBLE_DEVICES=gpu))
+    if r.returncode != 0:
+        return {"unavailable": f"reference driver exited {r.returncode}: {r.stderr[-300:]}"}
+    rec = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    return {"value": rec["particle_updates_per_s"], "unit": "particle-updates/s", "ms_per_step": rec["ms_per_step"],
+            "steps": steps, "warmup": warmup, "npm": rec["npm"], "dtype": "f32",
+            "how": "unmodified reference build (sm_100a), RunSimulation's step loop, CUDA events", "clocks":
+            clk.summary()}
 
 
 def run_reference(args, ws, rank):
@@ -543,6 +578,21 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": launched,
         "clocks": clocks,
     }
+    # ---- the same case over a long window from step 0: sorts and list rebuilds included --
+    if rank == 0 and args.amortized_steps > 0:
+        sim3 = LoquatSph(case=case, device=local, precision=4)
+        with ClockSampler(local) as clk3:
+            ms3 = sim3.step_timed(args.amortized_steps)
+        i3 = sim3.info()
+        line["amortized"] = {
+            "value": i3.npm * args.amortized_steps / (ms3 * 1e-3), "unit": "particle-updates/s",
+            "steps": args.amortized_steps, "ms_per_step": ms3 / args.amortized_steps, "from_step": 0,
+            "sections_that_sorted": i3.n_sorts, "searches_skipped": i3.n_search_skipped,
+            "interactions": 2 * i3.step, "interactions_on_kept_lists": i3.n_list_reuse,
+            "list_builds": 2 * i3.step - i3.n_build_skipped, "clocks": clk3.summary()}
+        sim3.close()
+    if rank == 0 and ws == 1 and not args.no_reference_cuda:
+        line["reference_cuda"] = reference_cuda_sample(case, args.reference_cuda_steps, 3, local)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         ups, dt, _ = cpu_sample(case, threads, 2)
@@ -775,6 +825,10 @@ def main():
     ap.add_argument("--workload", default="wall2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end and stage-profile passes")
+    ap.add_argument("--no-reference-cuda", action="store_true", help="skip timing the reference's CUDA build")
+    ap.add_argument("--reference-cuda-steps", type=int, default=50)
+    ap.add_argument("--amortized-steps", type=int, default=2000,
+                    help="steps of the long window from step 0 (sorts and list rebuilds included); 0: skip")
     ap.add_argument("--ix-kernel", type=int, default=None, help="interaction kernel: 0 global (default), 1 chunked")
     ap.add_argument("--skin", type=float, default=None, help="kept candidate-list skin in units of h (0: scan cells)")
     ap.add_argument("--strict", action="store_true", help="separately rounded interaction arithmetic")

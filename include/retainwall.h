@@ -38,7 +38,7 @@ enum {
 /* Device error word bits (rw_info.device_err). */
 enum {
   RW_DERR_CELL_RANGE = 1,   /* a live particle's cell left the grid (reference: out-of-bounds write) */
-  RW_DERR_COUNT = 2,        /* particle-count invariant npb+npm+deleted != np (src/loquat_grid.cu:251-254) */
+  RW_DERR_COUNT = 2,        /* particle-count invariant npb+npm+deleted != np (src/loquat_grid.cu:182-185) */
   RW_DERR_LIST = 4,         /* neighbour list exceeded its per-cell capacity (handled, reported)  */
   RW_DERR_PERM = 8,         /* sort produced an index outside [0, np) (guarded; never expected)  */
   RW_DERR_CLOSURE = 16      /* a tensor-core wait of the learned closure gave up                  */
@@ -131,6 +131,9 @@ typedef struct rw_info {
                                   kept lists stood)                                              */
   int32_t graph_kernels;       /* kernels of one captured step when no gated body is skipped     */
   int32_t search_body_kernels; /* kernels a skipped search does not launch                       */
+  int32_t pad_;
+  double time_max;             /* time-max of the parameter file (src/loquat_io.cu:192)          */
+  double output_frequency;     /* output-frequency of the parameter file (src/loquat_io.cu:195)  */
 } rw_info;
 
 typedef struct rw_ctx rw_ctx;
@@ -180,7 +183,7 @@ rw_status rw_destroy(rw_ctx* ctx);
 
 /* StepCalculation (src/loquat.cu:366-374): dt = cfl*h/cs, time of this step. */
 rw_status rw_begin_step(rw_ctx* ctx);
-/* LoquatGrid::NeighborSearch (src/loquat_grid.cu:216-260) followed by SortArraysPrimary
+/* LoquatGrid::NeighborSearch (src/loquat_grid.cu:147-191) followed by SortArraysPrimary
  * (section 0, src/loquat.cu:254-266) or SortArraysAll (section 1, src/loquat.cu:269-287). */
 rw_status rw_neighbor_search(rw_ctx* ctx, int section);
 /* LoquatSph::RigidBodyUpdate (src/adami_boundary.cu:175-203), on the device. */
@@ -189,7 +192,7 @@ rw_status rw_rigid_body_update(rw_ctx* ctx);
 rw_status rw_adami_boundary(rw_ctx* ctx);
 /* LoquatSph::FindCornerParticle (src/adami_boundary.cu:294-306). */
 rw_status rw_find_corner(rw_ctx* ctx);
-/* LoquatSph::StressRegularization (src/field_smoothing.cu:305-314). */
+/* LoquatSph::StressRegularization (src/field_smoothing.cu:92-101). */
 rw_status rw_shepard_filter(rw_ctx* ctx);
 /* LoquatSph::ParticleInteraction (src/particle_interaction.cu:310-313). */
 rw_status rw_particle_interaction(rw_ctx* ctx);
@@ -230,6 +233,12 @@ rw_status rw_wall_profile(rw_ctx* ctx, double x_wall, double z_top, double dz, i
  * defaults) and appends "time F[kN]" to <outdir>/time_history.txt. */
 rw_status rw_save(rw_ctx* ctx, const char* outdir);
 
+/* The particle file <project>.dat of a case, as the reference's generator writes it
+ * (SaveDatFile, src/GenCase.cu:70-116, read back by LoquatIo::LoadParticles,
+ * src/loquat_io.cu:222-264): one row per particle, boundary rows first with their
+ * normal; reals printed as %.9g, so a float case reads back exactly.  Host only. */
+rw_status rw_write_case_dat(const rw_case* c, const char* path);
+
 rw_status rw_get_info(rw_ctx* ctx, rw_info* out);
 rw_status rw_set_option(rw_ctx* ctx, int option, double value);
 /* Copy an array out (host_dst, bytes = rows x row size of the context's precision). */
@@ -257,7 +266,9 @@ rw_status rw_profile(rw_ctx* ctx, int nsteps, double* ms_per_stage, int n_stages
  * graph launch per step runs every case and the executor overlaps their kernels.  rw_batch_step is asynchronous unless
  * ms is non-NULL (then it waits and returns the device time of the nsteps launches);
  * call rw_batch_synchronize before reading any context.  The contexts must outlive the
- * batch and must not be stepped individually while it is in use. */
+ * batch and must not be stepped individually while it is in use.  Options set on a
+ * context after rw_batch_create (rw_set_option, rw_set_closure) take effect at the next
+ * rw_batch_step, which captures the batch's graph again first. */
 typedef struct rw_batch rw_batch;
 rw_status rw_batch_create(rw_ctx* const* ctxs, int n, rw_batch** out);
 rw_status rw_batch_step(rw_batch* b, int nsteps, double* ms);
@@ -276,12 +287,13 @@ rw_status rw_list_stats(rw_ctx* ctx, int64_t* out);
 rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen);
 
 /* Allocation-free cell-key sort.  No counterpart in the reference (which sorts with
- * cub::DeviceRadixSort into buffers it cudaMallocs, src/loquat_grid.cu:167-182); for
+ * cub::DeviceRadixSort into buffers it cudaMallocs, src/loquat_grid.cu:98-113); for
  * callers that cannot allocate device memory.  Stable sort of n cell keys (device
  * array d_keys, values in [0, max_key]) into d_sorted_keys, with d_perm[i] = index of
  * the key that lands at position i: the permutation NeighborSearch applies.  Uses a
- * fixed scratch array inside the library (about 8.6 MB, reserved on every GPU that
- * loads the library until the process exits) instead of allocating: n is limited to
+ * fixed scratch array inside the library (8,913,924 bytes: 8.9 MB, 8.5 MiB, reserved
+ * on every GPU that loads the library until the process exits) instead of
+ * allocating: n is limited to
  * RW_NOALLOC_MAX_KEYS and max_key to 2^24 - 1 (RW_EINVAL beyond).  Runs on `stream`
  * (a cudaStream_t, NULL = default stream) of the current device.  The first call on a
  * device looks up the scratch address (cudaGetSymbolAddress); make that first call

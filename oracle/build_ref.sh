@@ -6,10 +6,12 @@
 #       oracle/ref_driver.cu in place of src/main.cpp (per-stage dumps, timing)
 #   oracle/_ref/libref_hypo_f32.so, _f64.so     : host build of src/functions.h +
 #       src/constitutive_model.h (known answers for the oracle's restatement)
-# Usage: oracle/build_ref.sh [REFERENCE_SRC_DIR]   (default /root/reference/src)
+# Usage: oracle/build_ref.sh [REFERENCE_SRC_DIR]
+#   the directory defaults to $RW_REFERENCE_SRC, else to the read-only reference checkout
+#   of the development machine; without sources the prebuilt files are kept.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-SRC="${1:-/root/reference/src}"
+SRC="${1:-${RW_REFERENCE_SRC:-/root/reference/src}}"
 OUT="$HERE/_ref"
 if [ ! -f "$SRC/loquat.cu" ]; then
   echo "reference sources not found at $SRC; keeping prebuilt files in $OUT" >&2

@@ -41,6 +41,7 @@ def lib():
         dp = ct.POINTER(ct.c_double)
         L.orc_hypo_cs.argtypes = [ct.c_int, ct.c_double, ct.c_double, dp, dp, dp, dp, dp]
         L.orc_hypo_basic.argtypes = [ct.c_int, ct.c_double, dp, dp, dp, dp]
+        L.orc_dp.argtypes = [ct.c_int, ct.c_int, ct.c_double, dp, dp, dp, dp, ct.POINTER(ct.c_int)]
         L.orc_kernel_w.restype = ct.c_double
         L.orc_kernel_w.argtypes = [ct.c_int, ct.c_double, ct.c_double]
         L.orc_kernel_f.restype = ct.c_double
@@ -124,3 +125,14 @@ def hypo_basic(precision, dt, omega4, rate6, sigma6, par15):
     P = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_double))
     lib().orc_hypo_basic(precision, dt, P(om), P(rt), P(sg), P(pr))
     return sg
+
+
+def dp(precision, dt, omega4, rate6, sigma6, par15, mui=False):
+    """Drucker-Prager (mui=False; returns (stress, yield flag)) or mu(I)-DP (mui=True;
+    returns (stress, 0)) stress update."""
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    om, rt, sg, pr = f(omega4), f(rate6), f(sigma6).copy(), f(par15)
+    y = ct.c_int(0)
+    P = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_double))
+    lib().orc_dp(precision, 1 if mui else 0, dt, P(om), P(rt), P(sg), P(pr), ct.byref(y))
+    return sg, y.value

@@ -6,7 +6,9 @@
 // LoquatSph (src/loquat.h:44-126) can be called one at a time:
 //   * golden dumps of every device array after each stage or step,
 //   * device-timed step loops (CUDA events) of the reference's own step,
-//   * the reference's wall-force probe (src/utilities.cu:643-669).
+//   * the reference's wall-force probe (src/utilities.cu:643-669),
+//   * the reference's own output files (initial save and LoquatSph::Saving,
+//     src/loquat.cu:439-482,533-537) at chosen steps.
 // Nothing here changes the reference's arithmetic: the step sequence is the
 // one of LoquatSph::RunSimulation (src/loquat.cu:511-565) minus file output.
 //
@@ -21,11 +23,17 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
+#include <set>
 #include <string>
 #include <vector>
 
 namespace {
+
+// Arrays a dump writes (empty: all of them).
+std::set<std::string> g_keys;
+bool want_key(const char* k) { return g_keys.empty() || g_keys.count(k) > 0; }
 
 struct DumpWriter {
   std::FILE* f = nullptr;
@@ -52,6 +60,7 @@ struct DumpWriter {
     ++n;
   }
   void dev(const char* name, const void* dptr, int32_t elem, int64_t count) {
+    if (!want_key(name)) return;
     std::vector<char> h((size_t)elem * (size_t)count);
     if (count > 0) checkCudaErrors(cudaMemcpy(h.data(), dptr, h.size(), cudaMemcpyDeviceToHost));
     raw(name, h.data(), elem, count);
@@ -116,7 +125,7 @@ void zero_state(LoquatSph& s) {
 // One step, as RunSimulation's loop body (src/loquat.cu:548-561), with an
 // optional dump after every stage (PredictorSection / CorrectorSection bodies
 // of src/loquat.cu:376-436 spelled out).
-void step_once(LoquatSph& s, const std::string& stage_dir, int step) {
+void step_once(LoquatSph& s, const std::string& stage_dir, int step, std::ofstream* save_to) {
   s.StepCalculation();
   if (stage_dir.empty()) {
     s.PredictorSection();
@@ -160,6 +169,8 @@ void step_once(LoquatSph& s, const std::string& stage_dir, int step) {
     cudaDeviceSynchronize();
     d("c4_corrector");
   }
+  // RunSimulation saves after the corrector section, before time and step advance.
+  if (save_to) s.Saving(*save_to);
   s.time += static_cast<double>(s.par_host->dt);
   s.output_time += static_cast<double>(s.par_host->dt);
   s.step++;
@@ -168,7 +179,10 @@ void step_once(LoquatSph& s, const std::string& stage_dir, int step) {
 void usage() {
   std::fprintf(stderr,
                "usage: ref_driver <project> [--steps N] [--warmup W] [--time] [--dump-dir D]\n"
-               "                  [--dump-steps a,b,c] [--stage-step S] [--wall-force-every K]\n");
+               "                  [--dump-steps a,b,c] [--stage-step S] [--wall-force-every K]\n"
+               "                  [--dump-keys k1,k2] [--save-steps a,b]\n"
+               "  --save-steps: 0 = RunSimulation's initial output; s > 0 = Saving during step s\n"
+               "  (after its corrector section); files go to <project>/ as the reference writes them\n");
   std::exit(2);
 }
 
@@ -180,7 +194,16 @@ int main(int argc, char** argv) {
   int steps = 10, warmup = 0, stage_step = -1, wf_every = 0;
   bool timed = false;
   std::string dump_dir;
-  std::vector<int> dump_steps;
+  std::vector<int> dump_steps, save_steps;
+  auto int_list = [](const std::string& v, std::vector<int>& out) {
+    size_t p0 = 0;
+    while (p0 < v.size()) {
+      size_t p1 = v.find(',', p0);
+      if (p1 == std::string::npos) p1 = v.size();
+      out.push_back(std::stoi(v.substr(p0, p1 - p0)));
+      p0 = p1 + 1;
+    }
+  };
   for (int a = 2; a < argc; ++a) {
     std::string k = argv[a];
     auto next = [&]() -> std::string {
@@ -193,13 +216,15 @@ int main(int argc, char** argv) {
     else if (k == "--dump-dir") dump_dir = next();
     else if (k == "--stage-step") stage_step = std::stoi(next());
     else if (k == "--wall-force-every") wf_every = std::stoi(next());
-    else if (k == "--dump-steps") {
+    else if (k == "--dump-steps") int_list(next(), dump_steps);
+    else if (k == "--save-steps") int_list(next(), save_steps);
+    else if (k == "--dump-keys") {
       std::string v = next();
       size_t p0 = 0;
       while (p0 < v.size()) {
         size_t p1 = v.find(',', p0);
         if (p1 == std::string::npos) p1 = v.size();
-        dump_steps.push_back(std::stoi(v.substr(p0, p1 - p0)));
+        g_keys.insert(v.substr(p0, p1 - p0));
         p0 = p1 + 1;
       }
     } else usage();
@@ -221,6 +246,21 @@ int main(int argc, char** argv) {
   s.grid->PositionFromAbsolute2Relative(s.par_host, s.par_device, s.cellpos, s.pospres);
   s.grid->NeighborSearch(s.par_host, s.par_device, s.cellpos, s.idmassidx);
   s.SortArraysPrimary();
+  auto want_save = [&](int st) {
+    for (int d : save_steps)
+      if (d == st) return true;
+    return false;
+  };
+  std::ofstream history;
+  if (!save_steps.empty()) {
+    std::filesystem::create_directories(project);
+    if (want_save(0)) {  // RunSimulation's output of the initial configuration
+      s.CopyDataFromDeviceToHost();
+      s.io->SaveXml();
+      s.io->SaveParticles();
+    }
+    history.open((project + "/time_history.txt").c_str());
+  }
   s.TimerInitiation();
   checkCudaErrors(cudaDeviceSynchronize());
 
@@ -236,7 +276,7 @@ int main(int argc, char** argv) {
     return false;
   };
 
-  for (int w = 0; w < warmup; ++w) step_once(s, "", s.step);
+  for (int w = 0; w < warmup; ++w) step_once(s, "", s.step, nullptr);
   checkCudaErrors(cudaDeviceSynchronize());
 
   cudaEvent_t e0, e1;
@@ -250,7 +290,7 @@ int main(int argc, char** argv) {
       sd = dump_dir + "/stage";
       std::filesystem::create_directories(sd);
     }
-    step_once(s, sd, st);
+    step_once(s, sd, st, want_save(st + 1) ? &history : nullptr);
     if (!dump_dir.empty()) {
       if (want_dump(s.step)) dump_state(s, dump_dir + "/step_" + std::to_string(s.step) + ".rwd", s.step);
       if (wf_every > 0 && s.step % wf_every == 0)

@@ -47,6 +47,24 @@ void ref_hypo_basic(scalar dt, const scalar* omega4, const scalar* rate6, scalar
   sigma6[0] = s.xx; sigma6[1] = s.yy; sigma6[2] = s.zz; sigma6[3] = s.xy; sigma6[4] = s.xz; sigma6[5] = s.yz;
 }
 
+void ref_dp(scalar dt, const scalar* omega4, const scalar* rate6, scalar* sigma6, scalar* par15, int* yield) {
+  scalar4 om = {omega4[0], omega4[1], omega4[2], omega4[3]};
+  tensor2d d = {rate6[0], rate6[1], rate6[2], rate6[3], rate6[4], rate6[5]};
+  tensor2d s = {sigma6[0], sigma6[1], sigma6[2], sigma6[3], sigma6[4], sigma6[5]};
+  bool yld = false;
+  cuMatModDP(dt, om, d, s, par15, yld);
+  sigma6[0] = s.xx; sigma6[1] = s.yy; sigma6[2] = s.zz; sigma6[3] = s.xy; sigma6[4] = s.xz; sigma6[5] = s.yz;
+  *yield = yld ? 1 : 0;
+}
+
+void ref_mui_dp(scalar dt, const scalar* omega4, const scalar* rate6, scalar* sigma6, scalar* par15) {
+  scalar4 om = {omega4[0], omega4[1], omega4[2], omega4[3]};
+  tensor2d d = {rate6[0], rate6[1], rate6[2], rate6[3], rate6[4], rate6[5]};
+  tensor2d s = {sigma6[0], sigma6[1], sigma6[2], sigma6[3], sigma6[4], sigma6[5]};
+  cuMatModMuIDP(dt, om, d, s, par15);
+  sigma6[0] = s.xx; sigma6[1] = s.yy; sigma6[2] = s.zz; sigma6[3] = s.xy; sigma6[4] = s.xz; sigma6[5] = s.yz;
+}
+
 scalar ref_kernel_w(scalar par, scalar q) { return GetKernel(par, q); }
 scalar ref_kernel_f(scalar par, scalar q) { return GetGradKernel(par, q); }
 int ref_scalar_bytes() { return (int)sizeof(scalar); }

@@ -13,7 +13,7 @@
 //     threads rewrite it, src/particle_interaction.cu:147-166 vs :160-161,:233-235);
 //   * the gather-permute reads every permuted array from a full copy (the reference's
 //     shared cache leaves stale values for tail particles after a deletion,
-//     src/loquat_grid.cu:262-320 with sizes from src/loquat.cu:254-287).
+//     src/loquat_grid.cu:193-251 with sizes from src/loquat.cu:254-287).
 // Compile with -ffp-contract=off so the written evaluation order is the one executed.
 #include <algorithm>
 #include <atomic>
@@ -544,7 +544,7 @@ template <class T> void Sim<T>::init(const rw_case* cs) {
   part_idx.assign(np, 0);
   cell_beg.assign(p.ncell, -1);
   cell_end.assign(p.ncell, -1);
-  // PositionFromAbsolute2Relative, src/loquat_grid.cu:322-330.
+  // PositionFromAbsolute2Relative, src/loquat_grid.cu:253-271.
   const T half_ih = (T)(0.5 * (double)p.i_h);
   const T th = two_h();
   for (int i = 0; i < np; ++i) {
@@ -556,11 +556,11 @@ template <class T> void Sim<T>::init(const rw_case* cs) {
   neighbor_search(0);
 }
 
-// NeighborSearch (src/loquat_grid.cu:140-260) + SortArraysPrimary/All (src/loquat.cu:254-287).
+// NeighborSearch (src/loquat_grid.cu:147-191) + SortArraysPrimary/All (src/loquat.cu:254-287).
 template <class T> void Sim<T>::neighbor_search(int section) {
   Par<T>& p = P;
   const int np = p.np;
-  for (int i = 0; i < np; ++i) {  // cuGetParticleCellIndex, src/loquat_grid.cu:140-164
+  for (int i = 0; i < np; ++i) {  // cuGetParticleCellIndex, src/loquat_grid.cu:71-95
     if (cellpos[i].w == p.ncell_delete_m) {
       part_cel[i] = p.ncell_delete_m;
       part_idx[i] = i;
@@ -573,7 +573,7 @@ template <class T> void Sim<T>::neighbor_search(int section) {
     cellpos[i].w = part_cel[i];
     part_idx[i] = i;
   }
-  // SortParticleByCellIndex: a stable sort of (key, index) (src/loquat_grid.cu:167-182).
+  // SortParticleByCellIndex: a stable sort of (key, index) (src/loquat_grid.cu:98-113).
   std::vector<int> order(np);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return part_cel[a] < part_cel[b]; });
@@ -581,7 +581,7 @@ template <class T> void Sim<T>::neighbor_search(int section) {
   for (int i = 0; i < np; ++i) sk[i] = part_cel[order[i]];
   part_cel = sk;
   part_idx = order;
-  // cuFindBegEndInCell (src/loquat_grid.cu:185-213).
+  // cuFindBegEndInCell (src/loquat_grid.cu:116-144).
   std::fill(cell_beg.begin(), cell_beg.end(), -1);
   std::fill(cell_end.begin(), cell_end.end(), -1);
   for (int i = 0; i < np; ++i) {
@@ -593,7 +593,7 @@ template <class T> void Sim<T>::neighbor_search(int section) {
     }
     if (i == np - 1) cell_end[c] = i + 1;
   }
-  // Deleted-particle accounting (src/loquat_grid.cu:234-259).
+  // Deleted-particle accounting (src/loquat_grid.cu:164-190).
   int beg = cell_beg[p.ncell_delete_m];
   if (beg != -1) {
     int end = cell_end[p.ncell_delete_m];
@@ -603,7 +603,7 @@ template <class T> void Sim<T>::neighbor_search(int section) {
       p.np_delete_m += now;
     }
   }
-  // Gather-permute (src/loquat_grid.cu:262-320), array sets of src/loquat.cu:254-287.
+  // Gather-permute (src/loquat_grid.cu:193-251), array sets of src/loquat.cu:254-287.
   auto perm = [&](auto& v, int n) {
     auto src = v;
     for (int i = 0; i < n; ++i) v[i] = src[order[i]];
@@ -1406,6 +1406,27 @@ int orc_hypo_basic(int precision, double dt, const double* omega4, const double*
     V3<T> om{(T)omega4[0], (T)omega4[1], (T)omega4[2]};
     mat_hypo_basic((T)dt, om, D, sg, mp);
     sigma6[0] = sg.xx; sigma6[1] = sg.yy; sigma6[2] = sg.zz; sigma6[3] = sg.xy; sigma6[4] = sg.xz; sigma6[5] = sg.yz;
+  };
+  if (precision == 8) run(0.0);
+  else run(0.0f);
+  return RW_OK;
+}
+
+// *yield (DP only) receives the reference's yield flag.
+int orc_dp(int precision, int mui, double dt, const double* omega4, const double* rate6, double* sigma6,
+           const double* par15, int* yield) {
+  auto run = [&](auto zero) {
+    using T = decltype(zero);
+    T mp[RW_MATERIAL_SIZE];
+    for (int j = 0; j < RW_MATERIAL_SIZE; ++j) mp[j] = (T)par15[j];
+    S6<T> sg{(T)sigma6[0], (T)sigma6[1], (T)sigma6[2], (T)sigma6[3], (T)sigma6[4], (T)sigma6[5]};
+    S6<T> D{(T)rate6[0], (T)rate6[1], (T)rate6[2], (T)rate6[3], (T)rate6[4], (T)rate6[5]};
+    V3<T> om{(T)omega4[0], (T)omega4[1], (T)omega4[2]};
+    bool yld = false;
+    if (mui) mat_muidp((T)dt, om, D, sg, mp);
+    else mat_dp((T)dt, om, D, sg, mp, yld);
+    sigma6[0] = sg.xx; sigma6[1] = sg.yy; sigma6[2] = sg.zz; sigma6[3] = sg.xy; sigma6[4] = sg.xz; sigma6[5] = sg.yz;
+    if (yield) *yield = yld ? 1 : 0;
   };
   if (precision == 8) run(0.0);
   else run(0.0f);

@@ -90,7 +90,8 @@ class Info(ct.Structure):
         ("time", ct.c_double), ("dt", ct.c_double), ("h", ct.c_double), ("dr", ct.c_double),
         ("n_sorts", ct.c_int32), ("n_list_reuse", ct.c_int32),
         ("n_search_skipped", ct.c_int32), ("n_scan_skipped", ct.c_int32), ("n_build_skipped", ct.c_int32),
-        ("graph_kernels", ct.c_int32), ("search_body_kernels", ct.c_int32),
+        ("graph_kernels", ct.c_int32), ("search_body_kernels", ct.c_int32), ("pad_", ct.c_int32),
+        ("time_max", ct.c_double), ("output_frequency", ct.c_double),
     ]
 
 

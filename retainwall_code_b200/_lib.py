@@ -23,7 +23,7 @@ EXPORTS = [
     "rw_mlp_last_error", "rw_mlp_create", "rw_mlp_destroy", "rw_mlp_get_params", "rw_mlp_set_params",
     "rw_mlp_forward", "rw_mlp_grad", "rw_mlp_add_samples", "rw_mlp_samples", "rw_mlp_clear_samples",
     "rw_mlp_train", "rw_mlp_feature_ranges", "rw_mlp_collect", "rw_set_closure", "rw_closure_stats",
-    "rw_list_stats",
+    "rw_list_stats", "rw_write_case_dat",
 ]
 STAGE_NAMES = ["search_p", "rigid", "adami_p", "corner_p", "interaction_p", "predictor", "search_c", "adami_c",
                "corner_c", "interaction_c", "corrector"]
@@ -69,6 +69,7 @@ def lib() -> ct.CDLL:
     L.rw_cell_sort_noalloc.argtypes = [ct.c_void_p, ct.c_int32, ct.c_int32, ct.c_void_p, ct.c_void_p, ct.c_void_p]
     L.rw_wall_force.argtypes = [P, ct.c_int, ct.c_int, ct.c_void_p, ct.POINTER(ct.c_double)]
     L.rw_save.argtypes = [P, ct.c_char_p]
+    L.rw_write_case_dat.argtypes = [ct.POINTER(_abi.Case), ct.c_char_p]
     L.rw_get_info.argtypes = [P, ct.POINTER(_abi.Info)]
     L.rw_set_option.argtypes = [P, ct.c_int, ct.c_double]
     L.rw_get_array.argtypes = [P, ct.c_int, ct.c_void_p, ct.c_size_t]

@@ -162,6 +162,59 @@ def hypocs_model(phi_c_deg: float, e0: float, rho0: float, *, h_s: float = 2.6e9
     return [f32(v) for v in m]
 
 
+def hypo_basic_model(rho0: float, *, Ei: float = 20.0e6, Vi: float = 0.3, phi_c_deg: float = 35.0,
+                     cohesion: float = 0.0, p_ref: float = 1.0e5) -> List[float]:
+    """HypoBasic slots (``GetMaterial_HypoBasic``, src/GenCase.cu:42-50): Ei, Vi, phi_c
+    [rad], cohesion, p_ref; density clamps 0.8 / 1.2 rho0 in slots 13, 14.  Defaults are
+    the reference generator's HypoBasic material (src/GenCase.cu:380-383)."""
+    m = [0.0] * 15
+    m[0], m[1], m[2], m[3], m[4] = Ei, Vi, math.radians(phi_c_deg), cohesion, p_ref
+    m[13], m[14] = rho0 * 0.8, rho0 * 1.2
+    return [f32(v) for v in m]
+
+
+def _dp_fit(tan_x: float) -> float:
+    """Drucker-Prager coefficient matched to Mohr-Coulomb in plane strain:
+    3 tan x / sqrt(9 + 12 tan^2 x)."""
+    return 3.0 * tan_x / math.sqrt(9.0 + 12.0 * tan_x * tan_x)
+
+
+def dp_model(rho0: float, *, E: float = 1.5e6, V: float = 0.2, phi_deg: float = 25.0, psi_deg: float = 0.0,
+             cohesion: float = 0.0) -> List[float]:
+    """Elastic-perfectly-plastic Drucker-Prager slots (``GetMaterial_DP_EPP``,
+    src/GenCase.cu:16-25): bulk modulus E / 3(1 - 2V), shear modulus E / 2(1 + V), the
+    friction, dilatancy and cohesion coefficients of the plane-strain fit, density clamps
+    in slots 13, 14.  Defaults are the reference generator's DP material
+    (src/GenCase.cu:308-312)."""
+    tp, ts = math.tan(math.radians(phi_deg)), math.tan(math.radians(psi_deg))
+    m = [0.0] * 15
+    m[0] = E / (3.0 * (1.0 - 2.0 * V))
+    m[1] = E / (2.0 * (1.0 + V))
+    m[2], m[3] = _dp_fit(tp), _dp_fit(ts)
+    m[4] = 3.0 * cohesion / math.sqrt(9.0 + 12.0 * tp * tp)
+    m[13], m[14] = rho0 * 0.8, rho0 * 1.2
+    return [f32(v) for v in m]
+
+
+def mui_dp_model(rho0: float, *, E: float = 1.5e6, V: float = 0.3, phi1_deg: float = 20.9, phi2_deg: float = 32.76,
+                 I0: float = 0.279, rho_g: float = 2650.0, d_grain: float = 0.5e-3, lam: float = 0.1) -> List[float]:
+    """mu(I)-enhanced Drucker-Prager slots (``GetMaterial_MuI_DP_EPP``,
+    src/GenCase.cu:27-40): bulk and shear modulus, mu_s = tan phi1, mu_2 = tan phi2, I0,
+    grain density, grain diameter, the rate regularisation lambda [1/s]; density clamps in
+    slots 13, 14.  The defaults are common granular-flow values (mu_s, mu_2, I0 of
+    glass-bead flows); the reference's generator sets none."""
+    m = [0.0] * 15
+    m[0] = E / (3.0 * (1.0 - 2.0 * V))
+    m[1] = E / (2.0 * (1.0 + V))
+    m[2], m[3] = math.tan(math.radians(phi1_deg)), math.tan(math.radians(phi2_deg))
+    m[4], m[5], m[6], m[7] = I0, rho_g, d_grain, lam
+    m[13], m[14] = rho0 * 0.8, rho0 * 1.2
+    return [f32(v) for v in m]
+
+
+MODELS = {"hypo_cs": HYPO_CS, "hypo_basic": HYPO_BASIC, "dp": DP_EPP, "mui_dp": MUI_DP_EPP}
+
+
 def _base_params(dr: float, hdr: float, cs: float, cfl: float, rho0: float, model: List[float]) -> Dict[str, object]:
     p: Dict[str, object] = dict(
         dim=3, n_motion=0, periodbound=0,
@@ -225,7 +278,7 @@ class _Builder:
         return Case(params, codes, f(pospres), f(velrhop), f(idm), f(stress), strain, f(bnorm), motions, name)
 
 
-def _soil(b: _Builder, x0, y0, z0, nx, ny, nz, dr, rng, jitter, rho0, g, K0, model_id=0):
+def _soil(b: _Builder, x0, y0, z0, nx, ny, nz, dr, rng, jitter, rho0, g, K0, model_id=0, model_type=HYPO_CS):
     """Soil lattice with uniform jitter and geostatic stress sigma_zz = rho g depth."""
     ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
     pos = np.stack([x0 + (ix + 0.5) * dr, y0 + (iy + 0.5) * dr, z0 + (iz + 0.5) * dr], -1).reshape(-1, 3)
@@ -238,17 +291,20 @@ def _soil(b: _Builder, x0, y0, z0, nx, ny, nz, dr, rng, jitter, rho0, g, K0, mod
     s[:, 1] = szz * K0
     s[:, 2] = szz
     b.mpos.append(pos)
-    b.mcodes.append(np.tile(np.asarray([6, NONFIX, HYPO_CS, model_id], np.int64), (len(pos), 1)))
+    b.mcodes.append(np.tile(np.asarray([6, NONFIX, model_type, model_id], np.int64), (len(pos), 1)))
     b.mstr.append(s)
 
 
 def column_collapse(nx=24, ny=24, nz=48, dx=0.005, seed=1, phi_c=30.0, e0=0.70, rho0=1850.0,
-                    hdr=1.2, jitter=0.05, cs=60.0, cfl=0.1, runout=4.0, name="column") -> Case:
+                    hdr=1.2, jitter=0.05, cs=60.0, cfl=0.1, runout=4.0, name="column", model="hypo_cs") -> Case:
     """Granular column collapse: soil column in a box whose +x wall is absent at t = 0.
 
     Frictionless (free-slip, normal.w = +1) Adami walls on -x, -y, +y around the column,
     a no-slip floor (normal.w = -1) extending ``runout`` column widths in +x.  Geostatic
     stress with K0 = 1 - sin(phi_c).  dt = cfl h / cs (src/loquat.cu:366-374).
+    ``model`` selects the soil's constitutive law (a key of ``MODELS``): HypoCS with the
+    configuration's parameters (default), or the reference generator's HypoBasic, DP or
+    a mu(I)-DP material.
     """
     rng = np.random.default_rng(seed)
     h = dx * hdr
@@ -257,8 +313,11 @@ def column_collapse(nx=24, ny=24, nz=48, dx=0.005, seed=1, phi_c=30.0, e0=0.70, 
     W, D, H = nx * dx, ny * dx, nz * dx
     x0, y0, z0 = margin + bt, margin + bt + W, margin + bt  # room in -y for lateral spreading
     L = W * (1.0 + runout)
-    model = hypocs_model(phi_c, e0, rho0)
-    p = _base_params(dx, hdr, cs, cfl, rho0, model)
+    if model not in MODELS:
+        raise ValueError(f"unknown model {model!r}")
+    mat = {"hypo_cs": lambda: hypocs_model(phi_c, e0, rho0), "hypo_basic": lambda: hypo_basic_model(rho0),
+           "dp": lambda: dp_model(rho0), "mui_dp": lambda: mui_dp_model(rho0)}[model]()
+    p = _base_params(dx, hdr, cs, cfl, rho0, mat)
     b = _Builder()
     # floor (no slip), wide enough for run-out and lateral spreading
     b.box((x0 - bt, y0 - D - bt, z0 - bt), (x0 + L, y0 + 2 * D + bt, z0), dx, (0, FIX, INT_MIN, INT_MIN), (0, 0, 1, -1))
@@ -267,7 +326,7 @@ def column_collapse(nx=24, ny=24, nz=48, dx=0.005, seed=1, phi_c=30.0, e0=0.70, 
     b.box((x0, y0 - bt, z0), (x0 + W, y0, z0 + H + 2 * h), dx, (2, FIX, INT_MIN, INT_MIN), (0, 1, 0, 1))
     b.box((x0, y0 + D, z0), (x0 + W, y0 + D + bt, z0 + H + 2 * h), dx, (3, FIX, INT_MIN, INT_MIN), (0, -1, 0, 1))
     K0 = 1.0 - math.sin(math.radians(phi_c))
-    _soil(b, x0, y0, z0, nx, ny, nz, dx, rng, jitter, rho0, -9.81, K0)
+    _soil(b, x0, y0, z0, nx, ny, nz, dx, rng, jitter, rho0, -9.81, K0, model_type=MODELS[model])
     p["domain_size_x"] = f32(x0 + L + margin)
     p["domain_size_y"] = f32(y0 + 2 * D + bt + margin)
     p["domain_size_z"] = f32(z0 + H + 2 * h + margin)
@@ -526,13 +585,33 @@ def read_motion(path: str, n_motion: int) -> List[MotionTable]:
     return out
 
 
-def write_case(case: Case, project: str) -> None:
-    """Write ``<project>.xml/.dat[/.motion]`` in the reference layout."""
+def write_dat_native(path: str, case: Case) -> None:
+    """write_dat through the native library (rw_write_case_dat: the same bytes, rows
+    formatted by several host threads); for cases of millions of particles."""
+    import ctypes as ct
+
+    from . import _abi
+    from ._lib import check, lib
+
+    keep: list = []
+    c = _abi.case_struct(case, keep)
+    check(lib().rw_write_case_dat(ct.byref(c), path.encode()), "rw_write_case_dat", None)
+
+
+def write_case(case: Case, project: str, native: Optional[bool] = None) -> None:
+    """Write ``<project>.xml/.dat[/.motion]`` in the reference layout.  ``native``: write
+    the particle file through the native library (default: for cases above 100k
+    particles)."""
     d = os.path.dirname(project)
     if d:
         os.makedirs(d, exist_ok=True)
     write_xml(project + ".xml", case.params)
-    write_dat(project + ".dat", case)
+    if native is None:
+        native = case.np_ > 100_000
+    if native:
+        write_dat_native(project + ".dat", case)
+    else:
+        write_dat(project + ".dat", case)
     if int(case.params.get("n_motion", 0)) > 0:
         write_motion(project + ".motion", case.motions)
 

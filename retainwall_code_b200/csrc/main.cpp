@@ -28,44 +28,32 @@ int main(int argc, char** argv) {
   rw_get_info(ctx, &inf);
   std::printf("LOQUAT-compatible SPH step on device %d: np=%d npb=%d npm=%d ncell=%d dt=%.3e\n", device, inf.np,
               inf.npb, inf.npm, inf.ncell, inf.dt);
-  // The reference reads time-max/output-frequency from the parameter file; they are
-  // re-read here from output_0 of the case through rw_create's parameters.
-  if ((s = rw_save(ctx, project.c_str()))) return fail(ctx, s, "rw_save");
-  double time = inf.time, output_time = 0.0;
+  if ((s = rw_save(ctx, project.c_str()))) return fail(ctx, s, "rw_save");  // initial output
+  // time-max and output-frequency come from the parameter file (src/loquat_io.cu:192-195);
+  // RW_TIME_MAX overrides time-max (short runs).
   const char* tm = std::getenv("RW_TIME_MAX");
-  double time_max = tm ? std::atof(tm) : -1.0;
-  double out_freq = -1.0;
-  {  // time-max / output-frequency from the parameter file (src/loquat_io.cu:192-195)
-    std::FILE* f = std::fopen((project + ".xml").c_str(), "r");
-    if (f) {
-      char line[512];
-      while (std::fgets(line, sizeof line, f)) {
-        std::string l(line);
-        auto val = [&](const char* tag) {
-          size_t a = l.find('>'), b = l.find("</");
-          return std::atof(l.substr(a + 1, b - a - 1).c_str());
-        };
-        if (l.find("<time-max ") != std::string::npos && time_max < 0) time_max = val("time-max");
-        if (l.find("<output-frequency ") != std::string::npos) out_freq = val("output-frequency");
-      }
-      std::fclose(f);
-    }
-  }
-  // Run in chunks of whole steps between saves (src/loquat.cu:548-561).
+  const double time_max = tm ? std::atof(tm) : inf.time_max;
+  const double out_freq = inf.output_frequency, dt = inf.dt;
+  // The reference's loop (src/loquat.cu:548-561), one step per iteration: Saving runs
+  // inside a step when output_time > output-frequency, then time and output_time
+  // advance by dt.  The host counters are advanced the same way to find each save's
+  // step; the steps between saves run as one rw_step call.
+  double time = inf.time, output_time = 0.0;
   while (time < time_max) {
-    int n = 1;
-    if (out_freq > 0) {
-      n = (int)((out_freq - output_time) / inf.dt);
-      if (n < 1) n = 1;
+    int n = 0;
+    bool save = false;
+    while (time < time_max && !save) {
+      ++n;
+      save = output_time > out_freq;
+      if (save) output_time = 0.0;
+      time += dt;
+      output_time += dt;
     }
     if ((s = rw_step(ctx, n))) return fail(ctx, s, "rw_step");
     if ((s = rw_synchronize(ctx))) return fail(ctx, s, "rw_synchronize");
-    time += n * inf.dt;
-    output_time += n * inf.dt;
-    if (out_freq > 0 && output_time > out_freq) {
+    if (save) {
       if ((s = rw_save(ctx, project.c_str()))) return fail(ctx, s, "rw_save");
-      output_time = 0.0;
-      std::printf("Time = %0.5f saved\n", time);
+      std::printf("Time = %0.5f saved\n", time - dt);
     }
   }
   rw_destroy(ctx);

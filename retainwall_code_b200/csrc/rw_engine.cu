@@ -34,6 +34,9 @@ struct Fail : std::runtime_error {
 struct EngineBase {
   std::string err;
   int device = 0;
+  // Bumped whenever an option or the closure changes what a captured step does; a batch
+  // graph captured before the change is rebuilt before its next launch.
+  unsigned generation = 0;
   virtual ~EngineBase() = default;
   virtual void begin_step() = 0;
   virtual void neighbor_search(int section) = 0;
@@ -596,6 +599,7 @@ template <class T> struct Engine final : EngineBase {
       cudaGraphExecDestroy(gexec);
       gexec = nullptr;
     }
+    ++generation;
     if (!net) {
       P.closure = 0;
       cl_net = nullptr;
@@ -899,6 +903,8 @@ template <class T> struct Engine final : EngineBase {
     const bool ix_gates = ix_kernel == 0 && P.np > P.npb;
     o->graph_kernels = kernels_per_step() + (graph_cond ? 2 + (ix_gates ? 4 : 0) : 0);
     o->search_body_kernels = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 2 : 0);
+    o->time_max = cparams.time_max;
+    o->output_frequency = cparams.output_frequency;
   }
 
   // Kept candidate lists: radius 2h + skin; dropped once any particle may have moved
@@ -959,6 +965,7 @@ template <class T> struct Engine final : EngineBase {
       cudaGraphExecDestroy(gexec);
       gexec = nullptr;
     }
+    ++generation;
     return RW_OK;
   }
 
@@ -1183,7 +1190,7 @@ template <class T> struct Engine final : EngineBase {
   }
 
   // Saving (src/loquat.cu:439-482): output_N.xml + particles with the Shepard-smoothed
-  // stress (StressSavingRegularization, src/field_smoothing.cu:316-325) + time history.
+  // stress (StressSavingRegularization, src/field_smoothing.cu:103-111) + time history.
   void save(const char* outdir) override {
     std::string dir = outdir ? outdir : ".";
     ::mkdir(dir.c_str(), 0755);
@@ -1226,7 +1233,9 @@ template <class T> struct Engine final : EngineBase {
     const bool initial = saves++ == 0;
     if (!initial) output_number++;
     const std::string xmlp = dir + "/output_" + std::to_string(output_number) + ".xml";
-    int rc = write_output_xml(xmlp, cparams, P.np, P.npb, d.npm, d.time_d, (double)P.dt, output_number);
+    // The time written is the reference's par_host->time: that of the last step begun
+    // (StepCalculation, src/loquat.cu:366-374), the case's time before any step.
+    int rc = write_output_xml(xmlp, cparams, P.np, P.npb, d.npm, (double)d.time_f, (double)P.dt, output_number);
     if (rc) throw Fail(rc, "cannot write " + xmlp);
     if (P.output_format == 1) rc = write_frame_dat(dir + "/" + std::to_string(output_number) + ".dat", f);
     else rc = write_frame_vtu(dir, output_number, f);
@@ -1240,14 +1249,14 @@ template <class T> struct Engine final : EngineBase {
       std::FILE* fz = std::fopen((dir + "/stress_zz" + std::to_string(output_number) + ".txt").c_str(), "w");
       if (!fz) throw Fail(RW_EIO, "cannot write stress_zz file");
       for (int b = 0; b < nb; ++b)
-        std::fprintf(fz, "%.9g %.9g %.9g %.9g\n", prof[4 * b], prof[4 * b + 1], prof[4 * b + 2], prof[4 * b + 3]);
+        std::fprintf(fz, "%g %g %g %g\n", prof[4 * b], prof[4 * b + 1], prof[4 * b + 2], prof[4 * b + 3]);
       std::fclose(fz);
     }
     double wf[3];
     wall_force(1, 10, nullptr, wf);
     std::FILE* th = std::fopen((dir + "/time_history.txt").c_str(), "a");
     if (!th) throw Fail(RW_EIO, "cannot write time_history.txt");
-    std::fprintf(th, "%.9g %.9g\n", (double)d.time_f, 0.001 * wf[0]);
+    std::fprintf(th, "%g %g\n", (double)d.time_f, 0.001 * wf[0]);  // ostream's default 6 digits
     std::fclose(th);
   }
   void get6_cache(std::vector<T>& o) {
@@ -1266,6 +1275,7 @@ template <class T> struct Engine final : EngineBase {
 // ===================================================================================
 struct Batch {
   std::vector<EngineBase*> engines;
+  std::vector<unsigned> generations;  // the engines' generations when the graph was built
   int device = 0;
   cudaStream_t st = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -1317,7 +1327,20 @@ struct Batch {
     gated = ok;
     return ok;
   }
+  // Rebuilds the graph when an option of some context changed since it was captured.
+  void refresh() {
+    bool stale = !gexec;
+    for (size_t k = 0; k < engines.size(); ++k) stale = stale || engines[k]->generation != generations[k];
+    if (!stale) return;
+    if (gexec) {
+      cudaGraphExecDestroy(gexec);  // freed once launches in flight complete
+      gexec = nullptr;
+    }
+    build();
+  }
   void build() {
+    generations.clear();
+    for (EngineBase* e : engines) generations.push_back(e->generation);
     if (build_forked()) return;
     for (int attempt = 0; attempt < 2 && !gexec; ++attempt) {
       const bool gates = attempt == 0;
@@ -1576,25 +1599,34 @@ rw_status rw_batch_wall_force(rw_batch* b, int mode, int wall_id, const double* 
   return RW_OK;
 }
 
+namespace {
+struct EventPair {  // destroyed on every path out of the timed region
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ~EventPair() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+}  // namespace
+
 rw_status rw_batch_step(rw_batch* b, int nsteps, double* ms) {
   if (!b || nsteps < 0) return RW_EINVAL;
   try {
     RW_CU(cudaSetDevice(b->b.device));
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    b->b.refresh();  // options changed on a context since the capture: capture again
+    EventPair ev;
     if (ms) {
-      RW_CU(cudaEventCreate(&e0));
-      RW_CU(cudaEventCreate(&e1));
-      RW_CU(cudaEventRecord(e0, b->b.st));
+      RW_CU(cudaEventCreate(&ev.e0));
+      RW_CU(cudaEventCreate(&ev.e1));
+      RW_CU(cudaEventRecord(ev.e0, b->b.st));
     }
     for (int k = 0; k < nsteps; ++k) RW_CU(cudaGraphLaunch(b->b.gexec, b->b.st));
     if (ms) {
-      RW_CU(cudaEventRecord(e1, b->b.st));
-      RW_CU(cudaEventSynchronize(e1));
+      RW_CU(cudaEventRecord(ev.e1, b->b.st));
+      RW_CU(cudaEventSynchronize(ev.e1));
       float t = 0.f;
-      RW_CU(cudaEventElapsedTime(&t, e0, e1));
+      RW_CU(cudaEventElapsedTime(&t, ev.e0, ev.e1));
       *ms = t;
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
     }
   } catch (const Fail& f) {
     b->b.err = f.what();

@@ -5,6 +5,7 @@
 #include "rw_io.h"
 
 #include <algorithm>
+#include <charconv>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -12,6 +13,7 @@
 #include <iomanip>
 #include <numeric>
 #include <sstream>
+#include <thread>
 
 namespace rw {
 
@@ -280,7 +282,8 @@ int read_project(const std::string& project, HostCase* hc, std::string* msg) {
   return RW_OK;
 }
 
-// Values are printed like the reference's ofstream (default 6 significant digits).
+// Values are printed like the reference's ofstream (default 6 significant digits), here
+// and in the particle files.
 int write_output_xml(const std::string& path, const rw_case_params& p, int np, int npb, int npm, double time,
                      double dt, int output_number) {
   std::ofstream o(path);
@@ -332,7 +335,6 @@ int write_output_xml(const std::string& path, const rw_case_params& p, int np, i
   t("output-frequency", "scalar", p.output_frequency);
   t("output-number", "int", output_number);
   t("output-format", "int", p.output_format);
-  t("wall-friction-coefficient", "scalar", p.wall_friction);
   o << "</parameters>\n";
   return o ? RW_OK : RW_EIO;
 }
@@ -340,7 +342,6 @@ int write_output_xml(const std::string& path, const rw_case_params& p, int np, i
 int write_frame_dat(const std::string& path, const Frame& f) {
   std::ofstream o(path);
   if (!o) return RW_EIO;
-  o << std::setprecision(9);
   for (int i = 0; i < f.np; ++i) {
     const int32_t* c = &f.codes[4 * i];
     o << c[0] << " " << c[1] << " " << c[2] << " " << c[3];
@@ -369,7 +370,6 @@ int write_frame_vtu(const std::string& dir, int output_number, const Frame& f) {
     const size_t n = e - s;
     std::ofstream o(dir + "/" + std::to_string(id) + "_" + std::to_string(output_number) + ".vtu");
     if (!o) return RW_EIO;
-    o << std::setprecision(9);
     o << "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\" "
          "compressor=\"vtkZLibDataCompressor\">\n  <UnstructuredGrid GhostLevel=\"0\">\n";
     o << "    <Piece NumberOfPoints=\"" << n << "\" NumberOfCells=\"" << n << "\" Name=\"" << id << "\">\n      <PointData>\n";
@@ -418,4 +418,67 @@ int write_frame_vtu(const std::string& dir, int output_number, const Frame& f) {
   return RW_OK;
 }
 
+// SaveDatFile layout (src/GenCase.cu:70-116): codes(4) pos(4) velrhop(4) id mass w
+// stress(6) strain(6), plus the normal(4) on boundary rows; integers in decimal, reals
+// as printf's %.9g (enough digits to give a float back exactly).  Rows are formatted by
+// several host threads into separate buffers and written in order.
+int write_case_dat(const rw_case* c, const std::string& path) {
+  const int np = c->params.np, npb = c->params.npb;
+  if (np < 0 || npb < 0 || npb > np) return RW_EINVAL;
+  const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::string> part(nth);
+  auto rows = [&](int t) {
+    const long lo = (long)np * t / nth, hi = (long)np * (t + 1) / nth;
+    std::string& o = part[t];
+    o.reserve((size_t)(hi - lo) * 330);
+    char buf[64];
+    auto put_i = [&](int32_t v) {
+      auto r = std::to_chars(buf, buf + sizeof(buf), v);
+      o.append(buf, r.ptr);
+    };
+    auto put_d = [&](double v) {
+      o.push_back(' ');
+      auto r = std::to_chars(buf, buf + sizeof(buf), v, std::chars_format::general, 9);
+      o.append(buf, r.ptr);
+    };
+    for (long i = lo; i < hi; ++i) {
+      const int32_t* cc = c->codes + 4 * i;
+      put_i(cc[0]);
+      for (int k = 1; k < 4; ++k) {
+        o.push_back(' ');
+        put_i(cc[k]);
+      }
+      for (int k = 0; k < 4; ++k) put_d(c->pospres[4 * i + k]);
+      for (int k = 0; k < 4; ++k) put_d(c->velrhop[4 * i + k]);
+      put_d(c->idmassidx[4 * i + 0]);
+      put_d(c->idmassidx[4 * i + 1]);
+      put_d(c->idmassidx[4 * i + 3]);
+      for (int k = 0; k < 6; ++k) put_d(c->stress[6 * i + k]);
+      for (int k = 0; k < 6; ++k) put_d(c->strain[6 * i + k]);
+      if (i < npb)
+        for (int k = 0; k < 4; ++k) put_d(c->normal[4 * i + k]);
+      o.push_back('\n');
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nth; ++t) th.emplace_back(rows, t);
+  rows(0);
+  for (auto& x : th) x.join();
+  std::FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) return RW_EIO;
+  bool ok = true;
+  for (auto& s : part) ok = ok && std::fwrite(s.data(), 1, s.size(), f) == s.size();
+  ok = std::fclose(f) == 0 && ok;
+  return ok ? RW_OK : RW_EIO;
+}
+
 }  // namespace rw
+
+extern "C" rw_status rw_write_case_dat(const rw_case* c, const char* path) {
+  if (!c || !path) return RW_EINVAL;
+  try {
+    return rw::write_case_dat(c, path);
+  } catch (...) {
+    return RW_ENOMEM;
+  }
+}

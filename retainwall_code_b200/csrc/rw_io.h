@@ -39,4 +39,7 @@ int write_frame_dat(const std::string& path, const Frame& f);
 // LoquatIo::SaveParticles format 2 (src/loquat_io.cu:470-680): one <id>_<n>.vtu per block id.
 int write_frame_vtu(const std::string& dir, int output_number, const Frame& f);
 
+// SaveDatFile layout of a case (src/GenCase.cu:70-116).
+int write_case_dat(const rw_case* c, const std::string& path);
+
 }  // namespace rw

@@ -187,7 +187,7 @@ struct RawCase {
 };
 
 // One particle of LoadParticles' conversion with the absolute -> in-cell split of
-// src/loquat_grid.cu:322-330: cell = trunc(x / 2h), in-cell position = x - cell * 2h.
+// src/loquat_grid.cu:253-271: cell = trunc(x / 2h), in-cell position = x - cell * 2h.
 // Every product and difference is rounded on its own (no contraction), so the result
 // is the host arithmetic of the reference's loader, bit for bit.
 template <class T> __global__ void k_ingest(const Params<T> P, DevState<T> S, RawCase R, T half_ih) {
@@ -219,10 +219,10 @@ template <class T> __global__ void k_ingest(const Params<T> P, DevState<T> S, Ra
 
 // ---------------------------------------------------------------------------------
 // Cell list: keys, stable radix sort, ranges, gather-permute
-// (src/loquat_grid.cu:140-320, src/loquat.cu:254-287).
+// (src/loquat_grid.cu:71-261, src/loquat.cu:254-287).
 // ---------------------------------------------------------------------------------
 
-// cuGetParticleCellIndex (src/loquat_grid.cu:140-164).  A live particle whose cell is
+// cuGetParticleCellIndex (src/loquat_grid.cu:71-95).  A live particle whose cell is
 // outside the grid would make the reference write out of bounds; here its key is
 // clamped into the grid and RW_DERR_CELL_RANGE is raised.
 template <class T> __global__ void k_keys(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
@@ -375,7 +375,7 @@ static __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const int* k
   }
 }
 
-// cuFindBegEndInCell (src/loquat_grid.cu:185-213): [beg, end) of every occupied cell.
+// cuFindBegEndInCell (src/loquat_grid.cu:116-144): [beg, end) of every occupied cell.
 template <class T> __global__ void k_ranges(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.np || !dyn->cells_dirty) return;
@@ -386,7 +386,7 @@ template <class T> __global__ void k_ranges(const Params<T> P, DevState<T> S, co
   if (i == P.np - 1 || K[i + 1] != k) r[2 * k + 1] = i + 1;
 }
 
-// Deleted-particle accounting (src/loquat_grid.cu:234-254), on the device.
+// Deleted-particle accounting (src/loquat_grid.cu:164-190), on the device.
 template <class T> __global__ void k_count(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
   if (!dyn->cells_dirty) return;
   int2 d = S.range[P.ncell_delete_m];
@@ -2241,6 +2241,8 @@ __global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevSta
       atomicMax(reinterpret_cast<unsigned long long*>(&stats[3]), (unsigned long long)__double_as_longlong((double)sx));
     }
   }
+  __syncthreads();
+  mlp::drain_after_timeout(&sm.bar, sm.err, phase);
   mlp::block_teardown(sm.tmem, 64);
   if (tid == 0 && sm.err) atomicOr(&dyn->err, 16u);
 }

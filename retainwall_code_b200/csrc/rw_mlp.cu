@@ -115,6 +115,8 @@ __global__ void __launch_bounds__(TILE) k_forward(Net net, const float* __restri
 #pragma unroll
       for (int o = 0; o < OUT; ++o) Y[(size_t)s * OUT + o] = out[o];
   }
+  __syncthreads();
+  drain_after_timeout(&sm.bar, sm.err, phase);
   block_teardown(sm.tmem, 64);
   if (threadIdx.x == 0 && sm.err) atomicExch(err, 1);
 }
@@ -205,13 +207,17 @@ __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restr
   const uint32_t tl = sm.tmem + lane_off;
   uint32_t phase = 0;
   float lsum = 0.0f;
+  // After a timed-out wait (sm.err, seen by every thread after the next barrier) no
+  // MMA is issued and none is waited for; the tile loop ends at the next tile.
   auto wait_mma = [&]() {
+    if (sm.err) return;
     if (!tc::mbar_wait(&sm.bar, phase & 1u)) sm.err = 1;
     ++phase;
     tc::fence_after_sync();
   };
   for (int tile = blockIdx.x; tile * TILE < n; tile += gridDim.x) {
     __syncthreads();  // the previous tile's first-layer weight gradient has read sm.x
+    if (sm.err) break;
     const int r = tile * TILE + tid;
     const bool valid = r < n;
     const long long s = valid ? shuffled(first + r, n_all, sa, sc) : 0;
@@ -226,7 +232,7 @@ __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restr
     for (int l = 0; l <= NHID; ++l) {
       tc::fence_smem_to_async();
       __syncthreads();
-      if (tid == 0) {
+      if (tid == 0 && !sm.err) {
         tc::fence_after_sync();
         if (l == 0) issue_layer(sm.x, IN, sm.fw + FW1, HID, sm.tmem);
         else if (l < NHID)
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restr
     }
     tc::fence_smem_to_async();
     __syncthreads();
-    if (tid == 0) {  // dH4 = G5 W5
+    if (tid == 0 && !sm.err) {  // dH4 = G5 W5
       tc::fence_after_sync();
       issue_layer(sm.g5, OUTP, sm.bw + BW5, HID, sm.tmem + TCOL_DH);
       tc::mma_commit(&sm.bar);
@@ -291,7 +297,7 @@ __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restr
       tc::fence_before_sync();
       tc::fence_smem_to_async();
       __syncthreads();
-      if (l > 1 && tid == 0) {  // dH(l-1) = G(l) W(l)
+      if (l > 1 && tid == 0 && !sm.err) {  // dH(l-1) = G(l) W(l)
         tc::fence_after_sync();
         issue_layer(sm.g, HID, sm.bw + (l == 2 ? BW2 : l == 3 ? BW3 : BW4), HID, sm.tmem + TCOL_DH);
         tc::mma_commit(&sm.bar);
@@ -308,6 +314,7 @@ __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restr
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
   if ((tid & 31) == 0) atomicAdd(loss, (double)lsum);
+  drain_after_timeout(&sm.bar, sm.err, phase);
   block_teardown(sm.tmem, TRAIN_TMEM_COLS);
   if (tid == 0 && sm.err) atomicExch(err, 1);
 }

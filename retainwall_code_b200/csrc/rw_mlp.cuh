@@ -136,7 +136,9 @@ __device__ __forceinline__ void issue_layer(const unsigned char* a_tile, int K, 
 // Forward pass of the tile already in sm.x (rows = threads of this 128-thread block).
 // TMEM: columns [tcol, tcol + 64) of the allocation at sm.tmem.  Each thread receives
 // its row's six outputs (biases added).  phase counts the mbarrier phases used so far.
-// A wait that times out sets sm.err (the outputs are then meaningless).
+// A wait that times out sets sm.err: the outputs are then meaningless, and this and
+// every later call issue no further MMAs (all threads see sm.err after the barrier at
+// the top of a layer and return together).
 __device__ __forceinline__ void forward_tile(FwdSmem& sm, int tcol, uint32_t& phase, float* out) {
   const int tid = threadIdx.x, warp = tid >> 5;
   const uint32_t tbase = sm.tmem + (uint32_t)tcol;
@@ -144,6 +146,7 @@ __device__ __forceinline__ void forward_tile(FwdSmem& sm, int tcol, uint32_t& ph
   for (int l = 0; l <= NHID; ++l) {
     tc::fence_smem_to_async();
     __syncthreads();
+    if (sm.err) return;
     if (tid == 0) {
       tc::fence_after_sync();
       if (l == 0) issue_layer(sm.x, IN, sm.fw + FW1, HID, tbase);
@@ -188,6 +191,11 @@ __device__ __forceinline__ void block_setup(uint64_t* bar, uint32_t* tmem_slot, 
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
+}
+// After a timed-out wait (err set), the MMAs of the phase that timed out (phase - 1)
+// may still be running: one more bounded wait for it before the TMEM is released.
+__device__ __forceinline__ void drain_after_timeout(uint64_t* bar, int err, uint32_t phase) {
+  if (err && threadIdx.x == 0 && phase > 0) tc::mbar_wait(bar, (phase - 1u) & 1u);
 }
 __device__ __forceinline__ void block_teardown(uint32_t tmem, uint32_t ncols) {
   tc::fence_before_sync();

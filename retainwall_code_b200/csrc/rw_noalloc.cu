@@ -18,7 +18,8 @@ namespace {
 constexpr int kMaxKeys = RW_NOALLOC_MAX_KEYS;
 constexpr int kMaxTiles = (kMaxKeys + rw::RS_TILE - 1) / rw::RS_TILE;
 
-// Scratch: ping-pong keys/values, per-tile digit counts, digit totals, sort flag.
+// Scratch: ping-pong keys/values, per-tile digit counts, digit totals, sort flag:
+// 2 x 2^20 + 256 x 512 + 257 ints = 8,913,924 bytes (8.9 MB, 8.5 MiB).
 struct Scratch {
   int tk[kMaxKeys];
   int tv[kMaxKeys];
@@ -81,7 +82,8 @@ extern "C" rw_status rw_cell_sort_noalloc(const int32_t* d_keys, int32_t n, int3
     const bool to_out = ((passes - 1 - p) % 2) == 0;
     int* ko = to_out ? d_sorted_keys : s->tk;
     int* vo = to_out ? d_perm : s->tv;
-    if (p == 0 && to_out) {  // single pass: values must not be read and written in place
+    if (p == 0 && to_out) {  // odd pass count (1 or 3): pass 0 writes the caller's outputs, so
+                             // its values come from an identity in the scratch (not in place)
       k_fill_iota<<<(n + 255) / 256, 256, 0, st>>>(s->tv, n);
       vin = s->tv;
     }

@@ -74,7 +74,7 @@ template <class T> struct Dyn {
   double time_d;             // host-side `time` of RunSimulation, accumulated in double
   T time_f;                  // par.time (scalar copy of time_d, StepCalculation)
   T pad0_;
-  int npm, np_delete_m;      // live / deleted material counts (src/loquat_grid.cu:234-249)
+  int npm, np_delete_m;      // live / deleted material counts (src/loquat_grid.cu:164-181)
   int cur_main, cur_nrm, cur_ini;  // which ping-pong buffer holds each permuted group
   int need_sort;             // 1 when the new cell keys are not already in order
   unsigned err;              // RW_DERR_* bits

@@ -206,27 +206,30 @@ class LoquatSph:
     # -- RunSimulation ---------------------------------------------------------------------
     def run_simulation(self, outdir: Optional[str] = None, time_max: Optional[float] = None,
                        output_frequency: Optional[float] = None) -> None:
-        """The reference's main loop (src/loquat.cu:533-561): initial save, then steps with a
-        save whenever the accumulated output time exceeds output-frequency."""
-        from . import cases
-
-        params = cases.read_xml(self.project + ".xml") if self.project else {}
-        tmax = float(time_max if time_max is not None else params.get("time_max", 0.0))
-        freq = float(output_frequency if output_frequency is not None else params.get("output_frequency", 0.0))
+        """The reference's main loop (src/loquat.cu:533-561): the initial output, then
+        steps, with Saving inside the step in which output_time exceeds output-frequency
+        (time-max and output-frequency default to the parameter file's).  The steps
+        between two saves run as one captured-graph call."""
+        inf = self.info()
+        tmax = float(inf.time_max if time_max is None else time_max)
+        freq = float(inf.output_frequency if output_frequency is None else output_frequency)
         out = outdir or self.project or "."
         os.makedirs(out, exist_ok=True)
         self.save(out)
-        inf = self.info()
         t, ot, dt = inf.time, 0.0, inf.dt
         while t < tmax:
-            n = max(1, int((freq - ot) / dt)) if freq > 0 else max(1, int((tmax - t) / dt))
+            n, save = 0, False
+            while t < tmax and not save:
+                n += 1
+                save = ot > freq
+                if save:
+                    ot = 0.0
+                t += dt
+                ot += dt
             self.step(n)
             self.synchronize()
-            t += n * dt
-            ot += n * dt
-            if freq > 0 and ot > freq:
+            if save:
                 self.save(out)
-                ot = 0.0
 
 
 class Batch:

@@ -60,3 +60,27 @@ def test_roundtrip_files(tmp_path):
     assert np.float32(r.params[C.WALL_FRICTION_TAG]) == np.float32(c.params[C.WALL_FRICTION_TAG])
     m = r.motions[0]
     assert m.is_rotation and not m.is_translation and m.rotat_vel[1] == np.float32(-0.005)
+
+
+def test_native_dat_writer_matches_python(tmp_path):
+    """rw_write_case_dat (native, threaded) writes the same bytes as write_dat, on a
+    wall case (boundary rows with normals) and a case without boundary particles."""
+    import filecmp
+
+    import numpy as np
+
+    from retainwall_code_b200 import cases as C
+
+    wall = C.retaining_wall(nx=12, ny=6, nz=8, dx=0.005, mode="rotation")
+    b = C._Builder()
+    C._soil(b, 0.05, 0.05, 0.05, 3, 3, 3, 0.005, np.random.default_rng(3), 0.05, 1850.0, -9.81, 0.5)
+    p = C._base_params(0.005, 1.2, 60.0, 0.1, 1850.0, C.hypocs_model(30.0, 0.7, 1850.0))
+    p["domain_size_x"] = p["domain_size_y"] = p["domain_size_z"] = 0.15
+    free = b.case(p, [], "free", 1850.0, C.f32(1850.0 * 0.005 ** 3))
+    for k, c in enumerate((wall, free)):
+        a, n = str(tmp_path / f"py{k}"), str(tmp_path / f"nat{k}")
+        C.write_case(c, a, native=False)
+        C.write_case(c, n, native=True)
+        assert filecmp.cmp(a + ".dat", n + ".dat", shallow=False)
+        r = C.read_case(n)
+        np.testing.assert_array_equal(r.pospres.astype(np.float32), c.pospres.astype(np.float32))

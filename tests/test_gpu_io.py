@@ -74,7 +74,7 @@ def test_save_dat_format_roundtrips(tmp_path):
     assert len(rows) == case.np_
     assert len(rows[0].split()) == 31 and len(rows[-1].split()) == 27
     pos = np.array([list(map(float, r.split()[4:7])) for r in rows])
-    np.testing.assert_allclose(pos, s.get("pos_abs")[:, :3], rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(pos, s.get("pos_abs")[:, :3], rtol=5e-6, atol=1e-9)  # 6 significant digits
 
 
 def test_cli_runs_project(tmp_path):
@@ -94,7 +94,7 @@ def test_cli_runs_project(tmp_path):
 
 def test_case_ingest_matches_host_conversion():
     """rw_create_from_case copies the caller's double arrays as they are and converts them
-    on the device (LoadParticles' absolute -> in-cell split, src/loquat_grid.cu:322-330).
+    on the device (LoadParticles' absolute -> in-cell split, src/loquat_grid.cu:253-271).
     The state after creation equals the same conversion done on the host in float32,
     bit for bit, row by row (rows are matched through the original index that the
     loader keeps in idmassidx[:, 2], since creation also sorts by cell)."""

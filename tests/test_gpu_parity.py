@@ -260,6 +260,33 @@ def test_batch_equals_individual_runs():
     b.close()
 
 
+def test_batch_sees_options_set_after_creation():
+    """An option set on a context after rw_batch_create (here the wall friction and the
+    list skin) takes effect at the next batch step: the batch equals runs stepped alone
+    with the same option changes at the same step."""
+    from retainwall_code_b200 import Batch, _abi, cases as C
+
+    cs = [C.retaining_wall(nx=14, ny=6, nz=10, dx=0.005, seed=s, mode=m) for s, m in ((1, "active"), (2, "passive"))]
+    together = [LoquatSph(case=c) for c in cs]
+    b = Batch(together)
+    b.step(2)
+    together[0].set_option(_abi.OPT_WALL_FRICTION, 0.1)
+    together[1].set_option(_abi.OPT_LIST_SKIN, 0.0)
+    b.step(3)
+    b.synchronize()
+    for k, c in enumerate(cs):
+        alone = LoquatSph(case=c)
+        alone.step(2)
+        alone.set_option(*((_abi.OPT_WALL_FRICTION, 0.1) if k == 0 else (_abi.OPT_LIST_SKIN, 0.0)))
+        alone.step(3)
+        for key in ("cellpos", "pospres", "velrhop", "str", "contact_mag"):
+            np.testing.assert_array_equal(together[k].get(key), alone.get(key), err_msg=f"case {k} {key}")
+    plain = LoquatSph(case=cs[0])
+    plain.step(5)
+    assert not np.array_equal(plain.get("contact_mag"), together[0].get("contact_mag"))  # the friction acted
+    b.close()
+
+
 def test_autotune_picks_a_kernel():
     from retainwall_code_b200 import cases as C
 

@@ -1,0 +1,185 @@
+"""Branches of the step that the mini-case fixtures do not reach, each checked on the GPU
+against the CPU oracle and against the unmodified reference CUDA build run live:
+
+* the Shepard stress filter (src/field_smoothing.cu:26-101), applied every
+  ``stress-shepard-filter`` steps by PredictorSection (src/loquat.cu:392);
+* the other constitutive models of the dispatch (src/predictor_corrector.cu:72-75,
+  169-172): HypoBasic (src/constitutive_model.h:136-202), Drucker-Prager (:38-84) and
+  mu(I)-DP (:90-130);
+* a wall rotating about its toe and a wall translating into the soil (passive): the
+  rotation table of RigidBodyUpdate (src/adami_boundary.cu:175-203) and the Rodrigues
+  update of positions and normals in cuCorrectorBound
+  (src/predictor_corrector.cu:109-137).  The wall speeds are raised (2 rad/s, 0.2 m/s)
+  so that 100 steps move the wall by a measurable amount; the code path is the one of
+  the configured speeds.
+
+Bars as in tests/test_gpu_parity.py: integer work bit-exact, 1e-5 relative L2 where no
+contact wall is near, 1e-4 over the whole state next to a contact wall."""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from retainwall_code_b200 import LoquatSph, cases as C
+from tests._refrun import dumps, run_reference
+from tests._util import far_from_contact, golden, load_state, rel
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("part_idx", "cell_beg", "cell_end", "cellpos", "pospres", "velrhop", "str", "contact_var", "normal_m",
+        "contact_mag")
+
+
+def _ref_trajectory(tmp_path, case, prec, steps, dump_steps, name):
+    proj = str(tmp_path / name)
+    C.write_case(case, proj)
+    dd = str(tmp_path / (name + "_dump"))
+    run_reference(proj, prec, steps, dump_dir=dd, dump_steps=dump_steps, keys=KEYS)
+    return proj, dd
+
+
+def _column(model="hypo_cs", shepard=0):
+    c = C.column_collapse(nx=8, ny=8, nz=16, runout=1.0, name="col", model=model)
+    c.params["stress_shepard_filter"] = shepard
+    return c
+
+
+@pytest.mark.parametrize("model", ["hypo_basic", "dp", "mui_dp"])
+def test_constitutive_model_vs_reference_and_oracle(tmp_path, model):
+    case = _column(model)
+    proj, dd = _ref_trajectory(tmp_path, case, 4, 100, (10, 100), model)
+    sim = LoquatSph(proj)
+    orc = Oracle(C.read_case(proj), 4)
+    report = []
+    done = 0
+    for st in (10, 100):
+        sim.step(st - done)
+        orc.step(st - done)
+        done = st
+        g = dumps(dd, f"step_{st}.rwd", 4)
+        for k in ("cellpos", "part_idx", "cell_beg", "cell_end"):
+            if not np.array_equal(sim.get(k), g[k]):
+                report.append(f"step {st} {k} differs from the reference")
+        np.testing.assert_array_equal(sim.get("cellpos"), orc.get("cellpos"))
+        for k in ("pospres", "velrhop", "str"):
+            a = sim.get(k)
+            for who, b in (("reference", g[k]), ("oracle", orc.get(k))):
+                r = rel(a, b)
+                if not r < 1e-5:
+                    report.append(f"step {st} {k} vs {who}: {r:.2e}")
+        print(f"{model} step {st}: str vs reference {rel(sim.get('str'), g['str']):.2e}, "
+              f"vs oracle {rel(sim.get('str'), orc.get('str')):.2e}")
+    assert sim.info().device_err == 0
+    assert not report, "\n".join(report)
+
+
+def test_constitutive_models_fp64_vs_oracle():
+    """The three models in double against the oracle in double over 50 steps."""
+    for model in ("hypo_basic", "dp", "mui_dp"):
+        case = _column(model)
+        s = LoquatSph(case=case, precision=8)
+        o = Oracle(case, 8)
+        s.step(50)
+        o.step(50)
+        np.testing.assert_array_equal(s.get("cellpos"), o.get("cellpos"))
+        for k in ("pos_abs", "velrhop", "str"):
+            assert rel(s.get(k), o.get(k)) < 1e-9, (model, k, rel(s.get(k), o.get(k)))
+
+
+def test_shepard_stage_matches_oracle():
+    """One Shepard filter stage (rw_shepard_filter) from the reference's state after
+    step 1 of the column fixture, against the oracle's restatement of
+    cuStressRegularizationShepard + the copy back (src/field_smoothing.cu:26-101)."""
+    g = golden("col_mini")
+    case = _column()
+    s = LoquatSph(case=case)
+    o = Oracle(case, 4)
+    load_state(s, g)
+    load_state(o, g)
+    for st in ("begin_step", "neighbor_search_p"):
+        {"begin_step": s.step_calculation, "neighbor_search_p": lambda: s.neighbor_search(0)}[st]()
+        o.stage(st)
+    before = s.get("str")
+    s.stress_regularization()
+    o.stage("shepard")
+    after = s.get("str")
+    assert rel(after, before) > 1e-6  # the filter changed the stress
+    np.testing.assert_array_equal(after[:case.npb], before[:case.npb])  # boundary rows untouched
+    assert rel(after, o.get("str")) < 1e-6, rel(after, o.get("str"))
+
+
+@pytest.mark.parametrize("every", [1, 5])
+def test_shepard_filter_in_the_step_vs_reference_and_oracle(tmp_path, every):
+    """Whole steps with the filter on (every step / every 5th step) against the
+    reference and the oracle: the captured step applies it on the same steps."""
+    case = _column(shepard=every)
+    proj, dd = _ref_trajectory(tmp_path, case, 4, 20, (4, 5, 6, 20), f"shep{every}")
+    sim = LoquatSph(proj)
+    orc = Oracle(C.read_case(proj), 4)
+    plain = LoquatSph(case=_column(shepard=0))  # without the filter, to see that it acted
+    done = 0
+    report = []
+    for st in (4, 5, 6, 20):
+        sim.step(st - done)
+        orc.step(st - done)
+        plain.step(st - done)
+        done = st
+        g = dumps(dd, f"step_{st}.rwd", 4)
+        np.testing.assert_array_equal(sim.get("cellpos"), g["cellpos"])
+        for k in ("pospres", "velrhop", "str"):
+            a = sim.get(k)
+            for who, b in (("reference", g[k]), ("oracle", orc.get(k))):
+                r = rel(a, b)
+                if not r < 1e-5:
+                    report.append(f"step {st} {k} vs {who}: {r:.2e}")
+    assert rel(sim.get("str"), plain.get("str")) > 1e-5, "the filter left no trace"
+    assert not report, "\n".join(report)
+
+
+@pytest.mark.parametrize("mode", ["rotation", "passive"])
+def test_moving_wall_vs_reference_and_oracle(tmp_path, mode):
+    case = C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005, wall_friction=C.REFERENCE_WALL_FRICTION, mode=mode,
+                            wall_speed=0.2, rot_speed=2.0, name=mode)
+    proj, dd = _ref_trajectory(tmp_path, case, 4, 100, (10, 100), mode)
+    sim = LoquatSph(proj)
+    orc = Oracle(C.read_case(proj), 4)
+    report = []
+    done = 0
+    for st in (10, 100):
+        sim.step(st - done)
+        orc.step(st - done)
+        done = st
+        g = dumps(dd, f"step_{st}.rwd", 4)
+        np.testing.assert_array_equal(sim.get("cellpos"), g["cellpos"])
+        np.testing.assert_array_equal(sim.get("cellpos"), orc.get("cellpos"))
+        # rows are in cell order, the same in all three (permutations are bit-exact)
+        wall = (np.arange(case.np_) < case.npb) & (sim.get("codes")[:, 0] >= 10)
+        # the wall: absolute positions and normals, vs the reference and the oracle
+        two_h = 2.0 * case.params["dr"] * case.params["hdr"]
+        ref_abs = g["pospres"][:, :3].astype(np.float64) + g["cellpos"][:, :3] * np.float32(two_h)
+        ours = sim.get("pos_abs")[:, :3]
+        for who, b in (("reference", ref_abs), ("oracle", orc.get("pos_abs")[:, :3])):
+            r = rel(ours[wall], b[wall])
+            if not r < 1e-6:
+                report.append(f"step {st} wall positions vs {who}: {r:.2e}")
+        n_ours = sim.get("normal_m")[wall[:case.npb]]
+        for who, b in (("reference", g["normal_m"]), ("oracle", orc.get("normal_m"))):
+            r = rel(n_ours[:, :3], b[wall[:case.npb], :3])
+            if not r < 1e-6:
+                report.append(f"step {st} wall normals vs {who}: {r:.2e}")
+        # the soil: 1e-5 beyond 2h of the contact zone, 1e-4 over the whole state
+        far = far_from_contact(case, g["cellpos"], g["pospres"], g["contact_var"])
+        for k in ("pospres", "velrhop", "str"):
+            a = sim.get(k)
+            for who, b in (("reference", g[k]), ("oracle", orc.get(k))):
+                if not rel(a[far], b[far]) < 1e-5:
+                    report.append(f"step {st} {k} vs {who} beyond 2h of contact: {rel(a[far], b[far]):.2e}")
+                if not rel(a, b) < 1e-4:
+                    report.append(f"step {st} {k} vs {who}: {rel(a, b):.2e}")
+    orig = sim.get("idmassidx")[:, 2].astype(np.int64)
+    moved = np.abs(sim.get("pos_abs")[wall, :3] - case.pospres[orig[wall], :3]).max()
+    assert moved > 0.05 * case.params["dr"], moved
+    if mode == "rotation":
+        n = sim.get("normal_m")[wall[:case.npb], :3]
+        assert np.abs(n[:, 2]).max() > 1e-3  # the normals turned with the wall
+    assert sim.info().device_err == 0
+    assert not report, "\n".join(report)

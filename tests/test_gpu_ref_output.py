@@ -1,0 +1,123 @@
+"""The output files of rw_save against the reference's own writer, for the same case run
+on the same GPU: RunSimulation's initial output and one Saving after 20 steps
+(src/loquat.cu:439-482,533-537), in both particle formats.
+
+Compared, file by file:
+* the file names (output_N.xml, N.dat or <id>_N.vtu, stress_zzN.txt, time_history.txt);
+  the reference names its .dat files with a trailing newline character
+  (src/loquat_io.cu:434), which is stripped before the comparison;
+* output_N.xml: the same tags in the same order with the same text
+  (LoquatIo::SaveXml, src/loquat_io.cu:315-399);
+* the particle files (LoquatIo::SaveParticles, src/loquat_io.cu:430-680): the same
+  arrays, names, component counts and row order; integer-valued arrays equal; real
+  arrays within 1e-5 relative L2 in the initial output and 1e-4 after 20 steps (the
+  bar of the step's own parity tests next to a contact wall);
+* time_history.txt (GetValuesAtPoint, src/utilities.cu:578-669): the same times, the
+  wall force within 0.5 %;
+* stress_zzN.txt (GetValuesAlongLine, src/utilities.cu:266-367): the same depths, the
+  profile within 1e-3 relative L2."""
+import os
+import re
+import xml.etree.ElementTree as ET
+
+import numpy as np
+import pytest
+
+from retainwall_code_b200 import LoquatSph, cases as C
+from tests._refrun import run_reference
+from tests._util import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _files(d):
+    return {f.rstrip("\n"): os.path.join(d, f) for f in os.listdir(d)}
+
+
+def _vtu_arrays(path):
+    root = ET.parse(path).getroot()
+    piece = root.find("UnstructuredGrid/Piece")
+    out = [("NumberOfPoints", piece.get("NumberOfPoints"), None)]
+    for da in root.iter("DataArray"):
+        vals = np.array(da.text.split(), np.float64) if da.text and da.text.strip() else np.zeros(0)
+        out.append((da.get("Name"), da.get("NumberOfComponents"), vals))
+    return out
+
+
+def _numeric_rows(path):
+    with open(path) as f:
+        return [np.array(l.split(), np.float64) for l in f if l.strip()]
+
+
+def _compare_arrays(name, a, b, tol, report):
+    if a.shape != b.shape:
+        report.append(f"{name}: shape {a.shape} vs {b.shape}")
+        return
+    if np.array_equal(a, np.round(a)) and np.array_equal(b, np.round(b)):
+        if not np.array_equal(a, b):
+            report.append(f"{name}: integer values differ in {int(np.sum(a != b))} places")
+        return
+    r = rel(a, b)
+    if not r < tol:
+        report.append(f"{name}: relative L2 {r:.2e} >= {tol:g}")
+
+
+@pytest.mark.parametrize("fmt", [2, 1], ids=["vtu", "dat"])
+def test_output_files_vs_reference_writer(tmp_path, fmt):
+    case = C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005, wall_friction=C.REFERENCE_WALL_FRICTION, name="out")
+    case.params["output_format"] = fmt
+    ref_proj = str(tmp_path / "ref" / "out")
+    C.write_case(case, ref_proj)
+    run_reference(ref_proj, 4, 20, save_steps=(0, 20))
+    our_proj = str(tmp_path / "ours" / "out")
+    C.write_case(case, our_proj)
+    outdir = our_proj  # the reference writes into the folder named like the project
+    sim = LoquatSph(our_proj)
+    sim.save(outdir)
+    sim.step(20)
+    sim.save(outdir)
+    ref, ours = _files(ref_proj), _files(outdir)
+    report = []
+    if set(ref) != set(ours):
+        report.append(f"file names: reference only {sorted(set(ref) - set(ours))}, "
+                      f"ours only {sorted(set(ours) - set(ref))}")
+    for name in sorted(set(ref) & set(ours)):
+        a, b = ours[name], ref[name]
+        later = not re.search(r"(^|_)0\.(vtu|dat|xml)$", name)
+        tol = 1e-4 if later else 1e-5
+        if name.endswith(".xml"):
+            ta = [(e.tag, e.get("type"), e.text) for e in ET.parse(a).getroot()]
+            tb = [(e.tag, e.get("type"), e.text) for e in ET.parse(b).getroot()]
+            if ta != tb:
+                diff = [(x, y) for x, y in zip(ta, tb) if x != y]
+                report.append(f"{name}: {len(ta)} vs {len(tb)} tags; first differences {diff[:4]}")
+        elif name.endswith(".vtu"):
+            va, vb = _vtu_arrays(a), _vtu_arrays(b)
+            if [(n, c) for n, c, _ in va] != [(n, c) for n, c, _ in vb]:
+                report.append(f"{name}: arrays {[(n, c) for n, c, _ in va]} vs {[(n, c) for n, c, _ in vb]}")
+                continue
+            for (n, _, x), (_, _, y) in zip(va[1:], vb[1:]):
+                _compare_arrays(f"{name}/{n}", x, y, tol, report)
+        elif name.endswith(".dat"):
+            ra, rb = _numeric_rows(a), _numeric_rows(b)
+            if [len(r) for r in ra] != [len(r) for r in rb]:
+                report.append(f"{name}: row lengths differ")
+                continue
+            for col, cname in ((slice(0, 4), "codes"), (slice(4, 8), "pospres"), (slice(8, 12), "velrhop"),
+                               (slice(12, 15), "id mass w"), (slice(15, 21), "stress"), (slice(21, 27), "strain")):
+                _compare_arrays(f"{name}/{cname}", np.stack([r[col] for r in ra]), np.stack([r[col] for r in rb]), tol,
+                                report)
+        elif name == "time_history.txt":
+            ha, hb = np.array(_numeric_rows(a)), np.array(_numeric_rows(b))
+            if ha.shape != hb.shape or not np.array_equal(ha[:, 0], hb[:, 0]):
+                report.append(f"{name}: {ha.tolist()} vs {hb.tolist()}")
+            elif not np.all(np.abs(ha[:, 1] - hb[:, 1]) <= 5e-3 * np.abs(hb[:, 1])):
+                report.append(f"{name}: force {ha[:, 1]} vs {hb[:, 1]}")
+        elif name.startswith("stress_zz"):
+            pa, pb = np.array(_numeric_rows(a)), np.array(_numeric_rows(b))
+            if pa.shape != pb.shape or not np.allclose(pa[:, 0], pb[:, 0], rtol=1e-6, atol=0):
+                report.append(f"{name}: depths differ ({pa.shape} vs {pb.shape})")
+            elif not rel(pa[:, 1:], pb[:, 1:]) < 1e-3:
+                report.append(f"{name}: profile relative L2 {rel(pa[:, 1:], pb[:, 1:]):.2e}")
+    print(f"format {fmt}: compared {sorted(set(ref) & set(ours))}")
+    assert not report, "\n".join(report)

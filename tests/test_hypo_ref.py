@@ -54,3 +54,29 @@ def test_hypo_cs_double_to_float_sqrt_rounding():
         worst = max(worst, np.linalg.norm(s - r) / max(np.linalg.norm(r), 1e-300))
         assert m == G["f64/m_crt"][i]
     assert worst < 1e-7
+
+
+@pytest.mark.parametrize("prec,tag,npt", [(4, "f32", np.float32), (8, "f64", np.float64)])
+def test_drucker_prager_models(prec, tag, npt):
+    """Drucker-Prager (cuMatModDP, src/constitutive_model.h:38-84) and mu(I)-DP
+    (cuMatModMuIDP, :90-130), restated by the oracle, against the reference's own
+    functions on every third sample (cohesion, dilatancy, tension and shear yield
+    among them).  Float: bit-exact, yield flags included.  Double: mu(I)-DP bit-exact;
+    DP to float rounding, because the reference's FP64 build takes sqrtf of the
+    equivalent shear stress (:69) where the project's FP64 path is true double."""
+    from tests.golden.make_hypo_golden import plastic_params
+
+    worst = 0.0
+    for i in range(0, N, 3):
+        _, om, rate, sig, dt, _ = _args(i, npt)
+        pdp, pmu = (np.asarray(v, npt).astype(np.float64) for v in plastic_params(i, G["phi"][i]))
+        s, y = O.dp(prec, dt, om, rate, sig, pdp)
+        r = G[f"{tag}/dp"][i]
+        if prec == 4:
+            np.testing.assert_array_equal(s.astype(npt), r, err_msg=f"dp {i}")
+            assert y == G[f"{tag}/dp_yield"][i], i
+        else:
+            worst = max(worst, np.linalg.norm(s - r) / max(np.linalg.norm(r), 1e-300))
+        s, _ = O.dp(prec, dt, om, rate, sig, pmu, mui=True)
+        np.testing.assert_array_equal(s.astype(npt), G[f"{tag}/mui_dp"][i], err_msg=f"mui_dp {i}")
+    assert worst < 1e-7

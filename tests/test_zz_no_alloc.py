@@ -56,3 +56,33 @@ def test_noalloc_sort_rejects_oversize():
     big = (1 << 20) + 1
     assert L.rw_cell_sort_noalloc(ct.c_void_p(8), big, 100, ct.c_void_p(8), ct.c_void_p(8), None) == 1
     assert L.rw_cell_sort_noalloc(ct.c_void_p(8), 10, 1 << 24, ct.c_void_p(8), ct.c_void_p(8), None) == 1
+
+
+@pytest.mark.parametrize("max_key,n", [(200, 5000), ((1 << 24) - 1, 300_001), ((1 << 16) + 5, 2048 * 7 + 1)],
+                         ids=["one-pass", "three-pass", "three-pass-small"])
+def test_noalloc_sort_pass_counts(max_key, n):
+    """Key ranges that take one pass (max_key < 2^8) and three passes (max_key >= 2^16):
+    with an odd pass count the first pass writes the caller's outputs and reads its
+    values from an identity in the scratch.  Random keys, n not a multiple of the
+    2048-key tile, two calls in a row (the scratch keeps the previous call's contents);
+    the result equals numpy's stable argsort."""
+    import torch
+
+    from retainwall_code_b200 import _lib
+
+    L = _lib.lib()
+    rng = np.random.default_rng(max_key % 1000 + n)
+    keys = rng.integers(0, max_key + 1, n, dtype=np.int64).astype(np.int32)
+    keys[: n // 10] = max_key  # many ties at the top key
+    perm = np.argsort(keys, kind="stable").astype(np.int32)
+    dev = torch.device("cuda", 0)
+    keys_d = torch.from_numpy(keys).to(dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for call in range(2):
+        out_k = torch.full((n,), -7, dtype=torch.int32, device=dev)
+        out_p = torch.full((n,), -7, dtype=torch.int32, device=dev)
+        st = _call(L, keys_d, n, max_key, out_k, out_p, stream)
+        assert st == 0, (call, st)
+        torch.cuda.synchronize(dev)
+        np.testing.assert_array_equal(out_p.cpu().numpy(), perm, err_msg=f"call {call}: permutation")
+        np.testing.assert_array_equal(out_k.cpu().numpy(), keys[perm], err_msg=f"call {call}: keys")
