@@ -670,6 +670,49 @@ def precision_report(args):
     print(json.dumps(out), flush=True)
 
 
+def wallforce_report(args, device):
+    """The wall's lateral resultant over the 1.92M retaining wall's full trajectory
+    (20,000 steps at dt = 5e-6 s), in plain FP32 and in the precision form, against an
+    FP64 run of the same case: the resultant (nearest-wall sum, FP64 accumulation) is
+    sampled every `--wallforce-every` steps; reported are the largest deviation over the
+    trajectory relative to the largest FP64 magnitude, and the largest pointwise relative
+    deviation where the FP64 resultant is at least a tenth of its largest magnitude."""
+    import numpy as np
+
+    from retainwall_code_b200 import LoquatSph, _abi, cases as C
+
+    case = C.retaining_wall()
+    steps, every = args.wallforce_steps, args.wallforce_every
+    hist, times = {}, {}
+    for mode in ("f64", "f32", "f32_precision"):
+        sim = LoquatSph(case=case, device=device, precision=8 if mode == "f64" else 4)
+        if mode == "f32_precision":
+            sim.set_option(_abi.OPT_MIXED_PRECISION, 1)
+        wf, done, ms = [], 0, 0.0
+        while done < steps:
+            n = min(every, steps - done)
+            ms += sim.step_timed(n)
+            done += n
+            wf.append(sim.wall_force(0)[0])
+        if sim.info().device_err:
+            raise SystemExit(f"{mode}: device error word {sim.info().device_err}")
+        hist[mode], times[mode] = np.array(wf), ms / steps
+        sim.close()
+    ref = hist["f64"]
+    big = np.abs(ref) >= 0.1 * np.abs(ref).max()
+    out = {"metric": "wall lateral resultant vs FP64 over the full trajectory", "case": "retaining wall 200x80x120",
+           "steps": steps, "sample_every": every, "dt_s": 5e-6,
+           "f64_resultant_N": {"first": float(ref[0]), "last": float(ref[-1]), "max_abs": float(np.abs(ref).max())},
+           "ms_per_step": times}
+    for mode in ("f32", "f32_precision"):
+        d = np.abs(hist[mode] - ref)
+        out[mode] = {"max_dev_over_max_f64": float(d.max() / np.abs(ref).max()),
+                     "max_pointwise_rel_where_f64_above_10pct": float((d[big] / np.abs(ref[big])).max()),
+                     "final_rel": float(d[-1] / abs(ref[-1]))}
+    out["history_N"] = {k: [float(x) for x in v[:: max(1, len(v) // 20)]] for k, v in hist.items()}
+    print(json.dumps(out), flush=True)
+
+
 def closure_accuracy(net, steps, device, max_err=0.02):
     """FP64 runs against plain FP32 and FP32 with the learned closure, same seeds: the
     column collapse (config 1's case) for positions and stress invariants, a 41k
@@ -836,6 +879,10 @@ def main():
                     help="plain step graph without conditional nodes (for ncu, which replays single graph kernels)")
     ap.add_argument("--precision-report", action="store_true", help="precision form vs FP64 (configs 1 and 3)")
     ap.add_argument("--precision-steps", type=int, default=2000)
+    ap.add_argument("--wallforce-report", action="store_true",
+                    help="wall resultant of FP32 and the precision form vs FP64 over the 1.92M wall's trajectory")
+    ap.add_argument("--wallforce-steps", type=int, default=20000)
+    ap.add_argument("--wallforce-every", type=int, default=100)
     ap.add_argument("--batch-cases", type=int, default=64)
     ap.add_argument("--batch-forms", choices=["both", "closure", "precision"], default="both",
                     help="forms applied in the batch64_forms workload")
@@ -849,6 +896,9 @@ def main():
     args.warmup = max(3, args.warmup)
     if args.precision_report:
         precision_report(args)
+        return
+    if args.wallforce_report:
+        wallforce_report(args, 0)
         return
     if args.impl == "reference":  # host cores only: rank 0 runs, the other ranks exit
         ws = int(os.environ.get("WORLD_SIZE", "1"))

@@ -1126,6 +1126,88 @@ RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const ISt
   }
 }
 
+// Kept-list walk with the neighbour records loaded by lane pairs (float records).
+//
+// A warp's scattered record loads are bound by the L1 data stage, which delivers one
+// cache line per lane-request and cycle: each lane reading its own 64-byte record as two
+// 32-byte halves costs two wavefronts per lane and entry.  Here lanes 2k and 2k+1 load
+// both of their records together: in the first load both read record A (the even lane's;
+// even lane the first half, odd lane the second), in the second both read record B (the
+// odd lane's; odd lane the first half, even lane the second).  Each load then touches one
+// line per lane pair, half the wavefronts, and each lane hands the half it holds for its
+// partner over with one shuffle per word.  Every lane still evaluates its own list, in
+// its own order, with the values the single-lane walk reads: the sums are bit-identical.
+// All 32 lanes of the warp must call this (lanes without work pass cnt = 0).
+template <bool Strict>
+RWD void ix_walk_pairs(const Params<float>& P, const DevState<float>& S, const IState<float>& I, const unsigned* my,
+                       int stride, int cnt, Acc<float>& A) {
+  constexpr unsigned kAll = 0xffffffffu;
+  const int nit = __reduce_max_sync(kAll, cnt);  // warp-uniform trip count
+  if (nit == 0) return;
+  const bool odd = threadIdx.x & 1;
+  const int cnt_p = __shfl_xor_sync(kAll, cnt, 1);
+  const int cnt_a = odd ? cnt_p : cnt, cnt_b = odd ? cnt : cnt_p;  // even lane's, odd lane's
+  const float* __restrict__ base = reinterpret_cast<const float*>(S.rec);
+  const int half_a = odd ? 8 : 0, half_b = odd ? 0 : 8;  // float offset of the half each load takes
+  auto entry = [&](int k) -> unsigned { return k < cnt ? __ldcs(my + (size_t)k * stride) : 0u; };
+  auto ld8 = [](const float* q, bool ok, float (&v)[8]) {
+    if (ok) {
+      asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+          : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+          : "l"(q));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = 0.0f;
+    }
+  };
+  // loads of step e: record A (even lane's entry e) into x, record B (odd lane's) into y
+  auto issue = [&](int e, unsigned own, float (&x)[8], float (&y)[8]) {
+    const unsigned oth = __shfl_xor_sync(kAll, own, 1);
+    const unsigned ja = (odd ? oth : own) & 0x7ffffffu, jb = (odd ? own : oth) & 0x7ffffffu;
+    ld8(base + (size_t)ja * 16 + half_a, e < cnt_a, x);
+    ld8(base + (size_t)jb * 16 + half_b, e < cnt_b, y);
+  };
+  unsigned ent = entry(0);
+  unsigned ent1 = entry(1);
+  float x[8], y[8];
+  issue(0, ent, x, y);
+#pragma unroll 2  // alternating load registers instead of copying the prefetched ones
+  for (int e = 0; e < nit; ++e) {
+    float cx[8], cy[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      cx[k] = x[k];
+      cy[k] = y[k];
+    }
+    const int occ = (int)(ent >> 27);
+    if (e + 1 < nit) {
+      issue(e + 1, ent1, x, y);
+      ent = ent1;
+      ent1 = entry(e + 2);
+    }
+    // own record: first half kept (even lane: load A, odd lane: load B), second half
+    // received from the partner (which read it in the other load)
+    NbVals<float> nb;
+    float h1[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) h1[k] = __shfl_xor_sync(kAll, odd ? cx[k] : cy[k], 1);
+    nb.p = V4<float>{odd ? cy[0] : cx[0], odd ? cy[1] : cx[1], odd ? cy[2] : cx[2], odd ? cy[3] : cx[3]};
+    nb.vr = V4<float>{odd ? cy[4] : cx[4], odd ? cy[5] : cx[5], odd ? cy[6] : cx[6], odd ? cy[7] : cx[7]};
+    nb.a = V4<float>{h1[0], h1[1], h1[2], h1[3]};
+    nb.b = V4<float>{h1[4], h1[5], h1[6], h1[7]};
+    if (e < cnt) {
+      const int dz = (occ * 57) >> 9;
+      const int rr = occ - 9 * dz;
+      const int dy = (rr * 11) >> 5;
+      const int dx = rr - 3 * dy;
+      const float th = P.two_h;
+      pair_eval<Strict>(P, I, V3<float>{f_fma(small_float<float>(1 - dx), th, I.pos.x - nb.p.x),
+                                        f_fma(small_float<float>(1 - dy), th, I.pos.y - nb.p.y),
+                                        f_fma(small_float<float>(1 - dz), th, I.pos.z - nb.p.z)}, nb, A);
+    }
+  }
+}
+
 // Pair sums of particle i straight from global memory: phase 1 lists candidates in
 // shared memory (my[k * stride]), phase 2 evaluates them in order.  A list that fills
 // up is evaluated and emptied, and the scan resumes (order preserved).
@@ -1344,6 +1426,9 @@ template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Pa
 #ifndef RW_WALK_MIN_BLOCKS
 #define RW_WALK_MIN_BLOCKS 0  // resident blocks per SM the walk kernel's register budget aims at (0: none)
 #endif
+#ifndef RW_WALK_PAIRS
+#define RW_WALK_PAIRS 1  // float walk: records loaded by lane pairs (ix_walk_pairs); 0: one lane per record
+#endif
 template <class T, bool Strict, bool Walk>
 __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
     k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, int cpar) {
@@ -1351,10 +1436,31 @@ __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!Walk && t == 0) const_cast<Dyn<T>*>(dyn)->rec_stale = 0;  // the corner search has refreshed the records
   const int total = P.np - P.npb;
-  if (t >= total) return;
   const int i = P.npb + t;
   const int npm = dyn->npm;
   const bool keep = S.nbg && P.keep_lists;
+  if constexpr (Walk && sizeof(T) == 4 && RW_WALK_PAIRS) {
+    // every lane of a warp takes part in the pair loads, with or without a list of its own
+    const int kept = (keep && t < total && t < npm) ? S.nbg_cnt[t] : -1;
+    const bool mine = kept >= 0;
+    const int c = dyn->cur_main;
+    IState<T> I;
+    Acc<T> A;
+    V4<T> cv{};
+    I3 celli{0, 0, 0};
+    if (mine) {
+      const int4 cp = S.cellpos[c][i];
+      celli = I3{cp.x, cp.y, cp.z};
+      cv = S.cv[cpar][i];
+      ix_begin<Strict>(P, S, c, i, cv, I, A);
+    }
+    ix_walk_pairs<Strict>(P, S, I, S.nbg + (mine ? t : 0), S.nbg_stride, mine ? kept : 0, A);
+    if (!mine) return;
+    if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
+    ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
+    return;
+  }
+  if (t >= total) return;
   if (Walk) {
     if (!keep || t >= npm) return;
   } else if (t >= npm) {  // deleted slots keep their contact state
