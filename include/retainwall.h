@@ -219,9 +219,11 @@ rw_status rw_synchronize(rw_ctx* ctx);
  *         (0.04 + bound_thickness + 3 dr, bound_thickness + 0.04, bound_thickness + 1.04). */
 rw_status rw_wall_force(rw_ctx* ctx, int mode, int wall_id, const double* strip, double out_xyz[3]);
 /* Earth-pressure profile along the wall (GetValuesAlongLine, src/utilities.cu:266-367):
- * out[4*b] = depth b*dr, out[4*b+1..3] = contact_mag.xx / dr of the last soil particle
- * (index order, as the reference) in depth bin b of the 1st, 2nd, 3rd dr-thick band from
- * the wall face x_wall; bins of size dz below z_top; 0 for empty bins.  NaN x_wall, z_top
+ * out[4*b] = depth b*dr where the 1st band has a particle in bin b (the reference
+ * writes the depth together with that band's value; 0 otherwise), out[4*b+1..3] =
+ * contact_mag.xx / dr of the last soil particle (index order, as the reference) in depth
+ * bin b of the 1st, 2nd, 3rd dr-thick band from the wall face x_wall; bins of size dz
+ * below z_top; 0 for empty bins (the reference leaves them unwritten).  NaN x_wall, z_top
  * or dz select the reference's hard-coded values (face 0.04 + bound_thickness - 0.005 t,
  * top 0.04 + 1.0 + bound_thickness, dz = dr). */
 rw_status rw_wall_profile(rw_ctx* ctx, double x_wall, double z_top, double dz, int nbins, double* out);

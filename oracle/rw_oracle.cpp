@@ -551,7 +551,11 @@ template <class T> void Sim<T>::init(const rw_case* cs) {
     V3<T> a = xyz(pospres[i]) * half_ih;
     I3 c{(int)a.x, (int)a.y, (int)a.z};
     cellpos[i] = {c.x, c.y, c.z, 0};
-    pospres[i] = sub3(pospres[i], mulI(c, th));
+    // x - c 2h with one rounding: the reference's kernel is compiled with contraction,
+    // which fuses the product into the subtraction (src/loquat_grid.cu:259)
+    pospres[i].x = std::fma(-(T)c.x, th, pospres[i].x);
+    pospres[i].y = std::fma(-(T)c.y, th, pospres[i].y);
+    pospres[i].z = std::fma(-(T)c.z, th, pospres[i].z);
   }
   neighbor_search(0);
 }

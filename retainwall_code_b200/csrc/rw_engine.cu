@@ -574,20 +574,25 @@ template <class T> struct Engine final : EngineBase {
     cpar ^= 1;
   }
   void predictor() override {
+    if (P.closure) return integrate_closure(0);
     k_predictor<T><<<nblk(P.np, 256), 256, 0, st>>>(P, S, d_dyn);
     check_launch();
-    if (P.closure) launch_closure(0);
   }
   void corrector() override {
+    if (P.closure) return integrate_closure(1);
     k_corrector<T><<<nblk(P.npb + P.npm0, 256), 256, 0, st>>>(P, S, d_dyn);
     check_launch();
-    if (P.closure) launch_closure(1);
   }
-  void launch_closure(int stage) {
-    const long tiles = nblk(P.npm0, mlp::TILE);
+  // An integrator stage with the learned closure: one persistent launch, four 128-thread
+  // blocks per SM, each looping over tiles of rows (k_integrate_cl).
+  void integrate_closure(int stage) {
+    const long tiles = nblk(P.npb, mlp::TILE) + nblk(P.np - P.npb, mlp::TILE);
     const unsigned grid = (unsigned)std::max(1L, std::min(tiles, 4L * nsm));
-    k_closure<T><<<grid, mlp::TILE, sizeof(mlp::FwdSmem), st>>>(P, S, d_dyn, mlp::net_view(cl_net), cl_trust,
-                                                                 d_clstats, stage);
+    const mlp::Net net = mlp::net_view(cl_net);
+    if (stage == 0)
+      k_integrate_cl<T, 0><<<grid, mlp::TILE, sizeof(mlp::FwdSmem), st>>>(P, S, d_dyn, net, cl_trust, d_clstats);
+    else
+      k_integrate_cl<T, 1><<<grid, mlp::TILE, sizeof(mlp::FwdSmem), st>>>(P, S, d_dyn, net, cl_trust, d_clstats);
     check_launch();
   }
 
@@ -623,7 +628,9 @@ template <class T> struct Engine final : EngineBase {
     cl_trust.out_max = tmax * (1.0f + (float)margin);
     cl_trust.err_max = (float)cl_err_max;
     RW_CU(cudaSetDevice(device));
-    RW_CU(cudaFuncSetAttribute(k_closure<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RW_CU(cudaFuncSetAttribute(k_integrate_cl<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(mlp::FwdSmem)));
+    RW_CU(cudaFuncSetAttribute(k_integrate_cl<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(mlp::FwdSmem)));
     RW_CU(cudaMemsetAsync(d_clstats, 0, 4 * sizeof(double), st));
     RW_CU(cudaStreamSynchronize(st));
@@ -761,7 +768,6 @@ template <class T> struct Engine final : EngineBase {
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
     if (P.stress_shepard_filter != 0) k += 2;
-    if (P.closure) k += 2;
     if (P.npb == 0) k -= 2;
     return k;
   }
@@ -1235,7 +1241,9 @@ template <class T> struct Engine final : EngineBase {
     const std::string xmlp = dir + "/output_" + std::to_string(output_number) + ".xml";
     // The time written is the reference's par_host->time: that of the last step begun
     // (StepCalculation, src/loquat.cu:366-374), the case's time before any step.
-    int rc = write_output_xml(xmlp, cparams, P.np, P.npb, d.npm, (double)d.time_f, (double)P.dt, output_number);
+    // and the time step is the parameter file's until StepCalculation first sets it.
+    const double dt_out = initial && d.step == 0 ? (double)(T)cparams.dt : (double)P.dt;
+    int rc = write_output_xml(xmlp, cparams, P.np, P.npb, d.npm, (double)d.time_f, dt_out, output_number);
     if (rc) throw Fail(rc, "cannot write " + xmlp);
     if (P.output_format == 1) rc = write_frame_dat(dir + "/" + std::to_string(output_number) + ".dat", f);
     else rc = write_frame_vtu(dir, output_number, f);

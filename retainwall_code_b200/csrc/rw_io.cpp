@@ -339,9 +339,14 @@ int write_output_xml(const std::string& path, const rw_case_params& p, int np, i
   return o ? RW_OK : RW_EIO;
 }
 
+// Row layout of LoquatIo::SaveParticles format 1 (src/loquat_io.cu:440-461): every live
+// particle (boundary and soil) carries four normal columns, deleted particles do not and
+// end with a space.  The reference prints normal_m[i] for live soil rows too, reading
+// past its npb-entry normal array (src/loquat_io.cu:216,449); those columns are 0 here.
 int write_frame_dat(const std::string& path, const Frame& f) {
   std::ofstream o(path);
   if (!o) return RW_EIO;
+  const int live = f.npb + f.npm;
   for (int i = 0; i < f.np; ++i) {
     const int32_t* c = &f.codes[4 * i];
     o << c[0] << " " << c[1] << " " << c[2] << " " << c[3];
@@ -352,6 +357,10 @@ int write_frame_dat(const std::string& path, const Frame& f) {
     for (int k = 0; k < 6; ++k) o << " " << f.stn[6 * i + k];
     if (i < f.npb)
       for (int k = 0; k < 4; ++k) o << " " << f.normal[4 * i + k];
+    else if (i < live)
+      o << " 0 0 0 0";
+    else
+      o << " ";
     o << "\n";
   }
   return o ? RW_OK : RW_EIO;

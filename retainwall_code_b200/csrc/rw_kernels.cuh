@@ -186,10 +186,10 @@ struct RawCase {
   const double* normal;
 };
 
-// One particle of LoadParticles' conversion with the absolute -> in-cell split of
-// src/loquat_grid.cu:253-271: cell = trunc(x / 2h), in-cell position = x - cell * 2h.
-// Every product and difference is rounded on its own (no contraction), so the result
-// is the host arithmetic of the reference's loader, bit for bit.
+// One particle of LoadParticles' values with the absolute -> in-cell split of
+// PositionFromAbsolute2Relative (src/loquat_grid.cu:253-271): cell = trunc(x * (0.5/h)),
+// the product rounded on its own, in-cell position = x - cell * 2h with one rounding, as
+// the reference's kernel computes them.
 template <class T> __global__ void k_ingest(const Params<T> P, DevState<T> S, RawCase R, T half_ih) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= (size_t)P.np) return;
@@ -199,8 +199,10 @@ template <class T> __global__ void k_ingest(const Params<T> P, DevState<T> S, Ra
   S.pos_ori[0][i] = pa;
   const int cx = (int)rmul(pa.x, half_ih), cy = (int)rmul(pa.y, half_ih), cz = (int)rmul(pa.z, half_ih);
   S.cellpos[0][i] = int4{cx, cy, cz, 0};
-  S.pos[0][i] = V4<T>{add_rn(pa.x, -rmul((T)cx, P.two_h)), add_rn(pa.y, -rmul((T)cy, P.two_h)),
-                      add_rn(pa.z, -rmul((T)cz, P.two_h)), pa.w};
+  // x - c 2h as one fused multiply-add: the reference's kernel (cuPositionFromAbsolute2Relative,
+  // src/loquat_grid.cu:253-261) is compiled with contraction, which fuses that product
+  // into the subtraction
+  S.pos[0][i] = V4<T>{f_fma(-(T)cx, P.two_h, pa.x), f_fma(-(T)cy, P.two_h, pa.y), f_fma(-(T)cz, P.two_h, pa.z), pa.w};
   a = R.velrhop + 4 * i;
   S.vel[0][i] = V4<T>{(T)a[0], (T)a[1], (T)a[2], (T)a[3]};
   a = R.idmassidx + 4 * i;
@@ -1126,88 +1128,6 @@ RWD void ix_list_eval(const Params<T>& P, const DevState<T>& S, int c, const ISt
   }
 }
 
-// Kept-list walk with the neighbour records loaded by lane pairs (float records).
-//
-// A warp's scattered record loads are bound by the L1 data stage, which delivers one
-// cache line per lane-request and cycle: each lane reading its own 64-byte record as two
-// 32-byte halves costs two wavefronts per lane and entry.  Here lanes 2k and 2k+1 load
-// both of their records together: in the first load both read record A (the even lane's;
-// even lane the first half, odd lane the second), in the second both read record B (the
-// odd lane's; odd lane the first half, even lane the second).  Each load then touches one
-// line per lane pair, half the wavefronts, and each lane hands the half it holds for its
-// partner over with one shuffle per word.  Every lane still evaluates its own list, in
-// its own order, with the values the single-lane walk reads: the sums are bit-identical.
-// All 32 lanes of the warp must call this (lanes without work pass cnt = 0).
-template <bool Strict>
-RWD void ix_walk_pairs(const Params<float>& P, const DevState<float>& S, const IState<float>& I, const unsigned* my,
-                       int stride, int cnt, Acc<float>& A) {
-  constexpr unsigned kAll = 0xffffffffu;
-  const int nit = __reduce_max_sync(kAll, cnt);  // warp-uniform trip count
-  if (nit == 0) return;
-  const bool odd = threadIdx.x & 1;
-  const int cnt_p = __shfl_xor_sync(kAll, cnt, 1);
-  const int cnt_a = odd ? cnt_p : cnt, cnt_b = odd ? cnt : cnt_p;  // even lane's, odd lane's
-  const float* __restrict__ base = reinterpret_cast<const float*>(S.rec);
-  const int half_a = odd ? 8 : 0, half_b = odd ? 0 : 8;  // float offset of the half each load takes
-  auto entry = [&](int k) -> unsigned { return k < cnt ? __ldcs(my + (size_t)k * stride) : 0u; };
-  auto ld8 = [](const float* q, bool ok, float (&v)[8]) {
-    if (ok) {
-      asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-          : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
-          : "l"(q));
-    } else {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = 0.0f;
-    }
-  };
-  // loads of step e: record A (even lane's entry e) into x, record B (odd lane's) into y
-  auto issue = [&](int e, unsigned own, float (&x)[8], float (&y)[8]) {
-    const unsigned oth = __shfl_xor_sync(kAll, own, 1);
-    const unsigned ja = (odd ? oth : own) & 0x7ffffffu, jb = (odd ? own : oth) & 0x7ffffffu;
-    ld8(base + (size_t)ja * 16 + half_a, e < cnt_a, x);
-    ld8(base + (size_t)jb * 16 + half_b, e < cnt_b, y);
-  };
-  unsigned ent = entry(0);
-  unsigned ent1 = entry(1);
-  float x[8], y[8];
-  issue(0, ent, x, y);
-#pragma unroll 2  // alternating load registers instead of copying the prefetched ones
-  for (int e = 0; e < nit; ++e) {
-    float cx[8], cy[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      cx[k] = x[k];
-      cy[k] = y[k];
-    }
-    const int occ = (int)(ent >> 27);
-    if (e + 1 < nit) {
-      issue(e + 1, ent1, x, y);
-      ent = ent1;
-      ent1 = entry(e + 2);
-    }
-    // own record: first half kept (even lane: load A, odd lane: load B), second half
-    // received from the partner (which read it in the other load)
-    NbVals<float> nb;
-    float h1[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) h1[k] = __shfl_xor_sync(kAll, odd ? cx[k] : cy[k], 1);
-    nb.p = V4<float>{odd ? cy[0] : cx[0], odd ? cy[1] : cx[1], odd ? cy[2] : cx[2], odd ? cy[3] : cx[3]};
-    nb.vr = V4<float>{odd ? cy[4] : cx[4], odd ? cy[5] : cx[5], odd ? cy[6] : cx[6], odd ? cy[7] : cx[7]};
-    nb.a = V4<float>{h1[0], h1[1], h1[2], h1[3]};
-    nb.b = V4<float>{h1[4], h1[5], h1[6], h1[7]};
-    if (e < cnt) {
-      const int dz = (occ * 57) >> 9;
-      const int rr = occ - 9 * dz;
-      const int dy = (rr * 11) >> 5;
-      const int dx = rr - 3 * dy;
-      const float th = P.two_h;
-      pair_eval<Strict>(P, I, V3<float>{f_fma(small_float<float>(1 - dx), th, I.pos.x - nb.p.x),
-                                        f_fma(small_float<float>(1 - dy), th, I.pos.y - nb.p.y),
-                                        f_fma(small_float<float>(1 - dz), th, I.pos.z - nb.p.z)}, nb, A);
-    }
-  }
-}
-
 // Pair sums of particle i straight from global memory: phase 1 lists candidates in
 // shared memory (my[k * stride]), phase 2 evaluates them in order.  A list that fills
 // up is evaluated and emptied, and the scan resumes (order preserved).
@@ -1426,9 +1346,6 @@ template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Pa
 #ifndef RW_WALK_MIN_BLOCKS
 #define RW_WALK_MIN_BLOCKS 0  // resident blocks per SM the walk kernel's register budget aims at (0: none)
 #endif
-#ifndef RW_WALK_PAIRS
-#define RW_WALK_PAIRS 1  // float walk: records loaded by lane pairs (ix_walk_pairs); 0: one lane per record
-#endif
 template <class T, bool Strict, bool Walk>
 __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
     k_interaction(const Params<T> P, DevState<T> S, const Dyn<T>* dyn, int cpar) {
@@ -1436,31 +1353,10 @@ __global__ void __launch_bounds__(IX_THREADS, Walk ? RW_WALK_MIN_BLOCKS : 0)
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (!Walk && t == 0) const_cast<Dyn<T>*>(dyn)->rec_stale = 0;  // the corner search has refreshed the records
   const int total = P.np - P.npb;
+  if (t >= total) return;
   const int i = P.npb + t;
   const int npm = dyn->npm;
   const bool keep = S.nbg && P.keep_lists;
-  if constexpr (Walk && sizeof(T) == 4 && RW_WALK_PAIRS) {
-    // every lane of a warp takes part in the pair loads, with or without a list of its own
-    const int kept = (keep && t < total && t < npm) ? S.nbg_cnt[t] : -1;
-    const bool mine = kept >= 0;
-    const int c = dyn->cur_main;
-    IState<T> I;
-    Acc<T> A;
-    V4<T> cv{};
-    I3 celli{0, 0, 0};
-    if (mine) {
-      const int4 cp = S.cellpos[c][i];
-      celli = I3{cp.x, cp.y, cp.z};
-      cv = S.cv[cpar][i];
-      ix_begin<Strict>(P, S, c, i, cv, I, A);
-    }
-    ix_walk_pairs<Strict>(P, S, I, S.nbg + (mine ? t : 0), S.nbg_stride, mine ? kept : 0, A);
-    if (!mine) return;
-    if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
-    ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
-    return;
-  }
-  if (t >= total) return;
   if (Walk) {
     if (!keep || t >= npm) return;
   } else if (t >= npm) {  // deleted slots keep their contact state
@@ -1752,9 +1648,9 @@ template <class T, bool Strict> __global__ void __launch_bounds__(IX2_TB) k_inte
 // 100 spilled bytes): they stream about 300 B per particle, and at the two blocks
 // their natural 94 registers allow they wait on memory (measured 19% faster at
 // three blocks, another 5% at four).
-template <class T>
-__global__ void __launch_bounds__(256, 4) k_predictor(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One row of the predictor.  With the learned closure on, HypoCS rows keep their stress
+// here and the closure's pass updates it (and writes their record).
+template <class T> RWD void predictor_row(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, int i) {
   if (i >= P.np) return;
   const int c = dyn->cur_main, ci = dyn->cur_ini;
   const int npm = dyn->npm;
@@ -1814,6 +1710,11 @@ __global__ void __launch_bounds__(256, 4) k_predictor(const Params<T> P, DevStat
   if (!by_closure) write_rec(P, S.rec, i, ps, vr, sg, mass, code.x >= 10);
 }
 
+template <class T>
+__global__ void __launch_bounds__(256, 4) k_predictor(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  predictor_row(P, S, dyn, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------------
 // Corrector (src/predictor_corrector.cu:109-213): rigid walls and material.
 // ---------------------------------------------------------------------------------
@@ -1840,9 +1741,9 @@ template <class T> RWD void list_account(const Params<T>& P, const DevState<T>& 
   if (cell_moved || d > P.disp_lim) const_cast<Dyn<T>*>(dyn)->list_kill = 1;
 }
 
-template <class T>
-__global__ void __launch_bounds__(256, 4) k_corrector(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One row of the corrector (moving boundary rows and soil rows); with the learned
+// closure on, HypoCS rows keep their stress here, as in predictor_row.
+template <class T> RWD void corrector_row(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, int i) {
   const int npm = dyn->npm;
   if (i >= P.npb + npm) return;
   const int c = dyn->cur_main, ci = dyn->cur_ini;
@@ -1940,6 +1841,11 @@ __global__ void __launch_bounds__(256, 4) k_corrector(const Params<T> P, DevStat
   S.pos_ori[c][i] = po;
   S.accad[i] = po;
   if (!by_closure) write_rec(P, S.rec, i, ps, vr, sg, id.y, code.x >= 10);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256, 4) k_corrector(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  corrector_row(P, S, dyn, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------------
@@ -2052,7 +1958,8 @@ template <class T> __global__ void k_profile_read(const Params<T> P, DevState<T>
                                                   const int* last, double* out) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbins) return;
-  out[4 * b] = (double)b * (double)P.dr;
+  // the depth is written with the first band's value, as the reference's .xy
+  out[4 * b] = last[b] >= 0 ? (double)b * (double)P.dr : 0.0;
   for (int band = 0; band < 3; ++band) {
     const int i = last[band * nbins + b];
     out[4 * b + 1 + band] = i >= 0 ? (double)(S.cf[cpar][i].x / P.dr) : 0.0;
@@ -2247,19 +2154,15 @@ template <class T> __global__ void k_collect(const Params<T> P, DevState<T> S, c
 // the Jaumann term, the cut-offs and every particle outside the trust region (or whose
 // output leaves it) stay exact.  Every closure update is judged against the exact rate:
 // stats = [offered, used, sum of relative errors, largest relative error].
+// One tile of 128 soil slots (t = tile * 128 + thread); every thread of the block calls
+// it for the same tile (the network runs on the whole tile).
 template <class T>
-__global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevState<T> S, Dyn<T>* dyn, mlp::Net net,
-                                                        ClosureTrust tr, double* stats, int stage) {
-  extern __shared__ __align__(128) unsigned char raw[];
-  mlp::FwdSmem& sm = *reinterpret_cast<mlp::FwdSmem*>(raw);
-  mlp::load_fwd(sm, net);
-  if (threadIdx.x == 0) sm.err = 0;
-  mlp::block_setup(&sm.bar, &sm.tmem, 64);
+RWD void closure_tile(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, mlp::FwdSmem& sm,
+                      const ClosureTrust& tr, double* stats, int stage, int tile, uint32_t& phase) {
   const int npm = dyn->npm, c = dyn->cur_main;
   const int tid = threadIdx.x, lane = tid & 31;
   const T dt = stage == 0 ? T(0.5f) * P.dt : P.dt;
-  uint32_t phase = 0;
-  for (int tile = blockIdx.x; tile * mlp::TILE < npm; tile += gridDim.x) {
+  {
     const int t = tile * mlp::TILE + tid, i = P.npb + t;
     bool mine = false, act = false;
     float f[mlp::IN];
@@ -2347,10 +2250,45 @@ __global__ void __launch_bounds__(mlp::TILE) k_closure(const Params<T> P, DevSta
       atomicMax(reinterpret_cast<unsigned long long*>(&stats[3]), (unsigned long long)__double_as_longlong((double)sx));
     }
   }
+}
+
+// One integrator stage (0: predictor, 1: corrector) with the learned closure, in one
+// persistent launch: the rows of a tile are advanced as predictor_row / corrector_row do
+// (HypoCS stresses left to the closure), then the same block runs the closure on them.
+// Tiles: the boundary rows first (integrator only), then the soil slots (in the predictor
+// the deleted slots too, for their step-start copies).
+template <class T, int Stage>
+__global__ void __launch_bounds__(mlp::TILE) k_integrate_cl(const Params<T> P, DevState<T> S, Dyn<T>* dyn,
+                                                             mlp::Net net, ClosureTrust tr, double* stats) {
+  extern __shared__ __align__(128) unsigned char raw[];
+  mlp::FwdSmem& sm = *reinterpret_cast<mlp::FwdSmem*>(raw);
+  mlp::load_fwd(sm, net);
+  if (threadIdx.x == 0) sm.err = 0;
+  mlp::block_setup(&sm.bar, &sm.tmem, 64);
+  const int nb_tiles = (P.npb + mlp::TILE - 1) / mlp::TILE;
+  const int soil_rows = Stage == 0 ? P.np - P.npb : dyn->npm;
+  const int n_tiles = nb_tiles + (soil_rows + mlp::TILE - 1) / mlp::TILE;
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {  // block-uniform
+    if (tile < nb_tiles) {
+      const int i = tile * mlp::TILE + threadIdx.x;
+      if (i < P.npb) {
+        if (Stage == 0) predictor_row(P, S, dyn, i);
+        else corrector_row(P, S, dyn, i);
+      }
+      continue;
+    }
+    const int st = tile - nb_tiles, t = st * mlp::TILE + threadIdx.x;
+    if (t < soil_rows) {
+      if (Stage == 0) predictor_row(P, S, dyn, P.npb + t);
+      else corrector_row(P, S, dyn, P.npb + t);
+    }
+    closure_tile(P, S, dyn, sm, tr, stats, Stage, st, phase);
+  }
   __syncthreads();
   mlp::drain_after_timeout(&sm.bar, sm.err, phase);
   mlp::block_teardown(sm.tmem, 64);
-  if (tid == 0 && sm.err) atomicOr(&dyn->err, 16u);
+  if (threadIdx.x == 0 && sm.err) atomicOr(&dyn->err, 16u);
 }
 
 }  // namespace rw

@@ -140,48 +140,67 @@ struct TrainSmem {
 constexpr uint32_t TRAIN_TMEM_COLS = 512;  // Z1..Z4 at 0..255, output at 256, dH at 320
 constexpr int TCOL_Y = 256, TCOL_DH = 320;
 
-// acc[w0 + i * NOUT + o] += sum_b Hin[b][i] G[b][o];  acc[b0 + o] += sum_b G[b][o].
-// KIN x NOUT / OPT == 128: each thread owns OPT outputs of one input row i.
-template <int KIN, int GK, int NOUT, int OPT>
-__device__ __forceinline__ void wgrad(float* acc, int w0, int b0, const unsigned char* hin, const unsigned char* g) {
-  static_assert(KIN * NOUT / OPT == TILE, "one thread per output group");
-  const int tid = threadIdx.x;
-  const int i = tid / (NOUT / OPT), o0 = (tid % (NOUT / OPT)) * OPT;
-  float s[OPT];
+// Weight gradients on the tensor cores.  For the tile's 128 samples b,
+//   dW(l) = H(l-1)^T G(l)   (layers 2..5: M = 64 input features, N = the layer's outputs)
+//   dW(1)^T = G(1)^T X      (layer 1: M = 64 outputs, N = 16 inputs)
+// as D[64 x N] = A^T B with A and B the 128-row activation / signal tiles already in
+// shared memory, read MN-major (no transposed copy).  Issued by one thread; K = 128 in
+// eight steps of 16.
+__device__ __forceinline__ void issue_wgrad(const unsigned char* a_tile, int Ka, const unsigned char* b_tile, int Kb,
+                                            int N, uint32_t d_tmem) {
+  const uint32_t a0 = tc::smem_u32(a_tile), b0 = tc::smem_u32(b_tile);
+  const uint32_t idesc = tc::idesc_bf16_mn(64, N);
+  for (int ks = 0; ks < TILE / 16; ++ks)
+    tc::mma_bf16(d_tmem, tc::sdesc_mn(a0 + (uint32_t)(Ka * 32 * ks), Ka), tc::sdesc_mn(b0 + (uint32_t)(Kb * 32 * ks), Kb),
+                 idesc, ks > 0 ? 1u : 0u);
+}
+
+// Adds a 64 x N accumulator (M = 64 layout: row r in TMEM lane 32 (r / 16) + r % 16, so
+// lanes 0..15 of warp w hold rows 16 w .. 16 w + 15) into acc[base + col * 64 + row], for
+// the columns col < ncols.  tcol: the accumulator's first column.  Every lane takes part
+// in the TMEM loads; lanes 16..31 discard theirs.
+template <int N>
+__device__ __forceinline__ void add_wgrad(float* acc, uint32_t tmem, uint32_t tcol, int base, int ncols) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const uint32_t taddr = tmem + ((uint32_t)(w * 32) << 16) + tcol;
+  const int r = 16 * w + l;
 #pragma unroll
-  for (int k = 0; k < OPT; ++k) s[k] = 0.0f;
-  if constexpr (OPT % 8 == 0) {  // whole 16-byte runs of the G row: vector loads
-#pragma unroll 2
-    for (int b = 0; b < TILE; ++b) {
-      const float hv = load_elem<KIN>(hin, b, i);
+  for (int c = 0; c < N; c += 16) {
+    float v[16];
+    tc::tmem_ld16(taddr + (uint32_t)c, v);
+    if (l < 16)
 #pragma unroll
-      for (int k8 = 0; k8 < OPT; k8 += 8) {
-        const uint4 q = *reinterpret_cast<const uint4*>(g + tc::kmajor_off(b, o0 + k8, GK));
-        s[k8 + 0] = fmaf(hv, bf16_lo(q.x), s[k8 + 0]);
-        s[k8 + 1] = fmaf(hv, bf16_hi(q.x), s[k8 + 1]);
-        s[k8 + 2] = fmaf(hv, bf16_lo(q.y), s[k8 + 2]);
-        s[k8 + 3] = fmaf(hv, bf16_hi(q.y), s[k8 + 3]);
-        s[k8 + 4] = fmaf(hv, bf16_lo(q.z), s[k8 + 4]);
-        s[k8 + 5] = fmaf(hv, bf16_hi(q.z), s[k8 + 5]);
-        s[k8 + 6] = fmaf(hv, bf16_lo(q.w), s[k8 + 6]);
-        s[k8 + 7] = fmaf(hv, bf16_hi(q.w), s[k8 + 7]);
-      }
-    }
-  } else {
-#pragma unroll 4
-    for (int b = 0; b < TILE; ++b) {
-      const float hv = load_elem<KIN>(hin, b, i);
-#pragma unroll
-      for (int k = 0; k < OPT; ++k) s[k] = fmaf(hv, load_elem<GK>(g, b, o0 + k), s[k]);
-    }
+      for (int k = 0; k < 16; ++k)
+        if (c + k < ncols) acc[base + (c + k) * 64 + r] += v[k];
   }
-#pragma unroll
-  for (int k = 0; k < OPT; ++k) acc[w0 + i * NOUT + o0 + k] += s[k];
-  if (tid < NOUT) {
-    float t = 0.0f;
-    for (int b = 0; b < TILE; ++b) t += load_elem<GK>(g, b, tid);
-    acc[b0 + tid] += t;
+}
+
+// acc[b0 + o] += sum over the tile's 128 rows of G[b][o], for o < NB (G: 128 x Kg tile).
+// Thread o sums column o; the rows are visited in an order rotated by o / 8, so the four
+// 8-column groups of a warp read different banks.
+template <int Kg, int NB>
+__device__ __forceinline__ void add_bias_grad(float* acc, int b0, const unsigned char* g) {
+  const int o = threadIdx.x;
+  if (o >= NB) return;
+  float t = 0.0f;
+#pragma unroll 8
+  for (int k = 0; k < TILE; ++k) t += load_elem<Kg>(g, (k + (o >> 3)) & (TILE - 1), o);
+  acc[b0 + o] += t;
+}
+
+// The accumulator layout of the weight gradients in shared memory: W1 as the parameters
+// ([in][out]), W2..W5 transposed ([out][in], the rows of the tensor-core products).
+__device__ __forceinline__ int acc_index(int k) {
+  if (k >= P_W2 && k < P_B4 && !((k >= P_B2 && k < P_W3) || (k >= P_B3 && k < P_W4))) {
+    const int w0 = k < P_B2 ? P_W2 : k < P_B3 ? P_W3 : P_W4;
+    const int rel = k - w0;
+    return w0 + (rel % HID) * HID + rel / HID;
   }
+  if (k >= P_W5 && k < P_B5) {
+    const int rel = k - P_W5;
+    return P_W5 + (rel % OUT) * HID + rel / OUT;
+  }
+  return k;
 }
 
 __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restrict__ X, const float* __restrict__ Tg,
@@ -274,16 +293,19 @@ __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restr
     }
     tc::fence_smem_to_async();
     __syncthreads();
-    if (tid == 0 && !sm.err) {  // dH4 = G5 W5
+    if (tid == 0 && !sm.err) {  // dH4 = G5 W5 and dW5 = H4^T G5 (into the output's columns)
       tc::fence_after_sync();
       issue_layer(sm.g5, OUTP, sm.bw + BW5, HID, sm.tmem + TCOL_DH);
+      issue_wgrad(sm.h[NHID - 1], HID, sm.g5, OUTP, OUTP, sm.tmem + TCOL_Y);
       tc::mma_commit(&sm.bar);
     }
-    wgrad<HID, OUTP, OUT, 3>(sm.acc, P_W5, P_B5, sm.h[NHID - 1], sm.g5);
+    add_bias_grad<OUTP, OUT>(sm.acc, P_B5, sm.g5);
     wait_mma();
+    add_wgrad<OUTP>(sm.acc, sm.tmem, TCOL_Y, P_W5, OUT);  // warp-wide loads: unconditional
+    tc::fence_before_sync();
     // ---- hidden layers, last to first -------------------------------------------
     for (int l = NHID; l >= 1; --l) {
-      __syncthreads();  // the previous weight gradient has finished reading sm.g
+      __syncthreads();  // the previous bias gradient has finished reading sm.g
       const float* b = sm.bias + (l - 1) * HID;
 #pragma unroll 1
       for (int c = 0; c < HID; c += 16) {
@@ -297,20 +319,28 @@ __global__ void __launch_bounds__(TILE, 1) k_train(Net net, const float* __restr
       tc::fence_before_sync();
       tc::fence_smem_to_async();
       __syncthreads();
-      if (l > 1 && tid == 0 && !sm.err) {  // dH(l-1) = G(l) W(l)
+      // dH(l-1) = G(l) W(l) into the dH columns, and the weight gradient into Z(l)'s
+      // columns (read above): dW(l) = H(l-1)^T G(l), for layer 1 dW(1)^T = G(1)^T X
+      const uint32_t zcol = 64u * (l - 1);
+      if (tid == 0 && !sm.err) {
         tc::fence_after_sync();
-        issue_layer(sm.g, HID, sm.bw + (l == 2 ? BW2 : l == 3 ? BW3 : BW4), HID, sm.tmem + TCOL_DH);
+        if (l > 1) {
+          issue_layer(sm.g, HID, sm.bw + (l == 2 ? BW2 : l == 3 ? BW3 : BW4), HID, sm.tmem + TCOL_DH);
+          issue_wgrad(sm.h[l - 2], HID, sm.g, HID, HID, sm.tmem + zcol);
+        } else {
+          issue_wgrad(sm.g, HID, sm.x, IN, IN, sm.tmem + zcol);
+        }
         tc::mma_commit(&sm.bar);
       }
-      if (l == 1) wgrad<IN, HID, HID, 8>(sm.acc, P_W1, P_B1, sm.x, sm.g);
-      else
-        wgrad<HID, HID, HID, 32>(sm.acc, l == 2 ? P_W2 : l == 3 ? P_W3 : P_W4, l == 2 ? P_B2 : l == 3 ? P_B3 : P_B4,
-                                 sm.h[l - 2], sm.g);
-      if (l > 1) wait_mma();
+      add_bias_grad<HID, HID>(sm.acc, l == 1 ? P_B1 : l == 2 ? P_B2 : l == 3 ? P_B3 : P_B4, sm.g);
+      wait_mma();
+      if (l > 1) add_wgrad<HID>(sm.acc, sm.tmem, zcol, l == 2 ? P_W2 : l == 3 ? P_W3 : P_W4, HID);
+      else add_wgrad<IN>(sm.acc, sm.tmem, zcol, P_W1, IN);
+      tc::fence_before_sync();
     }
   }
   __syncthreads();
-  for (int k = tid; k < NPARAM; k += TILE) atomicAdd(&grad[k], sm.acc[k]);
+  for (int k = tid; k < NPARAM; k += TILE) atomicAdd(&grad[k], sm.acc[acc_index(k)]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
   if ((tid & 31) == 0) atomicAdd(loss, (double)lsum);

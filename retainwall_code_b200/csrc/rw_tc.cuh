@@ -3,7 +3,8 @@
 // (TMEM) allocation, MMA issue and completion through an mbarrier, TMEM loads, and the
 // fences that order them against ordinary thread code.
 //
-// Operand layout used everywhere in this project: K-major, no swizzle.  A tile of R rows
+// Operand layout used everywhere in this project: K-major, no swizzle (read transposed as
+// MN-major by the weight-gradient products, see sdesc_mn).  A tile of R rows
 // (M or N) by K columns of 16-bit elements is stored as 8-row x 16-byte core matrices;
 // element (r, k) lives at byte
 //     (r / 8) * SBO + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2,   SBO = (K / 8) * 128,
@@ -38,6 +39,20 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16, both K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+// The same with A and B both MN-major (bits 15 and 16: the operands are read transposed).
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(int M, int N) {
+  return idesc_bf16(M, N) | (1u << 15) | (1u << 16);
+}
+
+// A K-major, no-swizzle tile of 128 rows by Kc columns (the layout above) read as an
+// MN-major operand whose MN index is the tile's column and whose K index is its row:
+// the 8-row x 16-byte core matrices are then 8 K-rows of 8 MN elements, the core
+// matrices adjacent in MN are 128 bytes apart (stride byte offset) and the groups of 8
+// K-rows (Kc / 8) * 128 bytes apart (leading byte offset).  One MMA (K = 16) consumes
+// two such groups; the next one starts Kc * 32 bytes further.
+__device__ __forceinline__ uint64_t sdesc_mn(uint32_t saddr, int Kc) {
+  return sdesc(saddr, (uint32_t)Kc * 16u, 128u);
 }
 
 // ---- mbarrier ------------------------------------------------------------------------

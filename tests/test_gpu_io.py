@@ -18,7 +18,8 @@ def _wall_case():
 
 def test_wall_profile_matches_reference_loop_semantics():
     """Per (band, depth bin): value of the highest-index particle in it, as the
-    reference's sequential loop leaves it."""
+    reference's sequential loop leaves it; the depth of a bin only where the first band
+    has a particle (the reference writes it together with that band's value)."""
     s = LoquatSph(case=_wall_case())
     s.step(40)
     inf = s.info()
@@ -28,7 +29,6 @@ def test_wall_profile_matches_reference_loop_semantics():
     pos = s.get("pos_abs").astype(np.float32)
     cm = s.get("contact_mag")
     exp = np.zeros((nb, 4))
-    exp[:, 0] = np.arange(nb) * np.float64(np.float32(dr))
     for i in range(inf.npb, inf.np):
         px, pz = float(pos[i, 0]), float(pos[i, 2])
         if not (z_top - 1.0 <= pz <= z_top):
@@ -38,6 +38,8 @@ def test_wall_profile_matches_reference_loop_semantics():
                 b = int((z_top - pz) / dr)
                 if 0 <= b < nb:
                     exp[b, 1 + band] = float(np.float32(cm[i, 0]) / np.float32(dr))
+                    if band == 0:  # the depth is written with the first band's value
+                        exp[b, 0] = b * np.float64(np.float32(dr))
     np.testing.assert_allclose(prof, exp, rtol=1e-6, atol=1e-9)
     assert (prof[:, 1] != 0).any()
 
@@ -72,7 +74,7 @@ def test_save_dat_format_roundtrips(tmp_path):
     s.save(out)
     rows = open(os.path.join(out, "1.dat")).read().strip().split("\n")
     assert len(rows) == case.np_
-    assert len(rows[0].split()) == 31 and len(rows[-1].split()) == 27
+    assert all(len(r.split()) == 31 for r in rows)  # every live row carries the normal columns
     pos = np.array([list(map(float, r.split()[4:7])) for r in rows])
     np.testing.assert_allclose(pos, s.get("pos_abs")[:, :3], rtol=5e-6, atol=1e-9)  # 6 significant digits
 
@@ -94,9 +96,9 @@ def test_cli_runs_project(tmp_path):
 
 def test_case_ingest_matches_host_conversion():
     """rw_create_from_case copies the caller's double arrays as they are and converts them
-    on the device (LoadParticles' absolute -> in-cell split, src/loquat_grid.cu:253-271).
-    The state after creation equals the same conversion done on the host in float32,
-    bit for bit, row by row (rows are matched through the original index that the
+    on the device (LoadParticles' values, PositionFromAbsolute2Relative's absolute ->
+    in-cell split with the fused product of src/loquat_grid.cu:253-271).  The state after
+    creation equals the same conversion done on the host in float32, bit for bit, row by row (rows are matched through the original index that the
     loader keeps in idmassidx[:, 2], since creation also sorts by cell)."""
     c = C.retaining_wall(nx=24, ny=12, nz=16, dx=0.004, name="ingest")
     s = LoquatSph(case=c)
@@ -107,7 +109,8 @@ def test_case_ingest_matches_host_conversion():
     pa = c.pospres.astype(f32)
     cell = (pa[:, :3] * half_ih).astype(np.int32)  # truncation toward zero
     pos = pa.copy()
-    pos[:, :3] = pa[:, :3] - cell.astype(f32) * two_h
+    # x - c 2h with one rounding (exact in double, then rounded once to float)
+    pos[:, :3] = (pa[:, :3].astype(np.float64) - cell.astype(np.float64) * np.float64(two_h)).astype(f32)
     idx = s.get("idmassidx")[:, 2].astype(np.int64)
     assert np.array_equal(np.sort(idx), np.arange(c.np_))
     np.testing.assert_array_equal(s.get("pospres"), pos[idx].astype(np.float64))

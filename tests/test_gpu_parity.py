@@ -49,6 +49,8 @@ def test_initial_cell_list_bit_exact(cases, name):
         np.testing.assert_array_equal(s.get(k), g[f"init/{k}"] if f"init/{k}" in g else o.get(k), err_msg=k)
         np.testing.assert_array_equal(s.get(k), o.get(k), err_msg=k)
     np.testing.assert_array_equal(s.get("pospres"), o.get("pospres"))
+    # the in-cell positions of the reference's own loader, bit for bit
+    np.testing.assert_array_equal(s.get("pospres"), g["init/pospres"])
 
 
 @pytest.mark.parametrize("name", CASES)

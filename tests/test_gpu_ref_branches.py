@@ -9,7 +9,7 @@ against the CPU oracle and against the unmodified reference CUDA build run live:
 * a wall rotating about its toe and a wall translating into the soil (passive): the
   rotation table of RigidBodyUpdate (src/adami_boundary.cu:175-203) and the Rodrigues
   update of positions and normals in cuCorrectorBound
-  (src/predictor_corrector.cu:109-137).  The wall speeds are raised (2 rad/s, 0.2 m/s)
+  (src/predictor_corrector.cu:109-137).  The wall speeds are raised (2 rad/s, 0.02 m/s)
   so that 100 steps move the wall by a measurable amount; the code path is the one of
   the configured speeds.
 
@@ -137,8 +137,9 @@ def test_shepard_filter_in_the_step_vs_reference_and_oracle(tmp_path, every):
 
 @pytest.mark.parametrize("mode", ["rotation", "passive"])
 def test_moving_wall_vs_reference_and_oracle(tmp_path, mode):
+    speed, omega = 0.02, 2.0
     case = C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005, wall_friction=C.REFERENCE_WALL_FRICTION, mode=mode,
-                            wall_speed=0.2, rot_speed=2.0, name=mode)
+                            wall_speed=speed, rot_speed=omega, name=mode)
     proj, dd = _ref_trajectory(tmp_path, case, 4, 100, (10, 100), mode)
     sim = LoquatSph(proj)
     orc = Oracle(C.read_case(proj), 4)
@@ -175,9 +176,13 @@ def test_moving_wall_vs_reference_and_oracle(tmp_path, mode):
                     report.append(f"step {st} {k} vs {who} beyond 2h of contact: {rel(a[far], b[far]):.2e}")
                 if not rel(a, b) < 1e-4:
                     report.append(f"step {st} {k} vs {who}: {rel(a, b):.2e}")
+    assert not report, "\n".join(report)
     orig = sim.get("idmassidx")[:, 2].astype(np.int64)
     moved = np.abs(sim.get("pos_abs")[wall, :3] - case.pospres[orig[wall], :3]).max()
-    assert moved > 0.05 * case.params["dr"], moved
+    t = 100 * sim.info().dt
+    lever = case.pospres[case.codes[:, 0] >= 10, 2].max() - case.motions[0].pos_rp[2]
+    expect = speed * t if mode == "passive" else omega * t * lever
+    assert 0.5 * expect < moved < 2.0 * expect, (moved, expect)
     if mode == "rotation":
         n = sim.get("normal_m")[wall[:case.npb], :3]
         assert np.abs(n[:, 2]).max() > 1e-3  # the normals turned with the wall

