@@ -167,15 +167,24 @@ def test_moving_wall_vs_reference_and_oracle(tmp_path, mode):
             r = rel(n_ours[:, :3], b[wall[:case.npb], :3])
             if not r < 1e-6:
                 report.append(f"step {st} wall normals vs {who}: {r:.2e}")
-        # the soil: 1e-5 beyond 2h of the contact zone, 1e-4 over the whole state
+        # the soil: 1e-5 beyond 2h of the contact zone, 1e-4 over the whole state.  A wall
+        # pushed into the soil (passive) keeps most of the soil next to it in contact, and
+        # the reference's contact redistribution reads contact state that other threads
+        # of the same launch are rewriting (src/particle_interaction.cu:147-166); the
+        # product and the oracle read it as of the start of the stage and agree with each
+        # other to the bars above, while the reference moves away from both by 1e-4 of the
+        # stress (beyond 2h of the zone after 100 steps) and 1e-3 over the whole state.
         far = far_from_contact(case, g["cellpos"], g["pospres"], g["contact_var"])
+        ref_far, ref_all = (5e-4, 2e-3) if mode == "passive" else (1e-5, 1e-4)
         for k in ("pospres", "velrhop", "str"):
             a = sim.get(k)
-            for who, b in (("reference", g[k]), ("oracle", orc.get(k))):
-                if not rel(a[far], b[far]) < 1e-5:
+            for who, b, tf, ta in (("reference", g[k], ref_far, ref_all), ("oracle", orc.get(k), 1e-5, 1e-4)):
+                if not rel(a[far], b[far]) < tf:
                     report.append(f"step {st} {k} vs {who} beyond 2h of contact: {rel(a[far], b[far]):.2e}")
-                if not rel(a, b) < 1e-4:
+                if not rel(a, b) < ta:
                     report.append(f"step {st} {k} vs {who}: {rel(a, b):.2e}")
+            print(f"{mode} step {st} {k}: vs reference {rel(a[far], g[k][far]):.2e} beyond 2h, {rel(a, g[k]):.2e} "
+                  f"whole; vs oracle {rel(a[far], orc.get(k)[far]):.2e}, {rel(a, orc.get(k)):.2e}")
     assert not report, "\n".join(report)
     orig = sim.get("idmassidx")[:, 2].astype(np.int64)
     moved = np.abs(sim.get("pos_abs")[wall, :3] - case.pospres[orig[wall], :3]).max()
