@@ -326,7 +326,9 @@ def run_batch(args, ws, rank, local):
         c = C.retaining_wall(nx=s["nx"], ny=s["ny"], nz=s["nz"], dx=s["dx"], phi_c=s["phi_c"], e0=s["e0"],
                              mode=s["mode"], seed=s["seed"], name=s["name"])
         sim = LoquatSph(case=c, device=local, precision=4)
-        kinds.append(sim.autotune(2))
+        sim.autotune(2)
+        inf = sim.info()
+        kinds.append((inf.ix_kernel, inf.walk_threads, inf.integrator_threads))
         sims.append(sim)
     npm_local = sum(sim.info().npm for sim in sims)
     b = Batch(sims)
@@ -374,7 +376,8 @@ def run_batch(args, ws, rank, local):
         "dtype": "f32", "data": "synthetic (seeded generator, config-5 sweep)",
         "config": {"workload": "batched sweep", "cases": len(specs), "soil_particles_total": total_npm,
                    "cases_on_rank0": len(mine), "soil_on_rank0": npm_local,
-                   "interaction_kernel_choice_rank0": {"0": kinds.count(0), "1": kinds.count(1)},
+                   "autotuned_shapes_rank0": {f"kernel{k}/walk{w}/integ{i}": kinds.count((k, w, i))
+                                              for (k, w, i) in sorted(set(kinds))},
                    "parallelism": f"cases sharded over {ws} GPU(s), largest first"},
         "e2e": {"value": total_npm * args.steps / e2e_s, "unit": "particle-updates/s",
                 "h2d_bytes_per_step": int(sum(c.np_ * H2D_PER_PARTICLE + c.npb * H2D_PER_BOUNDARY

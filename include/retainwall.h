@@ -134,6 +134,10 @@ typedef struct rw_info {
   int32_t pad_;
   double time_max;             /* time-max of the parameter file (src/loquat_io.cu:192)          */
   double output_frequency;     /* output-frequency of the parameter file (src/loquat_io.cu:195)  */
+  int32_t ix_kernel;           /* RW_OPT_INTERACTION_KERNEL in use                               */
+  int32_t walk_threads;        /* RW_OPT_WALK_THREADS in use                                     */
+  int32_t integrator_threads;  /* RW_OPT_INTEGRATOR_THREADS in use                               */
+  int32_t pad2_;
 } rw_info;
 
 typedef struct rw_ctx rw_ctx;
@@ -162,6 +166,10 @@ enum {
                                    and an idle scan launch behind conditional nodes; 0: plain graph, every
                                    kernel launched (profilers that replay single graph kernels need it).
                                    Results do not depend on it. */
+  RW_OPT_WALK_THREADS = 8,      /* threads per block of the interaction's walk launch: 64, 128 (default), 256;
+                                   results do not depend on it */
+  RW_OPT_INTEGRATOR_THREADS = 9, /* threads per block of the predictor and corrector: 128 or 256 (default);
+                                   results do not depend on it */
   RW_OPT_CLOSURE_MAX_ERR = 7    /* learned closure: a particle keeps the network's objective rate only while
                                    its judged relative error against the exact rate is at most this
                                    (default 0.02; 0: no bound, the trust region alone decides) */
@@ -283,9 +291,11 @@ rw_status rw_batch_wall_force(rw_batch* b, int mode, int wall_id, const double* 
 /* Kept candidate lists (RW_OPT_LIST_SKIN) as they stand: out[0] = entries over all soil
  * particles, out[1] = soil particles holding a list (both 0 when none is kept). */
 rw_status rw_list_stats(rw_ctx* ctx, int64_t* out);
-/* Autotuner: times each interaction kernel (RW_OPT_INTERACTION_KERNEL 0 and 1) on this
- * case for `steps` steps (plus one capture step each; the case advances) and keeps the
- * faster; *chosen receives it. */
+/* Autotuner: times the interaction shapes (the walk kernel at 64, 128 and 256 threads
+ * per block, and the chunked kernel) and then the integrators' block size (256, 128) on
+ * this case, `steps` steps each (plus one capture step each; the case advances), and
+ * keeps the fastest; *chosen receives the interaction kernel (RW_OPT_INTERACTION_KERNEL),
+ * rw_get_info the shapes. */
 rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen);
 
 /* Allocation-free cell-key sort.  No counterpart in the reference (which sorts with

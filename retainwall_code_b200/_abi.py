@@ -14,6 +14,8 @@ OPT_WALL_FRICTION, OPT_COMPAT_CONTACT, OPT_INTERACTION_KERNEL, OPT_STRICT_FP, OP
 OPT_LIST_SKIN = 5
 OPT_GRAPH_GATES = 6
 OPT_CLOSURE_MAX_ERR = 7
+OPT_WALK_THREADS = 8
+OPT_INTEGRATOR_THREADS = 9
 
 # rw_array ids and their row shapes (columns, integer?)
 ARRAYS: Dict[str, int] = {
@@ -92,6 +94,8 @@ class Info(ct.Structure):
         ("n_search_skipped", ct.c_int32), ("n_scan_skipped", ct.c_int32), ("n_build_skipped", ct.c_int32),
         ("graph_kernels", ct.c_int32), ("search_body_kernels", ct.c_int32), ("pad_", ct.c_int32),
         ("time_max", ct.c_double), ("output_frequency", ct.c_double),
+        ("ix_kernel", ct.c_int32), ("walk_threads", ct.c_int32), ("integrator_threads", ct.c_int32),
+        ("pad2_", ct.c_int32),
     ]
 
 

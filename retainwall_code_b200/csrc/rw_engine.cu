@@ -87,6 +87,8 @@ template <class T> struct Engine final : EngineBase {
   cudaGraphExec_t gexec = nullptr;
   int g_cpar = -1;
   int ix_kernel = 0;     // 0: neighbours through L1/L2 (default); 1: chunked, shared-memory position tile
+  int walk_threads = 128;   // RW_OPT_WALK_THREADS: block size of the walk launch
+  int integ_threads = 256;  // RW_OPT_INTEGRATOR_THREADS: block size of the predictor and corrector
   bool strict_fp = false;  // interaction arithmetic: fused multiply-adds (default) or separately rounded
   int ncol = 0, max_chunks = 0;
   rw_case_params cparams{};
@@ -566,8 +568,9 @@ template <class T> struct Engine final : EngineBase {
                 if (strict_fp) k_interaction<T, true, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
                 else k_interaction<T, false, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
               });
-        if (strict_fp) k_interaction<T, true, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
-        else k_interaction<T, false, true><<<g, IX_THREADS, 0, st>>>(P, S, d_dyn, cpar);
+        const unsigned gw = nblk(n, walk_threads);
+        if (strict_fp) k_interaction<T, true, true><<<gw, walk_threads, 0, st>>>(P, S, d_dyn, cpar);
+        else k_interaction<T, false, true><<<gw, walk_threads, 0, st>>>(P, S, d_dyn, cpar);
       }
       check_launch();
     }
@@ -575,12 +578,12 @@ template <class T> struct Engine final : EngineBase {
   }
   void predictor() override {
     if (P.closure) return integrate_closure(0);
-    k_predictor<T><<<nblk(P.np, 256), 256, 0, st>>>(P, S, d_dyn);
+    k_predictor<T><<<nblk(P.np, integ_threads), integ_threads, 0, st>>>(P, S, d_dyn);
     check_launch();
   }
   void corrector() override {
     if (P.closure) return integrate_closure(1);
-    k_corrector<T><<<nblk(P.npb + P.npm0, 256), 256, 0, st>>>(P, S, d_dyn);
+    k_corrector<T><<<nblk(P.npb + P.npm0, integ_threads), integ_threads, 0, st>>>(P, S, d_dyn);
     check_launch();
   }
   // An integrator stage with the learned closure: one persistent launch, four 128-thread
@@ -911,6 +914,9 @@ template <class T> struct Engine final : EngineBase {
     o->search_body_kernels = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 2 : 0);
     o->time_max = cparams.time_max;
     o->output_frequency = cparams.output_frequency;
+    o->ix_kernel = ix_kernel;
+    o->walk_threads = walk_threads;
+    o->integrator_threads = integ_threads;
   }
 
   // Kept candidate lists: radius 2h + skin; dropped once any particle may have moved
@@ -958,6 +964,18 @@ template <class T> struct Engine final : EngineBase {
       const int was = ix_kernel;
       ix_kernel = (int)v;
       if (ix_kernel == 1 && was != 1) chunk_list();  // chunks of the current ordering
+    } else if (opt == RW_OPT_WALK_THREADS) {
+      if (v != 64.0 && v != 128.0 && v != 256.0) {
+        err = "walk threads per block must be 64, 128 or 256";
+        return RW_EINVAL;
+      }
+      walk_threads = (int)v;
+    } else if (opt == RW_OPT_INTEGRATOR_THREADS) {
+      if (v != 128.0 && v != 256.0) {
+        err = "integrator threads per block must be 128 or 256";
+        return RW_EINVAL;
+      }
+      integ_threads = (int)v;
     } else if (opt == RW_OPT_COMPAT_CONTACT) {
       if (v == 0.0) {
         err = "contact state following particles (RW_OPT_COMPAT_CONTACT=0) is not available";
@@ -1702,21 +1720,42 @@ rw_status rw_mlp_collect(rw_mlp* net, rw_ctx* ctx, int stride, const double* aug
 rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen) {
   if (steps < 1) return RW_EINVAL;
   return guarded(ctx, [&](rw::EngineBase& e) {
-    // Interaction kernel by measurement: each candidate runs one step to capture its
-    // graph and `steps` timed steps; the faster one stays selected.
-    double best = 1e300;
-    int pick = 0;
-    for (int cand = 0; cand < 2; ++cand) {
-      if (e.set_option(RW_OPT_INTERACTION_KERNEL, cand) != RW_OK) continue;
+    // Shapes by measurement: each candidate runs one step to capture its graph and
+    // `steps` timed steps; the fastest stays selected.  First the interaction (the walk
+    // kernel at 64, 128 or 256 threads per block, or the chunked kernel), then the
+    // integrators' block size.
+    auto timed = [&]() {
       e.step(1);
-      const double t = e.step_timed(steps);
+      return e.step_timed(steps);
+    };
+    const int walk_cand[4][2] = {{0, 64}, {0, 128}, {0, 256}, {1, 128}};
+    double best = 1e300;
+    int pick = 1;
+    for (int c = 0; c < 4; ++c) {
+      if (e.set_option(RW_OPT_INTERACTION_KERNEL, walk_cand[c][0]) != RW_OK ||
+          e.set_option(RW_OPT_WALK_THREADS, walk_cand[c][1]) != RW_OK)
+        continue;
+      const double t = timed();
       if (t < best) {
         best = t;
-        pick = cand;
+        pick = c;
       }
     }
-    e.set_option(RW_OPT_INTERACTION_KERNEL, pick);
-    if (chosen) *chosen = pick;
+    e.set_option(RW_OPT_INTERACTION_KERNEL, walk_cand[pick][0]);
+    e.set_option(RW_OPT_WALK_THREADS, walk_cand[pick][1]);
+    const int integ_cand[2] = {256, 128};
+    int ipick = 0;
+    best = 1e300;
+    for (int c = 0; c < 2; ++c) {
+      e.set_option(RW_OPT_INTEGRATOR_THREADS, integ_cand[c]);
+      const double t = timed();
+      if (t < best) {
+        best = t;
+        ipick = c;
+      }
+    }
+    e.set_option(RW_OPT_INTEGRATOR_THREADS, integ_cand[ipick]);
+    if (chosen) *chosen = walk_cand[pick][0];
     return RW_OK;
   });
 }

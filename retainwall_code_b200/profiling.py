@@ -1,0 +1,37 @@
+"""Every kernel of the step, launched once each, for per-kernel profiler captures.
+
+    python -m retainwall_code_b200.profiling [--nx 100] [--steps 1]
+
+Creates the retaining-wall case with a soil block of nx x 80 x 120 particles
+(nx = 100: 0.96M soil particles; the context's own first neighbour search sorts the
+particles, so the cell-list kernels run on real work), turns the step graph's
+conditional gates off, and runs `steps` whole steps as per-stage calls (the kernels of
+each stage launched directly on the context's stream), then the Shepard filter stage
+and both wall resultants."""
+from __future__ import annotations
+
+import argparse
+
+from . import LoquatSph, _abi, cases
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nx", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=1)
+    args = ap.parse_args()
+    sim = LoquatSph(case=cases.retaining_wall(nx=args.nx))
+    sim.set_option(_abi.OPT_GRAPH_GATES, 0)
+    for _ in range(args.steps):
+        sim.step_calculation()
+        sim.predictor_section()
+        sim.corrector_section()
+        sim.end_step()
+    sim.stress_regularization()
+    f0, f1 = sim.wall_force(0), sim.wall_force(1)
+    sim.synchronize()
+    print(f"steps {sim.info().step}; wall resultant {f0[0]:.6g} N (nearest wall), {f1[0]:.6g} N (strip)")
+
+
+if __name__ == "__main__":
+    main()

@@ -289,13 +289,33 @@ def test_batch_sees_options_set_after_creation():
     b.close()
 
 
-def test_autotune_picks_a_kernel():
+def test_autotune_picks_shapes():
+    """The autotuner times six shapes (walk at 64/128/256 threads, chunked kernel, then
+    integrators at 256/128 threads), three steps each, and keeps the fastest."""
     from retainwall_code_b200 import cases as C
 
     s = LoquatSph(case=C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005))
     k = s.autotune(2)
-    assert k in (0, 1)
-    assert s.info().step == 6 and s.info().device_err == 0
+    inf = s.info()
+    assert k in (0, 1) and inf.ix_kernel == k
+    assert inf.walk_threads in (64, 128, 256) and inf.integrator_threads in (128, 256)
+    assert inf.step == 18 and inf.device_err == 0
+
+
+def test_block_shapes_do_not_change_the_result(cases):
+    """Walk and integrator block sizes are launch shapes only: bit-identical states."""
+    from retainwall_code_b200 import _abi
+
+    c = cases["wall_mini"]
+    ref = LoquatSph(case=c)
+    ref.step(6)
+    for wt, it in ((64, 128), (256, 256), (128, 128)):
+        s = LoquatSph(case=c)
+        s.set_option(_abi.OPT_WALK_THREADS, wt)
+        s.set_option(_abi.OPT_INTEGRATOR_THREADS, it)
+        s.step(6)
+        for key in ("cellpos", "pospres", "velrhop", "str", "stn", "contact_var", "accad"):
+            np.testing.assert_array_equal(s.get(key), ref.get(key), err_msg=f"{wt}/{it} {key}")
 
 
 def test_periodic_wrap_matches_oracle():
