@@ -166,7 +166,7 @@ enum {
                                    and an idle scan launch behind conditional nodes; 0: plain graph, every
                                    kernel launched (profilers that replay single graph kernels need it).
                                    Results do not depend on it. */
-  RW_OPT_WALK_THREADS = 8,      /* threads per block of the interaction's walk launch: 64, 128 (default), 256;
+  RW_OPT_WALK_THREADS = 8,      /* threads per block of the interaction's walk launch: 64 or 128 (default);
                                    results do not depend on it */
   RW_OPT_INTEGRATOR_THREADS = 9, /* threads per block of the predictor and corrector: 128 or 256 (default);
                                    results do not depend on it */
@@ -291,8 +291,8 @@ rw_status rw_batch_wall_force(rw_batch* b, int mode, int wall_id, const double* 
 /* Kept candidate lists (RW_OPT_LIST_SKIN) as they stand: out[0] = entries over all soil
  * particles, out[1] = soil particles holding a list (both 0 when none is kept). */
 rw_status rw_list_stats(rw_ctx* ctx, int64_t* out);
-/* Autotuner: times the interaction shapes (the walk kernel at 64, 128 and 256 threads
- * per block, and the chunked kernel) and then the integrators' block size (256, 128) on
+/* Autotuner: times the interaction shapes (the walk kernel at 64 and 128 threads per
+ * block, and the chunked kernel) and then the integrators' block size (256, 128) on
  * this case, `steps` steps each (plus one capture step each; the case advances), and
  * keeps the fastest; *chosen receives the interaction kernel (RW_OPT_INTERACTION_KERNEL),
  * rw_get_info the shapes. */

@@ -965,8 +965,8 @@ template <class T> struct Engine final : EngineBase {
       ix_kernel = (int)v;
       if (ix_kernel == 1 && was != 1) chunk_list();  // chunks of the current ordering
     } else if (opt == RW_OPT_WALK_THREADS) {
-      if (v != 64.0 && v != 128.0 && v != 256.0) {
-        err = "walk threads per block must be 64, 128 or 256";
+      if (v != 64.0 && v != 128.0) {
+        err = "walk threads per block must be 64 or 128";
         return RW_EINVAL;
       }
       walk_threads = (int)v;
@@ -1722,16 +1722,16 @@ rw_status rw_autotune(rw_ctx* ctx, int steps, int* chosen) {
   return guarded(ctx, [&](rw::EngineBase& e) {
     // Shapes by measurement: each candidate runs one step to capture its graph and
     // `steps` timed steps; the fastest stays selected.  First the interaction (the walk
-    // kernel at 64, 128 or 256 threads per block, or the chunked kernel), then the
+    // kernel at 64 or 128 threads per block, or the chunked kernel), then the
     // integrators' block size.
     auto timed = [&]() {
       e.step(1);
       return e.step_timed(steps);
     };
-    const int walk_cand[4][2] = {{0, 64}, {0, 128}, {0, 256}, {1, 128}};
+    const int walk_cand[3][2] = {{0, 64}, {0, 128}, {1, 128}};
     double best = 1e300;
     int pick = 1;
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < 3; ++c) {
       if (e.set_option(RW_OPT_INTERACTION_KERNEL, walk_cand[c][0]) != RW_OK ||
           e.set_option(RW_OPT_WALK_THREADS, walk_cand[c][1]) != RW_OK)
         continue;

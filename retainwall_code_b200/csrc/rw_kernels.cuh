@@ -94,8 +94,9 @@ template <class T> struct DevState {
 
 // Interaction block size; capacity of a kept candidate list (entries per particle).
 constexpr int IX_THREADS = 128, IX_CAP = 96;
-// The walk launch takes 64, 128 (default) or 256 threads per block (RW_OPT_WALK_THREADS).
-constexpr int IX_WALK_MAX_THREADS = 256;
+// The walk launch takes 64 or 128 (default) threads per block (RW_OPT_WALK_THREADS); a
+// launch bound of 256 made the same code 14% slower.
+constexpr int IX_WALK_MAX_THREADS = 128;
 
 template <class T> RWD V3<T> ld3(const V4<T>* p, int i) { V4<T> v = p[i]; return {v.x, v.y, v.z}; }
 template <class T> RWD S6<T> ld6(const V4<T>* a, const V2<T>* b, int i) {
