@@ -218,7 +218,7 @@ def timed_steps(sim, steps: int, device: int):
     launched = (steps * i1.graph_kernels
                 - (i1.n_search_skipped - i0.n_search_skipped) * i1.search_body_kernels
                 - (i1.n_scan_skipped - i0.n_scan_skipped)
-                - (i1.n_build_skipped - i0.n_build_skipped))
+                - (i1.n_build_skipped - i0.n_build_skipped) * i1.build_body_kernels)
     return ms, launched, clk
 
 

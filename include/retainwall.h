@@ -131,13 +131,17 @@ typedef struct rw_info {
                                   kept lists stood)                                              */
   int32_t graph_kernels;       /* kernels of one captured step when no gated body is skipped     */
   int32_t search_body_kernels; /* kernels a skipped search does not launch                       */
-  int32_t pad_;
+  int32_t n_list_updates;      /* interactions that updated the kept lists in part: rebuilt those
+                                  next to a cell that particles entered or left, carried the
+                                  others through the section's permutation                        */
   double time_max;             /* time-max of the parameter file (src/loquat_io.cu:192)          */
   double output_frequency;     /* output-frequency of the parameter file (src/loquat_io.cu:195)  */
   int32_t ix_kernel;           /* RW_OPT_INTERACTION_KERNEL in use                               */
   int32_t walk_threads;        /* RW_OPT_WALK_THREADS in use                                     */
   int32_t integrator_threads;  /* RW_OPT_INTEGRATOR_THREADS in use                               */
-  int32_t pad2_;
+  int32_t n_lists_rebuilt;     /* soil particles' lists rebuilt by those updates                  */
+  int32_t build_body_kernels;  /* kernels a skipped list build does not launch                    */
+  int32_t pad_;
 } rw_info;
 
 typedef struct rw_ctx rw_ctx;

@@ -92,10 +92,10 @@ class Info(ct.Structure):
         ("time", ct.c_double), ("dt", ct.c_double), ("h", ct.c_double), ("dr", ct.c_double),
         ("n_sorts", ct.c_int32), ("n_list_reuse", ct.c_int32),
         ("n_search_skipped", ct.c_int32), ("n_scan_skipped", ct.c_int32), ("n_build_skipped", ct.c_int32),
-        ("graph_kernels", ct.c_int32), ("search_body_kernels", ct.c_int32), ("pad_", ct.c_int32),
+        ("graph_kernels", ct.c_int32), ("search_body_kernels", ct.c_int32), ("n_list_updates", ct.c_int32),
         ("time_max", ct.c_double), ("output_frequency", ct.c_double),
         ("ix_kernel", ct.c_int32), ("walk_threads", ct.c_int32), ("integrator_threads", ct.c_int32),
-        ("pad2_", ct.c_int32),
+        ("n_lists_rebuilt", ct.c_int32), ("build_body_kernels", ct.c_int32), ("pad_", ct.c_int32),
     ]
 
 

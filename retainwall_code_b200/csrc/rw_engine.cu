@@ -355,15 +355,23 @@ template <class T> struct Engine final : EngineBase {
       S.near_wall = reinterpret_cast<unsigned char*>(dalloc<unsigned>(near_wall_words));
       S.chunks = dalloc<Chunk>(max_chunks);
       S.nbg_stride = (int)(np - npb);
-      if ((size_t)IX_CAP * (np - npb) < ((size_t)1 << 31)) {  // list indices stay 32-bit
-        S.nbg = dalloc<unsigned>((size_t)IX_CAP * (np - npb));
-        S.nbg_cnt = dalloc<int>(np - npb);
+      // kept candidate lists, two buffers each (a list update after a permutation reads
+      // one and writes the other), their displacement bounds, and the marked cells
+      for (int b = 0; b < 2; ++b) {
+        if (lists_fit()) {  // list indices stay 32-bit
+          S.nbg[b] = dalloc<unsigned>((size_t)IX_CAP * (np - npb));
+          S.nbg_cnt[b] = dalloc<int>(np - npb);
+        }
+        S.dacc[b] = dalloc<float>(np);
+        if (npb > 0 && (size_t)IX_CAP * npb < ((size_t)1 << 31)) {  // boundary lists (Adami)
+          S.nbb[b] = dalloc<unsigned>((size_t)IX_CAP * npb);
+          S.nbb_cnt[b] = dalloc<int>(npb);
+        }
       }
-      S.dacc = dalloc<float>(np);
-      if (npb > 0 && (size_t)IX_CAP * npb < ((size_t)1 << 31)) {  // boundary lists (Adami)
-        S.nbb = dalloc<unsigned>((size_t)IX_CAP * npb);
-        S.nbb_cnt = dalloc<int>(npb);
-      }
+      S.inv = dalloc<int>(np);
+      S.cell_mark = dalloc<unsigned>(P.ncell_material);
+      S.marks = dalloc<int>(RW_MARK_CAP);
+      S.near_mark = reinterpret_cast<unsigned char*>(dalloc<unsigned>(near_wall_words));
       tab = dalloc<HypoC<T>>(kModelMax);
       d_clstats = dalloc<double>(4);
       d_count = dalloc<unsigned long long>(1);
@@ -396,8 +404,8 @@ template <class T> struct Engine final : EngineBase {
       const size_t raw = b_codes + 3 * b4 + 2 * b6 + b_nrm;
       unsigned char* stage = nullptr;
       bool temp = false;
-      if (S.nbg && (size_t)IX_CAP * (np - npb) * sizeof(unsigned) >= raw) {
-        stage = reinterpret_cast<unsigned char*>(S.nbg);
+      if (S.nbg[0] && (size_t)IX_CAP * (np - npb) * sizeof(unsigned) >= raw) {
+        stage = reinterpret_cast<unsigned char*>(S.nbg[0]);
       } else {
         RW_CU(cudaMalloc(reinterpret_cast<void**>(&stage), raw));
         temp = true;
@@ -512,6 +520,8 @@ template <class T> struct Engine final : EngineBase {
               k_clear_if<<<nsm, 256, 0, st>>>(reinterpret_cast<unsigned*>(S.near_wall), near_wall_words, dirty);
               k_mark_near_wall<T><<<nblk(P.npb, 256), 256, 0, st>>>(P, S, d_dyn);
             }
+            // cells next to the cells particles entered or left, for a list update
+            k_mark_dilate<T><<<nsm, 256, 0, st>>>(P, S, d_dyn);
           });
     k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
     if (ix_kernel == 1) chunk_list();
@@ -562,7 +572,10 @@ template <class T> struct Engine final : EngineBase {
         // the list build (only when the lists are to be rebuilt), the scan launch (only
         // for particles without a list, and deleted slots), then the walk
         gated([&](cudaGraphConditionalHandle h) { k_build_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
-              [&] { k_build_lists<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn); });
+              [&] {
+                k_build_lists<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn);
+                k_mark_clear<T><<<1, 1024, 0, st>>>(P, S, d_dyn);
+              });
         gated([&](cudaGraphConditionalHandle h) { k_scan_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
               [&] {
                 if (strict_fp) k_interaction<T, true, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
@@ -652,13 +665,13 @@ template <class T> struct Engine final : EngineBase {
   }
   void list_totals(long long* out) override {
     out[0] = out[1] = 0;
-    if (!S.nbg) return;
+    if (!S.nbg[0]) return;
     Dyn<T> d = dyn_host();
     if (!d.list_ok) return;
     unsigned long long* tot = nullptr;
     RW_CU(cudaMallocAsync((void**)&tot, 2 * sizeof(unsigned long long), st));
     RW_CU(cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), st));
-    k_list_totals<<<2 * nsm, 256, 0, st>>>(S.nbg_cnt, d.npm, tot);
+    k_list_totals<<<2 * nsm, 256, 0, st>>>(S.nbg_cnt[d.lbuf], d.npm, tot);
     unsigned long long h[2] = {0, 0};
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, st);
@@ -764,10 +777,10 @@ template <class T> struct Engine final : EngineBase {
 
   // Kernels launched by one whole step (launch_step), for launch accounting.
   int kernels_per_step() const {
-    // keys, check, sort, ranges, count, permute, flip, contact-wall cells, chunks
-    // keys, check, sort, clear + ranges, count, permute, [clear + near-wall marks], flip, [chunks]
-    const int search = 2 + 3 * S.sort_passes + 5 + (P.npb > 0 ? 2 : 0) + (ncol > 0 && ix_kernel == 1 ? 3 : 0);
-    const int ix = ix_kernel == 1 ? 1 : 3;             // chunked, or list build + scan + walk
+    // keys, check, sort, clear + ranges, count, permute, [clear + near-wall marks], mark
+    // dilation, flip, [chunks]
+    const int search = 2 + 3 * S.sort_passes + 6 + (P.npb > 0 ? 2 : 0) + (ncol > 0 && ix_kernel == 1 ? 3 : 0);
+    const int ix = ix_kernel == 1 ? 1 : 4;  // chunked, or list build + mark clear + scan + walk
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
     if (P.stress_shepard_filter != 0) k += 2;
@@ -911,7 +924,10 @@ template <class T> struct Engine final : EngineBase {
     // plus one gate per search and two per interaction (list build, scan launch)
     const bool ix_gates = ix_kernel == 0 && P.np > P.npb;
     o->graph_kernels = kernels_per_step() + (graph_cond ? 2 + (ix_gates ? 4 : 0) : 0);
-    o->search_body_kernels = 2 + 3 * S.sort_passes + 4 + (P.npb > 0 ? 2 : 0);
+    o->search_body_kernels = 2 + 3 * S.sort_passes + 5 + (P.npb > 0 ? 2 : 0);
+    o->build_body_kernels = 2;
+    o->n_list_updates = d.n_updates;
+    o->n_lists_rebuilt = d.n_rebuilt;
     o->time_max = cparams.time_max;
     o->output_frequency = cparams.output_frequency;
     o->ix_kernel = ix_kernel;
@@ -919,14 +935,15 @@ template <class T> struct Engine final : EngineBase {
     o->integrator_threads = integ_threads;
   }
 
-  // Kept candidate lists: radius 2h + skin; dropped once any particle may have moved
-  // 0.45 skin since they were built (two particles then close in by at most 0.9 skin,
-  // so every pair within 2h is still listed).
+  bool lists_fit() const { return (size_t)IX_CAP * (size_t)(P.np - P.npb) < ((size_t)1 << 31); }
+  // Kept candidate lists: radius 2h + skin; all rebuilt once any particle may have moved
+  // 0.45 skin since the last full build (two particles then close in by at most 0.9
+  // skin, so every pair within 2h is still listed by a list built since).
   void set_skin(double skin_h) {
     const double h_d = (double)P.h;
     const double skin = skin_h * h_d;
     const double rlist = (2.0 * h_d + skin) * (1.0 + 1e-4);
-    P.keep_lists = skin_h > 0.0 ? 1 : 0;
+    P.keep_lists = (skin_h > 0.0 && lists_fit()) ? 1 : 0;
     P.r2_list = (T)(rlist * rlist);
     P.disp_lim = (float)(0.45 * skin);
     P.disp_eps = (float)(std::ldexp(2.0 * h_d, -20));

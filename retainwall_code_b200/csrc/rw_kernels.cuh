@@ -81,16 +81,26 @@ template <class T> struct DevState {
   int* col_cnt;
   int* col_off;
   struct Chunk* chunks;
-  // Candidate lists of the soil particles (entry e of soil slot t at nbg[e * nbg_stride + t],
-  // encoded like the shared-memory lists), count per slot (-1: not kept).
-  unsigned* nbg;
-  int* nbg_cnt;
+  // Candidate lists of the soil particles (entry e of soil slot t at nbg[b][e * nbg_stride + t],
+  // encoded like the shared-memory lists), count per slot (-1: not kept).  Two buffers
+  // b, Dyn::lbuf the live one: a list update after a permutation reads the other.
+  unsigned* nbg[2];
+  int* nbg_cnt[2];
   int nbg_stride;
-  float* dacc;    // per slot: bound on the distance moved since the lists were built (not permuted)
-  unsigned* nbb;  // boundary particles' kept lists (entry e of particle i at nbb[e * npb + i])
-  int* nbb_cnt;
+  // Per particle: bound on the distance moved since the last full build of the lists
+  // (permuted with the particles, into the other buffer).
+  float* dacc[2];
+  unsigned* nbb[2];  // boundary particles' kept lists (entry e of particle i at nbb[b][e * npb + i])
+  int* nbb_cnt[2];
+  int* inv;          // inverse of the last permutation: new index of old index j
+  unsigned* cell_mark;        // per cell: marked since the last list update (listed in marks)
+  int* marks;                 // the marked cells (Dyn::n_marks of them, at most RW_MARK_CAP)
+  unsigned char* near_mark;   // per cell: a marked cell lies in its 27-cell neighbourhood
   unsigned char* near_wall;  // per cell: a contact-wall particle lies in its 27-cell neighbourhood
 };
+
+// Distinct cells one list update takes; more marked cells make it a full build.
+constexpr int RW_MARK_CAP = 8192;
 
 // Interaction block size; capacity of a kept candidate list (entries per particle).
 constexpr int IX_THREADS = 128, IX_CAP = 96;
@@ -433,6 +443,11 @@ template <class T> __global__ void k_permute(const Params<T> P, DevState<T> S, c
     S.cmp_p[n][i] = S.cmp_p[c][j];
     S.cmp_v[n][i] = S.cmp_v[c][j];
   }
+  // the lists' displacement bounds move with the particles (k_flip then flips lbuf), and
+  // a list update maps the entries through the inverse
+  const int lb = dyn->lbuf;
+  S.dacc[lb ^ 1][i] = S.dacc[lb][j];
+  S.inv[j] = i;
   const int npm = dyn->npm;
   const int nbm = P.npb + npm;
   const bool perm_str = (section == 0) || (npm != 0);
@@ -469,19 +484,29 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
     if (section == 0) dyn->cur_nrm ^= 1;
     else dyn->cur_ini ^= 1;
     dyn->n_sorts += 1;
+    dyn->lbuf ^= 1;  // k_permute carried the displacement bounds into the other buffer
   }
-  // Candidate lists: an interaction walks the kept lists when nothing was permuted and
-  // no particle changed cell or moved more than the skin allows since they were built
-  // (the integrators raise list_kill); otherwise k_build_lists builds new ones first.
-  // Lists built in the corrector section, from mid-step positions, are not kept.
+  // Candidate lists.  An interaction walks the kept lists (mode 1) when nothing was
+  // permuted and no particle changed cell since they were built or updated.  When
+  // particles changed cell (marked cells) in the step before a predictor section, the
+  // lists are updated (mode 2): the lists of particles next to a marked cell are
+  // rebuilt, the others carried through the permutation.  Every list is built anew
+  // (mode 0) when some particle moved more than the skin allows since the last full
+  // build (list_kill, raised by the integrators), after a host write, with too many
+  // marked cells, or in the corrector section: lists built there, from mid-step
+  // positions, are not kept, and a displacement bound counted from the start of the
+  // step does not cover them.
   if (section >= 0) {
     if (dyn->need_sort || dyn->host_dirty) dyn->rec_stale = 1;  // until the next interaction
     dyn->host_dirty = 0;
     dyn->cells_dirty = 0;  // the search is complete
-    const int reuse = (!dyn->need_sort && dyn->list_ok && !dyn->list_kill) ? 1 : 0;
-    dyn->ix_mode = reuse;
-    dyn->n_reuse += reuse;
-    if (!reuse) {
+    int mode = 1;
+    if (!dyn->list_ok || dyn->list_kill || dyn->n_marks > RW_MARK_CAP) mode = 0;
+    else if (dyn->need_sort || dyn->n_marks > 0) mode = section == 0 ? 2 : 0;
+    dyn->ix_mode = mode;
+    dyn->n_reuse += mode == 1;
+    dyn->n_updates += mode == 2;
+    if (mode == 0) {
       dyn->list_ok = 0;
       dyn->list_kill = 0;
       dyn->build_kill = section;
@@ -541,10 +566,10 @@ template <class T> __global__ void k_search_gate(Dyn<T>* dyn, cudaGraphCondition
   }
   cudaGraphSetConditional(h, d ? 1u : 0u);
 }
-// List build: needed when the lists are to be rebuilt (mode 0 with lists on).
+// List build: needed when the lists are to be built or updated (modes 0 and 2, lists on).
 template <class T>
 __global__ void k_build_gate(const Params<T> P, DevState<T> S, Dyn<T>* dyn, cudaGraphConditionalHandle h) {
-  const bool run = S.nbg && P.keep_lists && dyn->ix_mode == 0;
+  const bool run = S.nbg[0] && P.keep_lists && dyn->ix_mode != 1;
   if (!run) dyn->n_build_skipped += 1;
   cudaGraphSetConditional(h, run ? 1u : 0u);
 }
@@ -552,7 +577,7 @@ __global__ void k_build_gate(const Params<T> P, DevState<T> S, Dyn<T>* dyn, cuda
 // overflowed, or for deleted slots (their contact state is carried).
 template <class T>
 __global__ void k_scan_gate(const Params<T> P, DevState<T> S, Dyn<T>* dyn, cudaGraphConditionalHandle h) {
-  const bool run = !(S.nbg && P.keep_lists) || dyn->n_spill > 0 || dyn->npm < P.np - P.npb;
+  const bool run = !(S.nbg[0] && P.keep_lists) || dyn->n_spill > 0 || dyn->npm < P.np - P.npb;
   if (!run) {
     dyn->rec_stale = 0;  // what the scan launch does first
     dyn->n_scan_skipped += 1;
@@ -623,13 +648,28 @@ template <class T> RWD void period_wrap(const Params<T>& P, int4& cp, V4<T>& ps)
   ps = V4<T>{pr.x, pr.y, pr.z, ps.w};
 }
 
+// A kept list carried through a permutation: the list of old index o (column o of the
+// other buffer) becomes the list of new index i, each entry's particle index mapped to
+// its new index; the cell offsets and the order stand (a stable sort keeps the order
+// inside every cell whose particles all stayed).
+RWD void carry_list(const unsigned* __restrict__ src, const int* __restrict__ src_cnt, int o, unsigned* __restrict__ dst,
+                    int* __restrict__ dst_cnt, int i, size_t stride, const int* __restrict__ inv) {
+  constexpr unsigned kIdx = 0x7ffffffu;  // entry: particle index in the low 27 bits
+  const int cnt = src_cnt[o];
+  dst_cnt[i] = cnt;
+  for (int e = 0; e < cnt; ++e) {
+    const unsigned v = __ldcs(src + (size_t)e * stride + o);
+    __stcs(dst + (size_t)e * stride + i, (unsigned)inv[v & kIdx] | (v & ~kIdx));
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // Adami boundary (src/adami_boundary.cu:26-158).
 // ---------------------------------------------------------------------------------
 template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.npb) return;
-  if (dyn->ix_mode == 0) S.dacc[i] = 0.0f;  // candidate lists are rebuilt from these positions
+  if (dyn->ix_mode == 0) S.dacc[dyn->lbuf][i] = 0.0f;  // candidate lists are rebuilt from these positions
   if (dyn->npm == 0) return;
   const int c = dyn->cur_main;
   const V4<T>* __restrict__ pos = S.pos[c];
@@ -678,6 +718,8 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
       s = ld6(sa, sb, j);
     };
   };
+  const int lb = dyn->lbuf;
+  unsigned* __restrict__ nbb = S.nbb[lb];
   // The 27 cells in the reference's order; with `keep`, the candidates within the list
   // radius are recorded (same order) for later sections.
   auto scan = [&](const I3 cc, const V3<T> pp, bool keep) {
@@ -695,18 +737,23 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
           dr = dr - o;
           const T r2 = pair_r2(dr.x, dr.y, dr.z);
           if (keep && r2 < P.r2_list) {
-            if (cnt < IX_CAP) S.nbb[(size_t)cnt * P.npb + i] = (unsigned)j | ((unsigned)oc << 27);
+            if (cnt < IX_CAP) nbb[(size_t)cnt * P.npb + i] = (unsigned)j | ((unsigned)oc << 27);
             ++cnt;
           }
           pair(j, dr, r2, mat_of(j));
         }
       }
     }
-    if (keep) S.nbb_cnt[i] = cnt <= IX_CAP ? cnt : -1;
+    if (keep) S.nbb_cnt[lb][i] = cnt <= IX_CAP ? cnt : -1;
   };
-  const bool keep = S.nbb && P.keep_lists;
+  const bool keep = S.nbb[0] && P.keep_lists;
   const int mode = keep ? dyn->ix_mode : 0;
-  const int kept = mode == 1 ? S.nbb_cnt[i] : -1;
+  // A list update (mode 2) rebuilds the list next to a marked cell; otherwise the list
+  // stands, carried through this section's permutation when there was one.
+  const bool rebuild = mode == 0 || (mode == 2 && S.near_mark[key_of(P, celli)]);
+  if (mode == 2 && !rebuild && dyn->need_sort) carry_list(S.nbb[lb ^ 1], S.nbb_cnt[lb ^ 1], S.sperm[i], nbb,
+                                                          S.nbb_cnt[lb], i, P.npb, S.inv);
+  const int kept = (mode != 0 && !rebuild) ? S.nbb_cnt[lb][i] : -1;
   if (kept >= 0) {
     // Walk the kept list four entries at a time, each batch's neighbour data loaded
     // together and the next batch's entries loaded while it is in flight: a thread next
@@ -715,7 +762,7 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
     constexpr unsigned kNone = 0x7ffffffu;  // index of no particle (np < 2^27)
     auto entries = [&](int e0, unsigned* ent) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) ent[k] = e0 + k < kept ? __ldcs(S.nbb + (size_t)(e0 + k) * P.npb + i) : kNone;
+      for (int k = 0; k < 4; ++k) ent[k] = e0 + k < kept ? __ldcs(nbb + (size_t)(e0 + k) * P.npb + i) : kNone;
     };
     unsigned ent[4], nxt[4];
     entries(0, ent);
@@ -751,7 +798,7 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
       for (int k = 0; k < 4; ++k) ent[k] = nxt[k];
     }
   } else {
-    scan(celli, pos_i, mode == 0 && keep);
+    scan(celli, pos_i, rebuild && keep);
   }
   if (P.periodbound) {
     I3 cpb;
@@ -826,6 +873,45 @@ template <class T> __global__ void k_mark_near_wall(const Params<T> P, DevState<
   }
 }
 
+// Cells next to a marked cell (its 27-cell neighbourhood): a list update rebuilds the
+// lists of the particles in them.  Grid-stride over (marked cell, neighbour) pairs.
+template <class T> __global__ void k_mark_dilate(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
+  const int n = dyn->n_marks;
+  if (n > RW_MARK_CAP) return;  // a full build follows
+  const int ny = P.cell_num[1], nz = P.cell_num[2];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 27 * n; k += gridDim.x * blockDim.x) {
+    const int key = S.marks[k / 27];
+    const I3 off = off_of(k % 27);
+    const I3 cj{key / (ny * nz) + off.x, (key / nz) % ny + off.y, key % nz + off.z};
+    if (in_grid(P, cj)) S.near_mark[key_of(P, cj)] = 1;
+  }
+}
+
+// After a list build or update: unmark the marked cells and their neighbourhoods (every
+// cell when more were marked than listed), then empty the list.  One block, so that
+// the count is reset after every thread has read it.
+template <class T> __global__ void __launch_bounds__(1024) k_mark_clear(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
+  const int n = dyn->n_marks;
+  if (n == 0) return;
+  if (n > RW_MARK_CAP) {
+    for (int k = threadIdx.x; k < P.ncell_material; k += blockDim.x) {
+      S.cell_mark[k] = 0u;
+      S.near_mark[k] = 0;
+    }
+  } else {
+    const int ny = P.cell_num[1], nz = P.cell_num[2];
+    for (int k = threadIdx.x; k < 27 * n; k += blockDim.x) {
+      const int key = S.marks[k / 27];
+      const I3 off = off_of(k % 27);
+      const I3 cj{key / (ny * nz) + off.x, (key / nz) % ny + off.y, key % nz + off.z};
+      if (in_grid(P, cj)) S.near_mark[key_of(P, cj)] = 0;
+      if (k % 27 == 13) S.cell_mark[key] = 0u;  // offset (0, 0, 0): the cell itself
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) dyn->n_marks = 0;
+}
+
 template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
                                                                   int cpar) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -893,10 +979,10 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
   // carry j's position, velocity and contact flag in one 64-byte line; entries are read
   // four at a time and their records together, so a near-wall thread waits for two
   // loads per four entries instead of a chain of loads per entry.
-  const int kept = (S.nbg && P.keep_lists && dyn->ix_mode == 1) ? S.nbg_cnt[t] : -1;
+  const int kept = (S.nbg[0] && P.keep_lists && dyn->ix_mode == 1) ? S.nbg_cnt[dyn->lbuf][t] : -1;
   if (kept >= 0) {
     const Rec<T>* __restrict__ rec = S.rec;
-    const unsigned* __restrict__ lst = S.nbg + t;
+    const unsigned* __restrict__ lst = S.nbg[dyn->lbuf] + t;
     const size_t stride = (size_t)S.nbg_stride;
     constexpr unsigned kNone = 0x7ffffffu;  // index of no particle (np < 2^27)
     auto entries = [&](int e0, unsigned* ent) {
@@ -1288,31 +1374,46 @@ template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const Dev
   S.spin[i] = v4(skewpart(A.gv), T(0.f));
 }
 
-// Candidate lists of every live soil particle (mode 0 with lists on): the 27 cells in
-// the scan's order (cz, cy, cx; boundary range before material range; ascending j),
-// every candidate within the list radius, written column-major to HBM.  A list longer
-// than IX_CAP is marked -1 and counted (n_spill): the scan launch then takes that
-// particle.  Also starts the lists' displacement bounds.  Light (no pair arithmetic,
-// no shared-memory list), so it runs at full occupancy; the walk kernel then evaluates
-// the new lists as it does kept ones, with the same pairs in the same order as a scan.
+// Candidate lists of the live soil particles: the 27 cells in the scan's order (cz,
+// cy, cx; boundary range before material range; ascending j), every candidate within
+// the list radius, written column-major to HBM.  Mode 0 builds every list and starts
+// the displacement bounds; mode 2 (list update) rebuilds only the lists of particles
+// next to a marked cell and carries the others through the section's permutation, the
+// bounds running on from the last full build (a list built since then moved no more
+// than its particle's bound).  A list longer than IX_CAP is marked -1 and counted
+// (n_spill): the scan launch then takes that particle.  Light (no pair arithmetic, no
+// shared-memory list), so it runs at full occupancy; the walk kernel then evaluates
+// the lists with the same pairs in the same order as a scan.
 template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!S.nbg || !P.keep_lists || dyn->ix_mode != 0) return;
-  if (t == 0) {
+  const int mode = dyn->ix_mode;
+  if (!S.nbg[0] || !P.keep_lists || mode == 1) return;
+  if (t == 0 && mode == 0) {
     dyn->list_ok = 1;
     dyn->list_kill = dyn->build_kill;
   }
   if (t >= dyn->npm) return;
   const int i = P.npb + t;
-  S.dacc[i] = 0.0f;
+  const int lb = dyn->lbuf;
   const int c = dyn->cur_main;
-  const V4<T>* __restrict__ pos = S.pos[c];
   const int4 cp = S.cellpos[c][i];
   const I3 celli{cp.x, cp.y, cp.z};
+  const size_t stride = (size_t)S.nbg_stride;
+  if (mode == 2) {
+    if (!S.near_mark[key_of(P, celli)]) {
+      if (dyn->need_sort)
+        carry_list(S.nbg[lb ^ 1], S.nbg_cnt[lb ^ 1], S.sperm[i] - P.npb, S.nbg[lb], S.nbg_cnt[lb], t, stride, S.inv);
+      return;
+    }
+    const unsigned m = __activemask();
+    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&dyn->n_rebuilt, __popc(m));
+  } else {
+    S.dacc[lb][i] = 0.0f;
+  }
+  const V4<T>* __restrict__ pos = S.pos[c];
   const V3<T> pos_i = ld3(pos, i);
   const T th = P.two_h;
-  unsigned* __restrict__ out = S.nbg + t;
-  const size_t stride = (size_t)S.nbg_stride;
+  unsigned* __restrict__ out = S.nbg[lb] + t;
   int cnt = 0;
   for (int oc = 0; oc < 27; ++oc) {
     const I3 off = off_of(oc);
@@ -1335,10 +1436,10 @@ template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Pa
     }
   }
   if (cnt > IX_CAP) {
-    S.nbg_cnt[t] = -1;
+    S.nbg_cnt[lb][t] = -1;
     atomicAdd(&dyn->n_spill, 1);
   } else {
-    S.nbg_cnt[t] = cnt;
+    S.nbg_cnt[lb][t] = cnt;
   }
 }
 
@@ -1362,7 +1463,7 @@ __global__ void __launch_bounds__(Walk ? IX_WALK_MAX_THREADS : IX_THREADS, Walk 
   if (t >= total) return;
   const int i = P.npb + t;
   const int npm = dyn->npm;
-  const bool keep = S.nbg && P.keep_lists;
+  const bool keep = S.nbg[0] && P.keep_lists;
   if (Walk) {
     if (!keep || t >= npm) return;
   } else if (t >= npm) {  // deleted slots keep their contact state
@@ -1370,7 +1471,8 @@ __global__ void __launch_bounds__(Walk ? IX_WALK_MAX_THREADS : IX_THREADS, Walk 
     S.cf[cpar ^ 1][i] = S.cf[cpar][i];
     return;
   }
-  const int kept = keep ? S.nbg_cnt[t] : -1;
+  const int lb = dyn->lbuf;
+  const int kept = keep ? S.nbg_cnt[lb][t] : -1;
   if (Walk != (kept >= 0)) return;  // the other launch takes this particle
   const int c = dyn->cur_main;
   const int4 cp = S.cellpos[c][i];
@@ -1379,7 +1481,7 @@ __global__ void __launch_bounds__(Walk ? IX_WALK_MAX_THREADS : IX_THREADS, Walk 
   IState<T> I;
   Acc<T> A;
   ix_begin<Strict>(P, S, c, i, cv, I, A);
-  if (Walk) ix_list_eval<Strict, T, true>(P, S, c, I, S.nbg + t, S.nbg_stride, kept, A);
+  if (Walk) ix_list_eval<Strict, T, true>(P, S, c, I, S.nbg[lb] + t, S.nbg_stride, kept, A);
   else ix_sums_global<Strict>(P, S, c, celli, I, nbl + threadIdx.x, blockDim.x, IX_CAP, A);
   if (P.periodbound) ix_period<Strict>(P, S, c, i, celli, I, A);
   ix_finish<Strict>(P, S, c, cpar, i, celli, I, A, cv);
@@ -1696,7 +1798,7 @@ template <class T> RWD void predictor_row(const Params<T>& P, const DevState<T>&
   }
   {  // distance since the lists were built, after this half step
     const float a = (float)(f_sqrt(vr.x * vr.x + vr.y * vr.y + vr.z * vr.z) * hdt);
-    if (S.dacc[i] + a + P.disp_eps > P.disp_lim) const_cast<Dyn<T>*>(dyn)->list_kill = 1;
+    if (S.dacc[dyn->lbuf][i] + a + P.disp_eps > P.disp_lim) const_cast<Dyn<T>*>(dyn)->list_kill = 1;
   }
   const T* mp = P.model_par[code.w];
   vr.w = f_max(vr.w, mp[kMatSize - 2]);
@@ -1736,15 +1838,36 @@ template <class T> RWD I3 rebin(V4<T>& ps, T th) {
   return dc;
 }
 
-// Bookkeeping of the kept candidate lists for one particle's full step: a cell change
-// reorders its pairs and kills the lists; otherwise its distance bound grows by the
-// step (plus a rounding allowance) and must stay within the skin's share.
+// Marks a cell whose particles changed (once per cell: the first marker lists it).
+template <class T> RWD void mark_cell(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, I3 c) {
+  const int key = key_of(P, c);
+  if (atomicExch(&S.cell_mark[key], 1u) == 0u) {
+    const int k = atomicAdd(&const_cast<Dyn<T>*>(dyn)->n_marks, 1);
+    if (k < RW_MARK_CAP) S.marks[k] = key;
+  }
+}
+
+// Bookkeeping of the kept candidate lists for one particle's full step from cell `from`
+// to cell `to`.  Its distance bound grows by the step (plus a rounding allowance) and
+// must stay within the skin's share, else every list is rebuilt.  A cell change marks
+// both cells (the next list update rebuilds the lists around them); leaving the grid
+// (deletion) makes it a full build.
 template <class T> RWD void list_account(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, int i, float step,
-                                         int cell_moved) {
-  const float d = S.dacc[i] + step + P.disp_eps;
-  S.dacc[i] = d;
-  if (cell_moved) const_cast<Dyn<T>*>(dyn)->cells_dirty = 1;
-  if (cell_moved || d > P.disp_lim) const_cast<Dyn<T>*>(dyn)->list_kill = 1;
+                                         I3 from, I3 to) {
+  float* dacc = S.dacc[dyn->lbuf];
+  const float d = dacc[i] + step + P.disp_eps;
+  dacc[i] = d;
+  Dyn<T>* w = const_cast<Dyn<T>*>(dyn);
+  if (from.x != to.x || from.y != to.y || from.z != to.z) {
+    w->cells_dirty = 1;
+    if (!in_grid(P, from) || !in_grid(P, to)) {
+      w->list_kill = 1;
+    } else if (P.keep_lists) {
+      mark_cell(P, S, dyn, from);
+      mark_cell(P, S, dyn, to);
+    }
+  }
+  if (d > P.disp_lim) w->list_kill = 1;
 }
 
 // One row of the corrector (moving boundary rows and soil rows); with the learned
@@ -1776,7 +1899,8 @@ template <class T> RWD void corrector_row(const Params<T>& P, const DevState<T>&
     const I3 dc = rebin(ps, th);
     S.pos[c][i] = ps;
     S.cellpos[c][i] = int4{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z, cp.w};
-    list_account(P, S, dyn, i, (float)(f_sqrt(dot(vel, vel)) * P.dt), dc.x | dc.y | dc.z);
+    list_account(P, S, dyn, i, (float)(f_sqrt(dot(vel, vel)) * P.dt), I3{cp.x, cp.y, cp.z},
+                 I3{cp.x + dc.x, cp.y + dc.y, cp.z + dc.z});
     return;
   }
   const V4<T> vri = S.vel_ini[ci][i];
@@ -1819,7 +1943,7 @@ template <class T> RWD void corrector_row(const Params<T>& P, const DevState<T>&
   if (P.periodbound) period_wrap(P, cp, ps);
   {
     const V3<T> inc = xyz(vr + vri) * (T(0.5f) * P.dt);
-    list_account(P, S, dyn, i, (float)f_sqrt(dot(inc, inc)), (cp.x - cp0.x) | (cp.y - cp0.y) | (cp.z - cp0.z));
+    list_account(P, S, dyn, i, (float)f_sqrt(dot(inc, inc)), I3{cp0.x, cp0.y, cp0.z}, I3{cp.x, cp.y, cp.z});
   }
   S6<T> sg = ld6(S.stri_a[ci], S.stri_b[ci], i);
   const S6<T> D = ld6(S.ace_a, S.ace_b, i);

@@ -80,12 +80,19 @@ template <class T> struct Dyn {
   unsigned err;              // RW_DERR_* bits
   int step;
   int nchunks;               // live entries of the interaction chunk list
-  // Candidate lists kept across sections and steps: ix_mode 0 = build new lists (then
-  // walk them), 1 = walk the kept lists.  list_kill: some particle changed cell or
-  // moved too far since the lists were built; build_kill: lists built in this section
-  // are not to be kept (a corrector-section rebuild).
+  // Candidate lists kept across sections and steps: ix_mode 0 = build every list (then
+  // walk them), 1 = walk the kept lists, 2 = update them: rebuild the lists of the
+  // particles next to a cell that some particle entered or left (a marked cell), carry
+  // the others through the section's permutation, then walk.  list_kill: some particle
+  // moved too far since the last full build, or left the grid; build_kill: lists
+  // built in this section are not to be kept (a corrector-section rebuild).
   int ix_mode, list_ok, list_kill, build_kill;
   int n_sorts, n_reuse;      // sections that permuted / interactions that walked kept lists
+  // Marked cells since the last list update (distinct cells, listed in DevState::marks;
+  // more than RW_MARK_CAP: the next update is a full build).  lbuf: which of the two
+  // list / displacement-bound buffers is live (it flips with every permutation).
+  int n_marks, lbuf;
+  int n_updates, n_rebuilt;  // interactions that updated the lists / lists rebuilt by them
   // Soil neighbour records: the integrators rewrite them; the corner search rewrites
   // them after a permutation or a host write (rec_stale: set by the search, cleared by
   // the interaction that follows).
