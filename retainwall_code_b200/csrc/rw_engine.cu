@@ -369,9 +369,10 @@ template <class T> struct Engine final : EngineBase {
         }
       }
       S.inv = dalloc<int>(np);
+      S.queue = dalloc<int>(np - npb + 1);
       S.cell_mark = dalloc<unsigned>(P.ncell_material);
       S.marks = dalloc<int>(RW_MARK_CAP);
-      S.near_mark = reinterpret_cast<unsigned char*>(dalloc<unsigned>(near_wall_words));
+      S.near_mark = dalloc<unsigned>(P.ncell_material);
       tab = dalloc<HypoC<T>>(kModelMax);
       d_clstats = dalloc<double>(4);
       d_count = dalloc<unsigned long long>(1);
@@ -435,6 +436,7 @@ template <class T> struct Engine final : EngineBase {
 
     Dyn<T> d;
     std::memset(&d, 0, sizeof(d));
+    d.mark_gen = 1;  // cell marks start at generation 0: unmarked
     d.time_d = q.time;
     d.time_f = (T)q.time;
     d.npm = q.npm;
@@ -478,7 +480,7 @@ template <class T> struct Engine final : EngineBase {
                                (int)sizeof(Ix2Smem<T>)));
     RW_CU(cudaFuncSetAttribute(k_interaction2<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(Ix2Smem<T>)));
-    neighbor_search(0);
+    search(0);  // the first cell sort; the lists are built with the first step's boundary stage
     RW_CU(cudaStreamSynchronize(st));
   }
 
@@ -493,7 +495,23 @@ template <class T> struct Engine final : EngineBase {
     k_end<T><<<1, 1, 0, st>>>(P, d_dyn);
     check_launch();
   }
+  // The search, then the candidate lists, built or updated (only when they do not
+  // stand), before the boundary and corner stages so that the corner search walks them.
   void neighbor_search(int section) override {
+    search(section);
+    if (lists_kept()) {
+      const int n = P.np - P.npb;
+      gated([&](cudaGraphConditionalHandle h) { k_build_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
+            [&] {
+              k_build_lists<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn);
+              k_rebuild_lists<T><<<2 * nsm, 256, 0, st>>>(P, S, d_dyn);
+            });
+      check_launch();
+    }
+  }
+  // Soil candidate lists are kept only with the walk kernels.
+  bool lists_kept() const { return ix_kernel == 0 && P.np > P.npb && S.nbg[0] && P.keep_lists; }
+  void search(int section) {
     // Every kernel of the search returns at once when no particle changed cell since
     // the last one (Dyn::cells_dirty): keys, order, ranges and counts then stand.
     gated([&](cudaGraphConditionalHandle h) { k_search_gate<T><<<1, 1, 0, st>>>(d_dyn, h); },
@@ -523,7 +541,7 @@ template <class T> struct Engine final : EngineBase {
             // cells next to the cells particles entered or left, for a list update
             k_mark_dilate<T><<<nsm, 256, 0, st>>>(P, S, d_dyn);
           });
-    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0);
+    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, section, 0, lists_kept() ? 1 : 0);
     if (ix_kernel == 1) chunk_list();
     check_launch();
   }
@@ -539,7 +557,7 @@ template <class T> struct Engine final : EngineBase {
   }
   void rigid() override {
     if (P.n_motion <= 0) return;
-    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, -1, 1);
+    k_flip<T><<<1, 1, 0, st>>>(P, d_dyn, -1, 1, 0);
     check_launch();
   }
   void adami() override {
@@ -569,13 +587,8 @@ template <class T> struct Engine final : EngineBase {
         else k_interaction2<T, false><<<grid, IX2_TB, sizeof(Ix2Smem<T>), st>>>(P, S, d_dyn, cpar);
       } else {
         const unsigned g = nblk(n, IX_THREADS);
-        // the list build (only when the lists are to be rebuilt), the scan launch (only
-        // for particles without a list, and deleted slots), then the walk
-        gated([&](cudaGraphConditionalHandle h) { k_build_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
-              [&] {
-                k_build_lists<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn);
-                k_mark_clear<T><<<1, 1024, 0, st>>>(P, S, d_dyn);
-              });
+        // the scan launch (only for particles without a list, and deleted slots), then
+        // the walk (the lists were built or updated at the end of the search)
         gated([&](cudaGraphConditionalHandle h) { k_scan_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
               [&] {
                 if (strict_fp) k_interaction<T, true, false><<<g, IX_THREADS, sm1, st>>>(P, S, d_dyn, cpar);
@@ -780,7 +793,8 @@ template <class T> struct Engine final : EngineBase {
     // keys, check, sort, clear + ranges, count, permute, [clear + near-wall marks], mark
     // dilation, flip, [chunks]
     const int search = 2 + 3 * S.sort_passes + 6 + (P.npb > 0 ? 2 : 0) + (ncol > 0 && ix_kernel == 1 ? 3 : 0);
-    const int ix = ix_kernel == 1 ? 1 : 4;  // chunked, or list build + mark clear + scan + walk
+    // chunked, or [list build + rebuild (end of the search)] + scan + walk
+    const int ix = ix_kernel == 1 ? 1 : (lists_kept() ? 4 : 2);
     int k = 1 + 2 * search + 2 * (2 + ix) + 1 + 1 + 1;  // begin, 2 searches, 2x(adami, corner, interaction), predictor, corrector, end
     if (P.n_motion > 0) k += 1;
     if (P.stress_shepard_filter != 0) k += 2;
@@ -922,8 +936,8 @@ template <class T> struct Engine final : EngineBase {
     o->n_build_skipped = d.n_build_skipped;
     // kernels of the captured step graph when every gated body runs: the plain step
     // plus one gate per search and two per interaction (list build, scan launch)
-    const bool ix_gates = ix_kernel == 0 && P.np > P.npb;
-    o->graph_kernels = kernels_per_step() + (graph_cond ? 2 + (ix_gates ? 4 : 0) : 0);
+    const int ix_gates = ix_kernel == 0 && P.np > P.npb ? (lists_kept() ? 4 : 2) : 0;
+    o->graph_kernels = kernels_per_step() + (graph_cond ? 2 + ix_gates : 0);
     o->search_body_kernels = 2 + 3 * S.sort_passes + 5 + (P.npb > 0 ? 2 : 0);
     o->build_body_kernels = 2;
     o->n_list_updates = d.n_updates;

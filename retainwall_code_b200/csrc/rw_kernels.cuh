@@ -93,9 +93,10 @@ template <class T> struct DevState {
   unsigned* nbb[2];  // boundary particles' kept lists (entry e of particle i at nbb[b][e * npb + i])
   int* nbb_cnt[2];
   int* inv;          // inverse of the last permutation: new index of old index j
-  unsigned* cell_mark;        // per cell: marked since the last list update (listed in marks)
-  int* marks;                 // the marked cells (Dyn::n_marks of them, at most RW_MARK_CAP)
-  unsigned char* near_mark;   // per cell: a marked cell lies in its 27-cell neighbourhood
+  int* queue;        // soil slots whose lists a list update rebuilds (Dyn::n_queue of them)
+  unsigned* cell_mark;  // per cell: generation of its last mark (listed in marks when first marked)
+  int* marks;           // the cells marked in the current generation (Dyn::n_marks, at most RW_MARK_CAP)
+  unsigned* near_mark;  // per cell: generation of the last mark in its 27-cell neighbourhood
   unsigned char* near_wall;  // per cell: a contact-wall particle lies in its 27-cell neighbourhood
 };
 
@@ -478,7 +479,7 @@ template <class T> __global__ void k_permute(const Params<T> P, DevState<T> S, c
 // Buffer flip after a permute; in the predictor section also RigidBodyUpdate
 // (src/adami_boundary.cu:175-203), which the reference runs right after the sort.
 // Plain round-to-nearest products/sums, as the reference's host code computes.
-template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int section, int rigid) {
+template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int section, int rigid, int lists) {
   if (section >= 0 && dyn->need_sort) {
     dyn->cur_main ^= 1;
     if (section == 0) dyn->cur_nrm ^= 1;
@@ -495,17 +496,23 @@ template <class T> __global__ void k_flip(const Params<T> P, Dyn<T>* dyn, int se
   // build (list_kill, raised by the integrators), after a host write, with too many
   // marked cells, or in the corrector section: lists built there, from mid-step
   // positions, are not kept, and a displacement bound counted from the start of the
-  // step does not cover them.
+  // step does not cover them.  Without kept soil lists (lists = 0: lists off, or the
+  // chunked kernel) every section is mode 0 and no list stands.
   if (section >= 0) {
     if (dyn->need_sort || dyn->host_dirty) dyn->rec_stale = 1;  // until the next interaction
     dyn->host_dirty = 0;
     dyn->cells_dirty = 0;  // the search is complete
     int mode = 1;
-    if (!dyn->list_ok || dyn->list_kill || dyn->n_marks > RW_MARK_CAP) mode = 0;
+    if (!lists || !dyn->list_ok || dyn->list_kill || dyn->n_marks > RW_MARK_CAP) mode = 0;
     else if (dyn->need_sort || dyn->n_marks > 0) mode = section == 0 ? 2 : 0;
     dyn->ix_mode = mode;
     dyn->n_reuse += mode == 1;
     dyn->n_updates += mode == 2;
+    // the marks are consumed: the update tests this generation, new marks take the next
+    dyn->near_gen = dyn->mark_gen;
+    dyn->mark_gen += 1;
+    dyn->n_marks = 0;
+    dyn->n_queue = 0;
     if (mode == 0) {
       dyn->list_ok = 0;
       dyn->list_kill = 0;
@@ -657,9 +664,18 @@ RWD void carry_list(const unsigned* __restrict__ src, const int* __restrict__ sr
   constexpr unsigned kIdx = 0x7ffffffu;  // entry: particle index in the low 27 bits
   const int cnt = src_cnt[o];
   dst_cnt[i] = cnt;
-  for (int e = 0; e < cnt; ++e) {
-    const unsigned v = __ldcs(src + (size_t)e * stride + o);
-    __stcs(dst + (size_t)e * stride + i, (unsigned)inv[v & kIdx] | (v & ~kIdx));
+  // eight entries at a time, their loads and index lookups issued together (a thread
+  // waits for two loads per eight entries, not two per entry)
+  for (int e0 = 0; e0 < cnt; e0 += 8) {
+    unsigned v[8];
+    int m[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = e0 + k < cnt ? __ldcs(src + (size_t)(e0 + k) * stride + o) : 0u;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) m[k] = e0 + k < cnt ? inv[v[k] & kIdx] : 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (e0 + k < cnt) __stcs(dst + (size_t)(e0 + k) * stride + i, (unsigned)m[k] | (v[k] & ~kIdx));
   }
 }
 
@@ -750,7 +766,7 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
   const int mode = keep ? dyn->ix_mode : 0;
   // A list update (mode 2) rebuilds the list next to a marked cell; otherwise the list
   // stands, carried through this section's permutation when there was one.
-  const bool rebuild = mode == 0 || (mode == 2 && S.near_mark[key_of(P, celli)]);
+  const bool rebuild = mode == 0 || (mode == 2 && S.near_mark[key_of(P, celli)] == dyn->near_gen);
   if (mode == 2 && !rebuild && dyn->need_sort) carry_list(S.nbb[lb ^ 1], S.nbb_cnt[lb ^ 1], S.sperm[i], nbb,
                                                           S.nbb_cnt[lb], i, P.npb, S.inv);
   const int kept = (mode != 0 && !rebuild) ? S.nbb_cnt[lb][i] : -1;
@@ -873,43 +889,20 @@ template <class T> __global__ void k_mark_near_wall(const Params<T> P, DevState<
   }
 }
 
-// Cells next to a marked cell (its 27-cell neighbourhood): a list update rebuilds the
-// lists of the particles in them.  Grid-stride over (marked cell, neighbour) pairs.
+// Cells next to a marked cell (its 27-cell neighbourhood), tagged with the current
+// mark generation: a list update rebuilds the lists of the particles in them.
+// Grid-stride over (marked cell, neighbour) pairs.
 template <class T> __global__ void k_mark_dilate(const Params<T> P, DevState<T> S, const Dyn<T>* dyn) {
   const int n = dyn->n_marks;
   if (n > RW_MARK_CAP) return;  // a full build follows
+  const unsigned gen = dyn->mark_gen;
   const int ny = P.cell_num[1], nz = P.cell_num[2];
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 27 * n; k += gridDim.x * blockDim.x) {
     const int key = S.marks[k / 27];
     const I3 off = off_of(k % 27);
     const I3 cj{key / (ny * nz) + off.x, (key / nz) % ny + off.y, key % nz + off.z};
-    if (in_grid(P, cj)) S.near_mark[key_of(P, cj)] = 1;
+    if (in_grid(P, cj)) S.near_mark[key_of(P, cj)] = gen;
   }
-}
-
-// After a list build or update: unmark the marked cells and their neighbourhoods (every
-// cell when more were marked than listed), then empty the list.  One block, so that
-// the count is reset after every thread has read it.
-template <class T> __global__ void __launch_bounds__(1024) k_mark_clear(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
-  const int n = dyn->n_marks;
-  if (n == 0) return;
-  if (n > RW_MARK_CAP) {
-    for (int k = threadIdx.x; k < P.ncell_material; k += blockDim.x) {
-      S.cell_mark[k] = 0u;
-      S.near_mark[k] = 0;
-    }
-  } else {
-    const int ny = P.cell_num[1], nz = P.cell_num[2];
-    for (int k = threadIdx.x; k < 27 * n; k += blockDim.x) {
-      const int key = S.marks[k / 27];
-      const I3 off = off_of(k % 27);
-      const I3 cj{key / (ny * nz) + off.x, (key / nz) % ny + off.y, key % nz + off.z};
-      if (in_grid(P, cj)) S.near_mark[key_of(P, cj)] = 0;
-      if (k % 27 == 13) S.cell_mark[key] = 0u;  // offset (0, 0, 0): the cell itself
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) dyn->n_marks = 0;
 }
 
 template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<T> P, DevState<T> S, const Dyn<T>* dyn,
@@ -971,15 +964,16 @@ template <class T> __global__ void __launch_bounds__(128) k_corner(const Params<
     }
     cv.x += f_abs((ny.x * gker.x + ny.y * gker.y + ny.z * gker.z) * P.vol_def);
   };
-  // When this section's interaction walks the kept lists, they hold every boundary
-  // particle within 2h of i in the scan's order (per cell offset, the boundary range
-  // first, ascending index): walking their boundary entries visits the same candidates
-  // that pass the q < 2 test, in the same order, without the boundary cells' full ranges.
-  // The boundary neighbour records (written by the Adami kernel earlier in the section)
-  // carry j's position, velocity and contact flag in one 64-byte line; entries are read
-  // four at a time and their records together, so a near-wall thread waits for two
-  // loads per four entries instead of a chain of loads per entry.
-  const int kept = (S.nbg[0] && P.keep_lists && dyn->ix_mode == 1) ? S.nbg_cnt[dyn->lbuf][t] : -1;
+  // The candidate lists, current once the search has built, updated or kept them
+  // (list_ok), hold every boundary particle within 2h of i in the scan's order (per cell
+  // offset, the boundary range first, ascending index): walking their boundary entries
+  // visits the same candidates that pass the q < 2 test, in the same order, without the
+  // boundary cells' full ranges.  The boundary neighbour records (written by the Adami
+  // kernel earlier in the section) carry j's position, velocity and contact flag in one
+  // 64-byte line; entries are read four at a time and their records together, so a
+  // near-wall thread waits for two loads per four entries instead of a chain of loads
+  // per entry.
+  const int kept = (S.nbg[0] && P.keep_lists && dyn->list_ok) ? S.nbg_cnt[dyn->lbuf][t] : -1;
   if (kept >= 0) {
     const Rec<T>* __restrict__ rec = S.rec;
     const unsigned* __restrict__ lst = S.nbg[dyn->lbuf] + t;
@@ -1400,16 +1394,22 @@ template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Pa
   const I3 celli{cp.x, cp.y, cp.z};
   const size_t stride = (size_t)S.nbg_stride;
   if (mode == 2) {
-    if (!S.near_mark[key_of(P, celli)]) {
+    if (S.near_mark[key_of(P, celli)] != dyn->near_gen) {
       if (dyn->need_sort)
         carry_list(S.nbg[lb ^ 1], S.nbg_cnt[lb ^ 1], S.sperm[i] - P.npb, S.nbg[lb], S.nbg_cnt[lb], t, stride, S.inv);
       return;
     }
+    // next to a marked cell: queued for k_rebuild_lists (one warp per list), so that
+    // the few lists an update rebuilds do not wait on one thread's 27-cell scan each
     const unsigned m = __activemask();
-    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&dyn->n_rebuilt, __popc(m));
-  } else {
-    S.dacc[lb][i] = 0.0f;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&dyn->n_queue, __popc(m));
+    base = __shfl_sync(m, base, leader);
+    S.queue[base + __popc(m & ((1u << lane) - 1u))] = t;
+    return;
   }
+  S.dacc[lb][i] = 0.0f;
   const V4<T>* __restrict__ pos = S.pos[c];
   const V3<T> pos_i = ld3(pos, i);
   const T th = P.two_h;
@@ -1440,6 +1440,106 @@ template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Pa
     atomicAdd(&dyn->n_spill, 1);
   } else {
     S.nbg_cnt[lb][t] = cnt;
+  }
+}
+
+// The lists queued by a list update, one warp per list: the 27 cells x 2 ranges are 54
+// segments of candidates, flattened in the scan's order; the warp tests 32 consecutive
+// candidates at a time and appends the hits in order (ballot + prefix count), so the
+// list equals the one k_build_lists writes.  The displacement bounds run on.
+template <class T> __global__ void __launch_bounds__(256) k_rebuild_lists(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
+  constexpr int kSeg = 54, kWarps = 256 / 32;
+  __shared__ int seg_beg[kWarps][kSeg + 1];  // first flattened candidate of each segment
+  __shared__ int seg_j0[kWarps][kSeg];       // first particle index of each segment
+  if (!S.nbg[0] || !P.keep_lists || dyn->ix_mode != 2) return;
+  const int nq = dyn->n_queue;
+  if (blockIdx.x == 0 && threadIdx.x == 0) dyn->n_rebuilt += nq;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lb = dyn->lbuf, c = dyn->cur_main;
+  const V4<T>* __restrict__ pos = S.pos[c];
+  const size_t stride = (size_t)S.nbg_stride;
+  const T th = P.two_h;
+  int* beg = seg_beg[warp];
+  int* j0 = seg_j0[warp];
+  for (int q = blockIdx.x * kWarps + warp; q < nq; q += gridDim.x * kWarps) {
+    const int t = S.queue[q];
+    const int i = P.npb + t;
+    const int4 cp = S.cellpos[c][i];
+    const I3 celli{cp.x, cp.y, cp.z};
+    const V3<T> pos_i = ld3(pos, i);
+    int size[2], first[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int sg = lane + 32 * h;
+      size[h] = 0;
+      first[h] = 0;
+      if (sg < kSeg) {
+        const I3 off = off_of(sg >> 1);
+        const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
+        if (in_grid(P, cj)) {
+          const int k = key_of(P, cj);
+          const int2 rg = S.range[(sg & 1) ? k + P.ncell_material : k];
+          size[h] = rg.y - rg.x;
+          first[h] = rg.x;
+        }
+      }
+    }
+    int inc0 = size[0], inc1 = size[1];  // inclusive prefix sums over the lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int a = __shfl_up_sync(0xffffffffu, inc0, d), b = __shfl_up_sync(0xffffffffu, inc1, d);
+      if (lane >= d) {
+        inc0 += a;
+        inc1 += b;
+      }
+    }
+    const int tot0 = __shfl_sync(0xffffffffu, inc0, 31);
+    const int total = tot0 + __shfl_sync(0xffffffffu, inc1, 31);
+    beg[lane] = inc0 - size[0];
+    j0[lane] = first[0];
+    if (lane + 32 < kSeg) {
+      beg[lane + 32] = tot0 + inc1 - size[1];
+      j0[lane + 32] = first[1];
+    }
+    if (lane == 0) beg[kSeg] = total;
+    __syncwarp();
+    unsigned* __restrict__ out = S.nbg[lb] + t;
+    int cnt = 0;
+    for (int b0 = 0; b0 < total; b0 += 32) {
+      const int ci = b0 + lane;
+      bool hit = false;
+      unsigned ent = 0u;
+      if (ci < total) {
+        int lo = 0, hi = kSeg;  // the last segment starting at or before ci (it is not empty)
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (beg[mid] <= ci) lo = mid;
+          else hi = mid;
+        }
+        const int j = j0[lo] + (ci - beg[lo]);
+        const int oc = lo >> 1;
+        const V3<T> pmo = pos_i - mulI(off_of(oc), th);
+        const V4<T> pj = pos[j];
+        const T dx = pmo.x - pj.x, dy = pmo.y - pj.y, dz = pmo.z - pj.z;
+        hit = dx * dx + dy * dy + dz * dz < P.r2_list;
+        ent = (unsigned)j | ((unsigned)oc << 27);
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const int e = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (e < IX_CAP) __stcs(out + (size_t)e * stride, ent);
+      }
+      cnt += __popc(bal);
+    }
+    if (lane == 0) {
+      if (cnt > IX_CAP) {
+        S.nbg_cnt[lb][t] = -1;
+        atomicAdd(&dyn->n_spill, 1);
+      } else {
+        S.nbg_cnt[lb][t] = cnt;
+      }
+    }
+    __syncwarp();  // before the next list overwrites the segment table
   }
 }
 
@@ -1838,10 +1938,11 @@ template <class T> RWD I3 rebin(V4<T>& ps, T th) {
   return dc;
 }
 
-// Marks a cell whose particles changed (once per cell: the first marker lists it).
+// Marks a cell whose particles changed (once per generation: the first marker lists it).
 template <class T> RWD void mark_cell(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, I3 c) {
   const int key = key_of(P, c);
-  if (atomicExch(&S.cell_mark[key], 1u) == 0u) {
+  const unsigned gen = dyn->mark_gen;
+  if (atomicExch(&S.cell_mark[key], gen) != gen) {
     const int k = atomicAdd(&const_cast<Dyn<T>*>(dyn)->n_marks, 1);
     if (k < RW_MARK_CAP) S.marks[k] = key;
   }

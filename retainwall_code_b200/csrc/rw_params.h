@@ -89,10 +89,15 @@ template <class T> struct Dyn {
   int ix_mode, list_ok, list_kill, build_kill;
   int n_sorts, n_reuse;      // sections that permuted / interactions that walked kept lists
   // Marked cells since the last list update (distinct cells, listed in DevState::marks;
-  // more than RW_MARK_CAP: the next update is a full build).  lbuf: which of the two
-  // list / displacement-bound buffers is live (it flips with every permutation).
+  // more than RW_MARK_CAP: the next update is a full build).  Marks carry a generation
+  // number instead of being cleared: mark_gen is the one the integrators mark with,
+  // near_gen the one a list update tests (k_flip hands mark_gen over and advances it).
+  // lbuf: which of the two list / displacement-bound buffers is live (it flips with
+  // every permutation).
   int n_marks, lbuf;
+  unsigned mark_gen, near_gen;
   int n_updates, n_rebuilt;  // interactions that updated the lists / lists rebuilt by them
+  int n_queue;               // lists queued for rebuilding by the current update
   // Soil neighbour records: the integrators rewrite them; the corner search rewrites
   // them after a permutation or a host write (rec_stale: set by the search, cleared by
   // the interaction that follows).

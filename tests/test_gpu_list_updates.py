@@ -34,10 +34,13 @@ def _passive_wall():
 
 
 def _run_with_updates(case, steps, every, skin):
-    """Steps one at a time with list updates on, a lists-off twin and a chunked-kernel
-    twin; compares the three at every `every` steps and returns per-step counters."""
+    """Steps one at a time with list updates on (list skin `skin`), a twin with every
+    option at its default (skin 0.02 h, set at creation), a lists-off twin and a
+    chunked-kernel twin; compares the four at every `every` steps and returns per-step
+    counters of the first."""
     s = LoquatSph(case=case)
     s.set_option(_abi.OPT_LIST_SKIN, skin)
+    dflt = LoquatSph(case=case)
     scan = LoquatSph(case=case)
     scan.set_option(_abi.OPT_LIST_SKIN, 0.0)
     chunk = LoquatSph(case=case)
@@ -45,9 +48,8 @@ def _run_with_updates(case, steps, every, skin):
     rows = []
     prev = s.info()
     for k in range(1, steps + 1):
-        s.step(1)
-        scan.step(1)
-        chunk.step(1)
+        for x in (s, dflt, scan, chunk):
+            x.step(1)
         cur = s.info()
         rows.append((cur.n_sorts - prev.n_sorts, cur.n_list_updates - prev.n_list_updates,
                      cur.n_lists_rebuilt - prev.n_lists_rebuilt))
@@ -55,9 +57,11 @@ def _run_with_updates(case, steps, every, skin):
         if k % every == 0 or k == steps:
             for key in KEYS:
                 a = s.get(key)
+                np.testing.assert_array_equal(a, dflt.get(key), err_msg=f"step {k} {key} vs default skin")
                 np.testing.assert_array_equal(a, scan.get(key), err_msg=f"step {k} {key} vs scan")
                 np.testing.assert_array_equal(a, chunk.get(key), err_msg=f"step {k} {key} vs chunked")
-    assert s.info().device_err == 0 and scan.info().device_err == 0
+    assert all(x.info().device_err == 0 for x in (s, dflt, scan, chunk))
+    assert np.isfinite(s.get("pospres")).all()
     return s, np.array(rows)
 
 
