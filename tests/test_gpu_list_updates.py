@@ -94,8 +94,9 @@ def test_passive_wall_list_updates_equal_scans():
 
 
 def test_list_updates_gated_graph_equals_plain_graph():
-    """The mark dilation sits in the gated search body and the mark clearing in the
-    gated list build: the gated graph equals the plain one (every kernel launched)."""
+    """The mark dilation sits in the gated search body and the rebuild of the lists next
+    to marked cells in the gated list build: the gated graph equals the plain one (every
+    kernel launched)."""
     case = _column()
     g = LoquatSph(case=case)
     p = LoquatSph(case=case)
