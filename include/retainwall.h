@@ -139,7 +139,7 @@ typedef struct rw_info {
   int32_t ix_kernel;           /* RW_OPT_INTERACTION_KERNEL in use                               */
   int32_t walk_threads;        /* RW_OPT_WALK_THREADS in use                                     */
   int32_t integrator_threads;  /* RW_OPT_INTEGRATOR_THREADS in use                               */
-  int32_t n_lists_rebuilt;     /* soil particles' lists rebuilt by those updates                  */
+  int32_t n_lists_rebuilt;     /* candidate lists (soil and boundary) rebuilt by those updates    */
   int32_t build_body_kernels;  /* kernels a skipped list build does not launch                    */
   int32_t pad_;
 } rw_info;

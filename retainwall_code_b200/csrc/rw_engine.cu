@@ -369,7 +369,7 @@ template <class T> struct Engine final : EngineBase {
         }
       }
       S.inv = dalloc<int>(np);
-      S.queue = dalloc<int>(np - npb + 1);
+      S.queue = dalloc<int>(np + 1);
       S.cell_mark = dalloc<unsigned>(P.ncell_material);
       S.marks = dalloc<int>(RW_MARK_CAP);
       S.near_mark = dalloc<unsigned>(P.ncell_material);
@@ -500,11 +500,10 @@ template <class T> struct Engine final : EngineBase {
   void neighbor_search(int section) override {
     search(section);
     if (lists_kept()) {
-      const int n = P.np - P.npb;
       gated([&](cudaGraphConditionalHandle h) { k_build_gate<T><<<1, 1, 0, st>>>(P, S, d_dyn, h); },
             [&] {
-              k_build_lists<T><<<nblk(n, 256), 256, 0, st>>>(P, S, d_dyn);
-              k_rebuild_lists<T><<<2 * nsm, 256, 0, st>>>(P, S, d_dyn);
+              k_build_lists<T><<<nblk(P.np, 256), 256, 0, st>>>(P, S, d_dyn);
+              k_rebuild_lists<T><<<4 * nsm, 256, 0, st>>>(P, S, d_dyn);
             });
       check_launch();
     }

@@ -93,7 +93,7 @@ template <class T> struct DevState {
   unsigned* nbb[2];  // boundary particles' kept lists (entry e of particle i at nbb[b][e * npb + i])
   int* nbb_cnt[2];
   int* inv;          // inverse of the last permutation: new index of old index j
-  int* queue;        // soil slots whose lists a list update rebuilds (Dyn::n_queue of them)
+  int* queue;        // rows whose lists a list update rebuilds (Dyn::n_queue of them)
   unsigned* cell_mark;  // per cell: generation of its last mark (listed in marks when first marked)
   int* marks;           // the cells marked in the current generation (Dyn::n_marks, at most RW_MARK_CAP)
   unsigned* near_mark;  // per cell: generation of the last mark in its 27-cell neighbourhood
@@ -655,6 +655,13 @@ template <class T> RWD void period_wrap(const Params<T>& P, int4& cp, V4<T>& ps)
   ps = V4<T>{pr.x, pr.y, pr.z, ps.w};
 }
 
+// A list update rebuilds the list of a particle in cell c when c lies next to a cell
+// marked in the generation being consumed; a cell outside the grid (a wall particle
+// moved out of it) always counts as marked.
+template <class T> RWD bool near_marked(const Params<T>& P, const DevState<T>& S, const Dyn<T>* dyn, I3 c) {
+  return !in_grid(P, c) || S.near_mark[key_of(P, c)] == dyn->near_gen;
+}
+
 // A kept list carried through a permutation: the list of old index o (column o of the
 // other buffer) becomes the list of new index i, each entry's particle index mapped to
 // its new index; the cell offsets and the order stand (a stable sort keeps the order
@@ -764,11 +771,10 @@ template <class T> __global__ void __launch_bounds__(128) k_adami(const Params<T
   };
   const bool keep = S.nbb[0] && P.keep_lists;
   const int mode = keep ? dyn->ix_mode : 0;
-  // A list update (mode 2) rebuilds the list next to a marked cell; otherwise the list
-  // stands, carried through this section's permutation when there was one.
-  const bool rebuild = mode == 0 || (mode == 2 && S.near_mark[key_of(P, celli)] == dyn->near_gen);
-  if (mode == 2 && !rebuild && dyn->need_sort) carry_list(S.nbb[lb ^ 1], S.nbb_cnt[lb ^ 1], S.sperm[i], nbb,
-                                                          S.nbb_cnt[lb], i, P.npb, S.inv);
+  // In a list update (mode 2) the lists next to a marked cell were rebuilt and the
+  // others carried through this section's permutation, if any, before this kernel
+  // (k_build_lists, k_rebuild_lists); only a full build (mode 0) keeps them here.
+  const bool rebuild = mode == 0;
   const int kept = (mode != 0 && !rebuild) ? S.nbb_cnt[lb][i] : -1;
   if (kept >= 0) {
     // Walk the kept list four entries at a time, each batch's neighbour data loaded
@@ -1377,36 +1383,52 @@ template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const Dev
 // than its particle's bound).  A list longer than IX_CAP is marked -1 and counted
 // (n_spill): the scan launch then takes that particle.  Light (no pair arithmetic, no
 // shared-memory list), so it runs at full occupancy; the walk kernel then evaluates
-// the lists with the same pairs in the same order as a scan.
+// the lists with the same pairs in the same order as a scan.  One thread per particle,
+// boundary rows first: in an update after a permutation the boundary rows carry their
+// Adami lists too (the Adami kernel, which holds many registers and runs few warps,
+// only rebuilds the ones next to a marked cell).
 template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   const int mode = dyn->ix_mode;
   if (!S.nbg[0] || !P.keep_lists || mode == 1) return;
-  if (t == 0 && mode == 0) {
+  if (row == 0 && mode == 0) {
     dyn->list_ok = 1;
     dyn->list_kill = dyn->build_kill;
   }
-  if (t >= dyn->npm) return;
-  const int i = P.npb + t;
   const int lb = dyn->lbuf;
   const int c = dyn->cur_main;
-  const int4 cp = S.cellpos[c][i];
-  const I3 celli{cp.x, cp.y, cp.z};
-  const size_t stride = (size_t)S.nbg_stride;
-  if (mode == 2) {
-    if (S.near_mark[key_of(P, celli)] != dyn->near_gen) {
-      if (dyn->need_sort)
-        carry_list(S.nbg[lb ^ 1], S.nbg_cnt[lb ^ 1], S.sperm[i] - P.npb, S.nbg[lb], S.nbg_cnt[lb], t, stride, S.inv);
-      return;
-    }
-    // next to a marked cell: queued for k_rebuild_lists (one warp per list), so that
-    // the few lists an update rebuilds do not wait on one thread's 27-cell scan each
+  // queues a row whose list k_rebuild_lists rebuilds (one warp per list), so that the
+  // few lists an update rebuilds do not each wait on one thread's 27-cell scan
+  auto enqueue = [&] {
     const unsigned m = __activemask();
     const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
     int base = 0;
     if (lane == leader) base = atomicAdd(&dyn->n_queue, __popc(m));
     base = __shfl_sync(m, base, leader);
-    S.queue[base + __popc(m & ((1u << lane) - 1u))] = t;
+    S.queue[base + __popc(m & ((1u << lane) - 1u))] = row;
+  };
+  if (row < P.npb) {
+    if (mode == 2 && S.nbb[0]) {
+      const int4 cb = S.cellpos[c][row];
+      if (near_marked(P, S, dyn, I3{cb.x, cb.y, cb.z})) enqueue();
+      else if (dyn->need_sort)
+        carry_list(S.nbb[lb ^ 1], S.nbb_cnt[lb ^ 1], S.sperm[row], S.nbb[lb], S.nbb_cnt[lb], row, P.npb, S.inv);
+    }
+    return;
+  }
+  const int t = row - P.npb;
+  if (t >= dyn->npm) return;
+  const int i = row;
+  const int4 cp = S.cellpos[c][i];
+  const I3 celli{cp.x, cp.y, cp.z};
+  const size_t stride = (size_t)S.nbg_stride;
+  if (mode == 2) {
+    if (!near_marked(P, S, dyn, celli)) {
+      if (dyn->need_sort)
+        carry_list(S.nbg[lb ^ 1], S.nbg_cnt[lb ^ 1], S.sperm[i] - P.npb, S.nbg[lb], S.nbg_cnt[lb], t, stride, S.inv);
+      return;
+    }
+    enqueue();  // next to a marked cell
     return;
   }
   S.dacc[lb][i] = 0.0f;
@@ -1443,10 +1465,11 @@ template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Pa
   }
 }
 
-// The lists queued by a list update, one warp per list: the 27 cells x 2 ranges are 54
-// segments of candidates, flattened in the scan's order; the warp tests 32 consecutive
-// candidates at a time and appends the hits in order (ballot + prefix count), so the
-// list equals the one k_build_lists writes.  The displacement bounds run on.
+// The lists queued by a list update (soil rows' interaction lists and boundary rows'
+// Adami lists), one warp per list: the 27 cells x 2 ranges are 54 segments of
+// candidates, flattened in the scan's order; the warp tests 32 consecutive candidates
+// at a time and appends the hits in order (ballot + prefix count), so the list holds
+// the pairs a full build lists, in the same order.  The displacement bounds run on.
 template <class T> __global__ void __launch_bounds__(256) k_rebuild_lists(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
   constexpr int kSeg = 54, kWarps = 256 / 32;
   __shared__ int seg_beg[kWarps][kSeg + 1];  // first flattened candidate of each segment
@@ -1457,13 +1480,15 @@ template <class T> __global__ void __launch_bounds__(256) k_rebuild_lists(const 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lb = dyn->lbuf, c = dyn->cur_main;
   const V4<T>* __restrict__ pos = S.pos[c];
-  const size_t stride = (size_t)S.nbg_stride;
   const T th = P.two_h;
   int* beg = seg_beg[warp];
   int* j0 = seg_j0[warp];
   for (int q = blockIdx.x * kWarps + warp; q < nq; q += gridDim.x * kWarps) {
-    const int t = S.queue[q];
-    const int i = P.npb + t;
+    // a soil row's list, or a boundary row's Adami list (without the boundary ranges
+    // unless the particle belongs to a contact wall, as the Adami scan keeps it)
+    const int i = S.queue[q];
+    const bool bnd = i < P.npb;
+    const bool with_bnd_range = !bnd || S.codes[c][i].x >= 10;
     const int4 cp = S.cellpos[c][i];
     const I3 celli{cp.x, cp.y, cp.z};
     const V3<T> pos_i = ld3(pos, i);
@@ -1473,7 +1498,7 @@ template <class T> __global__ void __launch_bounds__(256) k_rebuild_lists(const 
       const int sg = lane + 32 * h;
       size[h] = 0;
       first[h] = 0;
-      if (sg < kSeg) {
+      if (sg < kSeg && ((sg & 1) || with_bnd_range)) {
         const I3 off = off_of(sg >> 1);
         const I3 cj{celli.x + off.x, celli.y + off.y, celli.z + off.z};
         if (in_grid(P, cj)) {
@@ -1503,7 +1528,9 @@ template <class T> __global__ void __launch_bounds__(256) k_rebuild_lists(const 
     }
     if (lane == 0) beg[kSeg] = total;
     __syncwarp();
-    unsigned* __restrict__ out = S.nbg[lb] + t;
+    const size_t stride = bnd ? (size_t)P.npb : (size_t)S.nbg_stride;
+    unsigned* __restrict__ out = bnd ? S.nbb[lb] + i : S.nbg[lb] + (i - P.npb);
+    int* __restrict__ count = bnd ? S.nbb_cnt[lb] + i : S.nbg_cnt[lb] + (i - P.npb);
     int cnt = 0;
     for (int b0 = 0; b0 < total; b0 += 32) {
       const int ci = b0 + lane;
@@ -1532,12 +1559,8 @@ template <class T> __global__ void __launch_bounds__(256) k_rebuild_lists(const 
       cnt += __popc(bal);
     }
     if (lane == 0) {
-      if (cnt > IX_CAP) {
-        S.nbg_cnt[lb][t] = -1;
-        atomicAdd(&dyn->n_spill, 1);
-      } else {
-        S.nbg_cnt[lb][t] = cnt;
-      }
+      *count = cnt > IX_CAP ? -1 : cnt;  // an overflowed boundary list: Adami scans for it
+      if (cnt > IX_CAP && !bnd) atomicAdd(&dyn->n_spill, 1);
     }
     __syncwarp();  // before the next list overwrites the segment table
   }

@@ -8,9 +8,12 @@ particles, so the cell-list kernels run on real work), turns the step graph's
 conditional gates off, and runs `steps` whole steps as per-stage calls (the kernels of
 each stage launched directly on the context's stream), then the Shepard filter stage
 and both wall resultants.  With --vx the soil starts moving along +x at that speed
-(m/s): at 0.05 m/s a few dozen particles change cell in the first step, so the second
-step's predictor section updates the candidate lists after a sort (mark dilation, list
-carry, rebuilds next to the marked cells), as the long run does once the wall moves."""
+(m/s), its block moved by dx/10 along x first: the generator's lattice keeps every
+particle at least 0.05 dx from every cell face, and the shift brings a band of
+particles up to the x faces.  At 0.05 m/s about 150 particles change cell in the first
+step, so the second step's predictor section updates the candidate lists after a sort
+(mark dilation, list carry, rebuilds next to the marked cells), as the long run does
+once the wall has moved the soil."""
 from __future__ import annotations
 
 import argparse
@@ -26,6 +29,7 @@ def main() -> None:
     args = ap.parse_args()
     case = cases.retaining_wall(nx=args.nx)
     if args.vx:
+        case.pospres[case.npb:, 0] += 0.1 * case.params["dr"]
         case.velrhop[case.npb:, 0] = args.vx
     sim = LoquatSph(case=case)
     sim.set_option(_abi.OPT_GRAPH_GATES, 0)

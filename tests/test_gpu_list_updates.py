@@ -75,12 +75,12 @@ def test_column_collapse_list_updates_equal_scans():
     inf = s.info()
     assert updates.sum() >= 20, updates.sum()
     assert ((sorts > 0) & (updates > 0)).sum() >= 5  # updates that carried lists through a sort
-    # the updates rebuilt a part of the lists, not all of them
-    assert 0 < rebuilt.sum() < 0.8 * updates.sum() * inf.npm
+    # the updates rebuilt a part of the lists (soil and boundary), not all of them
+    assert 0 < rebuilt.sum() < 0.8 * updates.sum() * inf.np
     full = 2 * inf.step - inf.n_build_skipped - inf.n_list_updates
     assert full < updates.sum()
     print(f"column: {updates.sum()} updates ({((sorts > 0) & (updates > 0)).sum()} after a sort), "
-          f"{full} full builds, {rebuilt.sum() / max(updates.sum(), 1):.0f} of {inf.npm} lists rebuilt per update")
+          f"{full} full builds, {rebuilt.sum() / max(updates.sum(), 1):.0f} of {inf.np} lists rebuilt per update")
 
 
 def test_passive_wall_list_updates_equal_scans():
