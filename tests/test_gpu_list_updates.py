@@ -125,3 +125,28 @@ def test_list_updates_under_the_default_skin_fp64():
     for key in KEYS:
         np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
     assert a.info().n_list_updates > 0 and a.info().device_err == 0
+
+
+def test_too_many_marked_cells_make_a_full_build():
+    """More than 8192 cells marked in one step (the capacity of the marked-cell list) turn
+    the next update into a full build.  A 384k-particle wall whose soil block is moved
+    onto the cell faces (dx/10 along x: the generator's lattice otherwise keeps every
+    particle 0.05 dx from them) and thrown at 10 m/s: in each step about 7,500 particles
+    change cell.  The run equals the lists-off run bit for bit, and its interactions
+    rebuilt every list instead of updating them."""
+    c = C.retaining_wall(nx=40, ny=80, nz=120, name="burst")
+    c.pospres[c.npb:, 0] += 0.1 * c.params["dr"]
+    c.velrhop[c.npb:, 0] = 10.0
+    a = LoquatSph(case=c)
+    a.set_option(_abi.OPT_LIST_SKIN, 1.0)
+    b = LoquatSph(case=c)
+    b.set_option(_abi.OPT_LIST_SKIN, 0.0)
+    for _ in range(3):
+        a.step(1)
+        b.step(1)
+    for key in KEYS:
+        np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
+    inf = a.info()
+    full = 2 * inf.step - inf.n_build_skipped - inf.n_list_updates
+    assert inf.n_sorts >= 3 and full >= 3, (inf.n_sorts, full, inf.n_list_updates)
+    assert inf.device_err == 0
