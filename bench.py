@@ -395,8 +395,10 @@ def run_batch_forms(args, ws, rank, local):
     """The three forms together on the batched sweep: the 64 cases advanced in one graph
     launch per step with the precision form (compensated integration, FP64 norms) and the
     learned closure (trained as in the closure workload), against the same batch in plain
-    FP32.  value = aggregate particle-updates/s of the combined form; each case's wall
-    resultant after the timed steps is compared with its plain run."""
+    FP32.  value = aggregate particle-updates/s of the combined form.  Each case's wall
+    resultant after the timed steps (averaged over 50 further steps) is compared with its
+    plain FP32 run and, together with the plain run's, with an FP64 run of the same batch
+    (the FP64 step is pinned to the oracle's double-precision restatement)."""
     import numpy as np
 
     from retainwall_code_b200 import Batch, LoquatSph, _abi, cases as C
@@ -408,10 +410,10 @@ def run_batch_forms(args, ws, rank, local):
                               mode=s["mode"], seed=s["seed"], name=s["name"]) for s in mine]
     net, training = train_closure(args, local) if args.batch_forms != "precision" else (None, None)
     res = {}
-    for form in ("plain", "forms"):
+    for form in ("plain", "forms", "f64"):
         sims = []
         for c in cases:
-            sim = LoquatSph(case=c, device=local, precision=4)
+            sim = LoquatSph(case=c, device=local, precision=8 if form == "f64" else 4)
             if form == "forms":
                 if args.batch_forms in ("both", "precision"):
                     sim.set_option(_abi.OPT_MIXED_PRECISION, 1)
@@ -442,9 +444,11 @@ def run_batch_forms(args, ws, rank, local):
     total_npm = sum(s["nx"] * s["ny"] * s["nz"] for s in specs)
     value = total_npm * args.steps / (res["forms"]["ms"] * 1e-3)
     plain = total_npm * args.steps / (res["plain"]["ms"] * 1e-3)
-    fp, ff = res["plain"]["forces"], res["forms"]["forces"]
+    fp, ff, fd = res["plain"]["forces"], res["forms"]["forces"], res["f64"]["forces"]
     scale = np.maximum(np.abs(fp), 1e-9)
     rel = np.abs(ff - fp) / scale
+    scale64 = np.maximum(np.abs(fd), 1e-9)
+    rel64 = {"forms": np.abs(ff - fd) / scale64, "plain": np.abs(fp - fd) / scale64}
     offered = sum(st["offered"] for st in res["forms"]["stats"])
     used = sum(st["used"] for st in res["forms"]["stats"])
     judged = [st["mean_rel_err"] for st in res["forms"]["stats"] if st["used"] > 0]
@@ -463,11 +467,17 @@ def run_batch_forms(args, ws, rank, local):
                                      "cases_within_1pct": int((rel <= 0.01).sum()), "cases": int(len(rel)),
                                      "per_case": [[s["mode"], s["nx"] * s["ny"] * s["nz"], float(a), float(b)]
                                                   for s, a, b in zip(mine, fp, ff)]},
+        "wall_force_vs_fp64": {"averaged_over_steps": 50, "f64_ms_per_step": res["f64"]["ms"] / args.steps,
+                               **{k: {"max_rel": float(v.max()), "median_rel": float(np.median(v)),
+                                      "cases_within_1pct": int((v <= 0.01).sum()),
+                                      "cases_within_half_pct": int((v <= 0.005).sum())}
+                                  for k, v in rel64.items()},
+                               "per_case_f64": [float(x) for x in fd]},
         "closure": {"offered": offered, "used": used, "used_share": used / max(offered, 1),
                     "mean_judged_rel_err_over_cases": float(np.mean(judged)) if judged else None},
         "training": training,
         "clocks": res["forms"]["clocks"],
-        "device_err": max(res["forms"]["err"], res["plain"]["err"]),
+        "device_err": max(res["forms"]["err"], res["plain"]["err"], res["f64"]["err"]),
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
