@@ -341,6 +341,12 @@ def run_batch(args, ws, rank, local):
     total_npm = sum(s["nx"] * s["ny"] * s["nz"] for s in specs)
     value = total_npm * args.steps / (ms * 1e-3)
     infos = [sim.info() for sim in sims]
+    npb_local = sum(i.npb for i in infos)
+    # per particle the step advances (soil and boundary): smaller cases carry more wall
+    # and floor per soil particle, which the soil-only metric does not see
+    per_particle = {"soil_rank0": npm_local, "boundary_rank0": npb_local,
+                    "ns_per_soil_particle": ms / args.steps * 1e6 / max(npm_local, 1) if ws == 1 else None,
+                    "ns_per_particle": ms / args.steps * 1e6 / max(npm_local + npb_local, 1) if ws == 1 else None}
     lists = {"sections_that_sorted": sum(i.n_sorts for i in infos),
              "interactions_on_kept_lists": sum(i.n_list_reuse for i in infos),
              "interactions": sum(2 * i.step for i in infos),
@@ -385,6 +391,7 @@ def run_batch(args, ws, rank, local):
                 "d2h_bytes_per_step": 24 * len(mine),
                 "note": "upload of every case from pinned host arrays + batched steps + one wall-force read per step (rank 0)"},
         "candidate_lists_rank0": lists,
+        "per_particle": per_particle,
         "clocks": clk.summary(),
     }
     if rank == 0:
