@@ -2146,7 +2146,52 @@ template <class T> __global__ void __launch_bounds__(128) k_shepard(const Params
       }
     }
   };
-  scan(celli, pos_i);
+  // Inside the step (only_filter_steps) the filter runs after the corner search, where
+  // the candidate lists are current (built, updated or kept at the end of the search)
+  // and so are the neighbour records.  A list holds every material neighbour within
+  // 2h in the scan's order (per cell offset, ascending index): walking its material
+  // entries, with position, density and volume from the records, visits the same pairs
+  // in the same order.  Entries four at a time, their data loaded together.
+  const int kept = (only_filter_steps && S.nbg[0] && P.keep_lists && dyn->list_ok) ? S.nbg_cnt[dyn->lbuf][t] : -1;
+  if (kept >= 0) {
+    const Rec<T>* __restrict__ rec = S.rec;
+    const unsigned* __restrict__ lst = S.nbg[dyn->lbuf] + t;
+    const size_t stride = (size_t)S.nbg_stride;
+    constexpr unsigned kNone = 0x7ffffffu;
+    for (int e0 = 0; e0 < kept; e0 += 4) {
+      unsigned ent[4];
+      NbVals<T> nb[4];
+      S6<T> sj[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) ent[k] = e0 + k < kept ? __ldcs(lst + (size_t)(e0 + k) * stride) : kNone;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int j = (int)(ent[k] & kNone);
+        if (j == (int)kNone || j < P.npb) continue;
+        nb[k] = load_nb(rec, j);
+        sj[k] = ld6(S.str_a[c], S.str_b[c], j);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int j = (int)(ent[k] & kNone);
+        if (j == (int)kNone || j < P.npb) continue;
+        V3<T> dr = pos_i - V3<T>{nb[k].p.x, nb[k].p.y, nb[k].p.z};
+        dr = dr - mulI(off_of((int)(ent[k] >> 27)), th);
+        const T r2 = pair_r2(dr.x, dr.y, dr.z);
+        if (!(r2 < P.r2_prefilter)) continue;
+        T r = pair_r(r2);
+        T q = r * P.i_h;
+        if (q < T(2.0f)) {
+          T ker = kernel_w(P.knorm, q);
+          T vol = f_abs(nb[k].a.y);  // mass / density, as the record stores it
+          sumker += ker * vol;
+          sh = sh + sj[k] * (ker * vol);
+        }
+      }
+    }
+  } else {
+    scan(celli, pos_i);
+  }
   if (P.periodbound) {
     I3 cpb;
     V3<T> ppb;

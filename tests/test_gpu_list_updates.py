@@ -150,3 +150,28 @@ def test_too_many_marked_cells_make_a_full_build():
     full = 2 * inf.step - inf.n_build_skipped - inf.n_list_updates
     assert inf.n_sorts >= 3 and full >= 3, (inf.n_sorts, full, inf.n_list_updates)
     assert inf.device_err == 0
+
+
+@pytest.mark.parametrize("every", [1, 3])
+def test_shepard_filter_on_lists_equals_scan(every):
+    """The Shepard stress filter inside the step (src/field_smoothing.cu:26-101, applied
+    every `stress-shepard-filter` steps) walks the candidate lists when they are kept:
+    the moving column with the filter on equals the runs that filter by scanning the
+    cells (list skin 0, chunked kernel), bit for bit, through cell changes and list
+    updates."""
+    case = _column()
+    case.params["stress_shepard_filter"] = every
+    runs = {}
+    for name, opt in (("lists", None), ("scan", (_abi.OPT_LIST_SKIN, 0.0)), ("chunk", (_abi.OPT_INTERACTION_KERNEL, 1))):
+        s = LoquatSph(case=case)
+        if opt:
+            s.set_option(*opt)
+        s.step(120)
+        runs[name] = s
+    plain = LoquatSph(case=_column())
+    plain.step(120)
+    for key in KEYS:
+        np.testing.assert_array_equal(runs["lists"].get(key), runs["scan"].get(key), err_msg=key)
+        np.testing.assert_array_equal(runs["lists"].get(key), runs["chunk"].get(key), err_msg=key)
+    assert not np.array_equal(runs["lists"].get("str"), plain.get("str"))  # the filter acted
+    assert runs["lists"].info().n_list_updates > 0 and runs["lists"].info().device_err == 0
