@@ -4,7 +4,7 @@ Default workload: the 1.92M-particle translating retaining wall (soil block 200x
 at dx = 2.5 mm, 262,500 Adami/contact boundary particles, FP32), synthetic seeded
 inputs from retainwall_code_b200.cases.retaining_wall.  A step is one whole
 StepCalculation + PredictorSection + CorrectorSection (src/loquat.cu:548-561), replayed
-from a captured CUDA graph; the state (~1.6 GB) is larger than L2, so no flush is needed.
+from a captured CUDA graph; the state (~3.6 GB) is larger than L2, so no flush is needed.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload wall2|wall2_half|col1|batch64|batch64_forms|closure] [--precision-report]
@@ -586,7 +586,7 @@ def run_ours(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
         "config": dict(cfg, parallelism=f"replicas x{ws}", np=inf.np, npb=inf.npb, ncell=inf.ncell,
-                       l2="state 1.6 GB > L2: no flush needed"),
+                       l2="device state 3.6 GB (double-buffered candidate lists included) > L2 (126 MB): no flush needed"),
         "e2e": {"value": e2e, "unit": "particle-updates/s", "h2d_bytes_per_step": int(h2d / e2e_steps),
                 "d2h_bytes_per_step": 24, "note": "case upload from pinned host arrays + per-step rw_step + wall-force read"},
         "roofline": roof,
