@@ -163,9 +163,12 @@ enum {
                                    stepping. */
   RW_OPT_LIST_SKIN = 5,         /* skin of the kept candidate lists, in units of h (default 0.02; 0 = scan
                                    the cells in every interaction).  The interaction keeps each particle's
-                                   candidates within 2h + skin and walks them instead of the 27 cells until
-                                   a sort permutes, a particle changes cell, or a particle may have moved
-                                   0.45 skin; results do not depend on it. */
+                                   candidates within 2h + skin and walks them instead of the 27 cells.
+                                   After particles change cell, the next predictor section rebuilds only
+                                   the lists next to the cells they entered or left and carries the others
+                                   through the sort's permutation; every list is rebuilt once a particle
+                                   may have moved 0.45 skin since the last full build.  Results do not
+                                   depend on it. */
   RW_OPT_GRAPH_GATES = 6,       /* 1 (default): the captured step graph skips a search with no cell change
                                    and an idle scan launch behind conditional nodes; 0: plain graph, every
                                    kernel launched (profilers that replay single graph kernels need it).
