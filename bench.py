@@ -599,7 +599,9 @@ def run_ours(args, ws, rank, local):
         "clocks": clocks,
     }
     # ---- the same case over a long window from step 0: sorts and list rebuilds included --
-    if rank == 0 and args.amortized_steps > 0:
+    # (a property of one case on one GPU: single-GPU runs only, so that a multi-GPU run
+    # does not hold every GPU while rank 0 runs it)
+    if rank == 0 and ws == 1 and args.amortized_steps > 0:
         sim3 = LoquatSph(case=case, device=local, precision=4)
         with ClockSampler(local) as clk3:
             ms3 = sim3.step_timed(args.amortized_steps)
