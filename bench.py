@@ -75,12 +75,13 @@ def make_case(workload: str):
     if workload == "wall2":
         return C.retaining_wall(), {"workload": "retaining wall, active translation 1 mm/s",
                                     "soil": "200x80x120", "dx_m": 0.0025, "npm": 1920000,
-                                    "wall_friction": "tan(2/3 phi_c)"}
+                                    "wall_friction": "tan(2/3 phi_c)", "trajectory_steps": 20000}
     if workload == "wall2_half":  # half-length block, for profiler captures
         return C.retaining_wall(nx=100), {"workload": "retaining wall (half length)", "soil": "100x80x120",
-                                          "dx_m": 0.0025, "npm": 960000}
+                                          "dx_m": 0.0025, "npm": 960000, "trajectory_steps": 20000}
     if workload == "col1":
-        return C.column_collapse(), {"workload": "column collapse", "soil": "24x24x48", "dx_m": 0.005, "npm": 27648}
+        return C.column_collapse(), {"workload": "column collapse", "soil": "24x24x48", "dx_m": 0.005, "npm": 27648,
+                                     "trajectory_steps": 2000}
     raise SystemExit(f"unknown workload {workload}")
 
 
@@ -251,18 +252,20 @@ def cpu_sample(case, threads: int, steps: int, precision: int = 4):
     return npm * steps / dt, dt, t_init
 
 
-def reference_cuda_sample(case, steps: int, warmup: int, device: int):
-    """The reference's own CUDA build (oracle/_ref/ref_driver_f32, built from the reference's
-    sources) on the same case files and the same GPU: its step loop timed with CUDA events
-    by the driver, clocks sampled meanwhile.  The reference hard-codes the wall friction
-    (0.58108); the step's work does not depend on its value."""
+def reference_cuda_sample(case, steps: int, warmup: int, device: int, precision: int = 4):
+    """The reference's own CUDA build (oracle/_ref/ref_driver_f32, or ref_driver_f64 for
+    FP64, built from the reference's sources) on the same case files and the same GPU:
+    its step loop timed with CUDA events by the driver, clocks sampled meanwhile.  The
+    reference hard-codes the wall friction (0.58108); the step's work does not depend on
+    its value."""
     import tempfile
 
     from retainwall_code_b200 import cases as C
 
-    drv = os.path.join(ROOT, "oracle", "_ref", "ref_driver_f32")
+    name = "ref_driver_f64" if precision == 8 else "ref_driver_f32"
+    drv = os.path.join(ROOT, "oracle", "_ref", name)
     if not os.path.exists(drv):
-        return {"unavailable": "oracle/_ref/ref_driver_f32 not built (needs the reference sources)"}
+        return {"unavailable": f"oracle/_ref/{name} not built (needs the reference sources)"}
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     gpu = vis.split(",")[device] if vis else str(device)  # the driver runs on its device 0
     with tempfile.TemporaryDirectory() as d:
@@ -276,7 +279,7 @@ def reference_cuda_sample(case, steps: int, warmup: int, device: int):
         return {"unavailable": f"reference driver exited {r.returncode}: {r.stderr[-300:]}"}
     rec = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
     return {"value": rec["particle_updates_per_s"], "unit": "particle-updates/s", "ms_per_step": rec["ms_per_step"],
-            "steps": steps, "warmup": warmup, "npm": rec["npm"], "dtype": "f32",
+            "steps": steps, "warmup": warmup, "npm": rec["npm"], "dtype": "f64" if precision == 8 else "f32",
             "how": "unmodified reference build (sm_100a), RunSimulation's step loop, CUDA events", "clocks":
             clk.summary()}
 
@@ -498,7 +501,8 @@ def run_ours(args, ws, rank, local):
 
     case, cfg = make_case(args.workload)
     # ---- device-resident throughput ----------------------------------------------------
-    sim = LoquatSph(case=case, device=local, precision=4)
+    prec = args.precision or (8 if args.workload == "col1" else 4)  # configuration 1 is FP64
+    sim = LoquatSph(case=case, device=local, precision=prec)
     if args.ix_kernel is not None:
         sim.set_option(_abi.OPT_INTERACTION_KERNEL, args.ix_kernel)
     if args.strict:
@@ -536,7 +540,7 @@ def run_ours(args, ws, rank, local):
     host_case = pinned_case(case)
     barrier(ws)
     t0 = time.perf_counter()
-    sim2 = LoquatSph(case=host_case, device=local, precision=4)
+    sim2 = LoquatSph(case=host_case, device=local, precision=prec)
     e2e_steps = args.steps
     for _ in range(e2e_steps):
         sim2.step(1)
@@ -553,7 +557,7 @@ def run_ours(args, ws, rank, local):
     # ---- roofline of the dominant kernel ------------------------------------------------
     pk, kind = peaks()
     list_entries, list_parts = sim2_lists
-    ib = interaction_bytes(inf, inf.ncell, 4, list_entries)
+    ib = interaction_bytes(inf, inf.ncell, prec, list_entries)
     achieved = ib / (ix_ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": "k_interaction", "achieved": achieved, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "peak_source": kind,
@@ -584,9 +588,12 @@ def run_ours(args, ws, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": "particle-updates/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+        "vs_baseline": None, "dtype": "f64" if prec == 8 else "f32", "data": "synthetic (seeded generator)",
         "config": dict(cfg, parallelism=f"replicas x{ws}", np=inf.np, npb=inf.npb, ncell=inf.ncell,
-                       l2="device state 3.6 GB (double-buffered candidate lists included) > L2 (126 MB): no flush needed"),
+                       l2=("device state 3.6 GB (double-buffered candidate lists included) > L2 (126 MB): "
+                           "no flush needed") if inf.np > 1_000_000 else
+                          ("the state fits in L2 (126 MB): steps run L2-warm, as a run of this case does; "
+                           "not flushed")),
         "e2e": {"value": e2e, "unit": "particle-updates/s", "h2d_bytes_per_step": int(h2d / e2e_steps),
                 "d2h_bytes_per_step": 24, "note": "case upload from pinned host arrays + per-step rw_step + wall-force read"},
         "roofline": roof,
@@ -601,32 +608,37 @@ def run_ours(args, ws, rank, local):
     # ---- the same case over a long window from step 0: sorts and list rebuilds included --
     # (a property of one case on one GPU: single-GPU runs only, so that a multi-GPU run
     # does not hold every GPU while rank 0 runs it)
-    if rank == 0 and ws == 1 and args.amortized_steps > 0:
-        sim3 = LoquatSph(case=case, device=local, precision=4)
+    n_am = min(args.amortized_steps, cfg.get("trajectory_steps", args.amortized_steps))
+    if rank == 0 and ws == 1 and n_am > 0:
+        sim3 = LoquatSph(case=case, device=local, precision=prec)
         with ClockSampler(local) as clk3:
-            ms3 = sim3.step_timed(args.amortized_steps)
+            ms3 = sim3.step_timed(n_am)
         i3 = sim3.info()
         line["amortized"] = {
-            "value": i3.npm * args.amortized_steps / (ms3 * 1e-3), "unit": "particle-updates/s",
-            "steps": args.amortized_steps, "ms_per_step": ms3 / args.amortized_steps, "from_step": 0,
+            "value": i3.npm * n_am / (ms3 * 1e-3), "unit": "particle-updates/s",
+            "steps": n_am, "ms_per_step": ms3 / n_am, "from_step": 0,
             "sections_that_sorted": i3.n_sorts, "searches_skipped": i3.n_search_skipped,
             "interactions": 2 * i3.step, "interactions_on_kept_lists": i3.n_list_reuse,
             "list_updates": i3.n_list_updates,
             "lists_rebuilt_per_update": i3.n_lists_rebuilt / max(i3.n_list_updates, 1),
             "full_list_builds": 2 * i3.step - i3.n_build_skipped - i3.n_list_updates,
-            "vs_headline_window": (ms3 / args.amortized_steps) / (ms / args.steps),
+            "vs_headline_window": (ms3 / n_am) / (ms / args.steps),
             "clocks": clk3.summary()}
         sim3.close()
     if rank == 0 and ws == 1 and not args.no_reference_cuda:
-        line["reference_cuda"] = reference_cuda_sample(case, args.reference_cuda_steps, 3, local)
+        line["reference_cuda"] = reference_cuda_sample(case, args.reference_cuda_steps, 3, local, prec)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        ups, dt, _ = cpu_sample(case, threads, 2)
+        n_cpu = max(2, min(100, int(4e6 // max(npm, 1))))  # about 4M particle-updates of host work
+        ups, dt, _ = cpu_sample(case, threads, n_cpu, precision=prec)
         line["cpu_baseline"] = {"value": ups, "unit": "particle-updates/s", "cores": threads, "kind": "port",
-                                "sample": f"2 whole steps of the full {npm}-particle case (+1 warm-up)"}
-        ups64, _, _ = cpu_sample(case, threads, 1, precision=8)
-        line["cpu_baseline_f64"] = {"value": ups64, "unit": "particle-updates/s", "cores": threads, "kind": "port",
-                                    "sample": f"1 whole FP64 step of the full {npm}-particle case (+1 warm-up)"}
+                                "sample": f"{n_cpu} whole {'FP64' if prec == 8 else 'FP32'} steps of the full "
+                                          f"{npm}-particle case (+1 warm-up)"}
+        if prec == 4:
+            ups64, _, _ = cpu_sample(case, threads, 1, precision=8)
+            line["cpu_baseline_f64"] = {"value": ups64, "unit": "particle-updates/s", "cores": threads,
+                                        "kind": "port",
+                                        "sample": f"1 whole FP64 step of the full {npm}-particle case (+1 warm-up)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -921,6 +933,9 @@ def main():
                     help="steps of the long window from step 0 (sorts, list updates and rebuilds included; "
                          "default: the 1.92M wall's whole 20,000-step trajectory); 0: skip")
     ap.add_argument("--ix-kernel", type=int, default=None, help="interaction kernel: 0 global (default), 1 chunked")
+    ap.add_argument("--precision", type=int, choices=[4, 8], default=None,
+                    help="bytes per scalar of the single-case workloads (default: 8 for col1, which the "
+                         "configuration runs in FP64, else 4)")
     ap.add_argument("--skin", type=float, default=None, help="kept candidate-list skin in units of h (0: scan cells)")
     ap.add_argument("--strict", action="store_true", help="separately rounded interaction arithmetic")
     ap.add_argument("--no-gates", action="store_true",
