@@ -175,3 +175,19 @@ def test_shepard_filter_on_lists_equals_scan(every):
         np.testing.assert_array_equal(runs["lists"].get(key), runs["chunk"].get(key), err_msg=key)
     assert not np.array_equal(runs["lists"].get("str"), plain.get("str"))  # the filter acted
     assert runs["lists"].info().n_list_updates > 0 and runs["lists"].info().device_err == 0
+
+
+def test_periodic_wraps_update_lists():
+    """Periodic y planes (src/loquat_grid.cu's periodic images, `period_wrap` in the
+    corrector): the soil thrown along +y at 3 m/s crosses cell faces and, near the +y
+    plane, wraps to the other end of the grid.  Both cells of each wrap are marked and
+    the lists next to them rebuilt; the run equals scanning the cells, bit for bit."""
+    c = C.retaining_wall(nx=16, ny=8, nz=12, dx=0.005, wall_friction=C.REFERENCE_WALL_FRICTION, periodic_y=True,
+                         name="periodic")
+    c.velrhop[c.npb:, 1] = 3.0
+    s, rows = _run_with_updates(c, 150, 25, 0.6)
+    assert rows[:, 1].sum() > 0 and rows[:, 0].sum() > 0  # updates, sorts
+    idx = s.get("idmassidx")[:, 2].astype(np.int64)
+    y0 = c.pospres[idx[c.npb:], 1]
+    y1 = s.get("pos_abs")[c.npb:, 1]
+    assert (y1 < y0 - 0.01).any()  # some particles wrapped to the low side
