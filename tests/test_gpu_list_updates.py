@@ -191,3 +191,19 @@ def test_periodic_wraps_update_lists():
     y0 = c.pospres[idx[c.npb:], 1]
     y1 = s.get("pos_abs")[c.npb:, 1]
     assert (y1 < y0 - 0.01).any()  # some particles wrapped to the low side
+
+
+def test_precision_form_with_list_updates_equals_scan():
+    """The precision form permutes its compensation terms with the state; through list
+    updates after sorts it equals the same form scanning the cells, bit for bit."""
+    case = _column()
+    a, b = LoquatSph(case=case), LoquatSph(case=case)
+    for x in (a, b):
+        x.set_option(_abi.OPT_MIXED_PRECISION, 1)
+    a.set_option(_abi.OPT_LIST_SKIN, 0.6)
+    b.set_option(_abi.OPT_LIST_SKIN, 0.0)
+    a.step(150)
+    b.step(150)
+    for key in KEYS:
+        np.testing.assert_array_equal(a.get(key), b.get(key), err_msg=key)
+    assert a.info().n_list_updates > 0 and a.info().n_sorts > 10 and a.info().device_err == 0
