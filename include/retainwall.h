@@ -177,9 +177,13 @@ enum {
                                    results do not depend on it */
   RW_OPT_INTEGRATOR_THREADS = 9, /* threads per block of the predictor and corrector: 128 or 256 (default);
                                    results do not depend on it */
-  RW_OPT_CLOSURE_MAX_ERR = 7    /* learned closure: a particle keeps the network's objective rate only while
+  RW_OPT_CLOSURE_MAX_ERR = 7,   /* learned closure: a particle keeps the network's objective rate only while
                                    its judged relative error against the exact rate is at most this
                                    (default 0.02; 0: no bound, the trust region alone decides) */
+  RW_OPT_ASYNC_SAVE = 10        /* 1: rw_save gathers the output state and returns while a background task
+                                   formats and writes the files (one save in flight); the next rw_save,
+                                   rw_synchronize or rw_destroy waits for it, and the first two report its
+                                   status.  0 (default): rw_save returns once the files are written. */
 };
 
 const char* rw_status_string(rw_status s);
@@ -249,6 +253,9 @@ rw_status rw_wall_profile(rw_ctx* ctx, double x_wall, double z_top, double dz, i
  * Shepard-smoothed stress, stress_zzN.txt (rw_wall_profile with the reference's
  * defaults) and appends "time F[kN]" to <outdir>/time_history.txt. */
 rw_status rw_save(rw_ctx* ctx, const char* outdir);
+/* (The reference's Saving writes its files before the step loop goes on; with
+ * RW_OPT_ASYNC_SAVE the files are written while later steps run.  Formatting uses every
+ * host core either way.) */
 
 /* The particle file <project>.dat of a case, as the reference's generator writes it
  * (SaveDatFile, src/GenCase.cu:70-116, read back by LoquatIo::LoadParticles,

@@ -16,6 +16,7 @@ OPT_GRAPH_GATES = 6
 OPT_CLOSURE_MAX_ERR = 7
 OPT_WALK_THREADS = 8
 OPT_INTEGRATOR_THREADS = 9
+OPT_ASYNC_SAVE = 10
 
 # rw_array ids and their row shapes (columns, integer?)
 ARRAYS: Dict[str, int] = {

@@ -24,6 +24,8 @@ int main(int argc, char** argv) {
   rw_ctx* ctx = nullptr;
   rw_status s = rw_create(project.c_str(), device, precision, &ctx);
   if (s) return fail(nullptr, s, "rw_create");
+  // each save's files are written while the following steps run
+  if ((s = rw_set_option(ctx, RW_OPT_ASYNC_SAVE, 1.0))) return fail(ctx, s, "rw_set_option");
   rw_info inf;
   rw_get_info(ctx, &inf);
   std::printf("LOQUAT-compatible SPH step on device %d: np=%d npb=%d npm=%d ncell=%d dt=%.3e\n", device, inf.np,
@@ -56,6 +58,7 @@ int main(int argc, char** argv) {
       std::printf("Time = %0.5f saved\n", time - dt);
     }
   }
+  if ((s = rw_synchronize(ctx))) return fail(ctx, s, "rw_synchronize");  // the last save's files
   rw_destroy(ctx);
   return 0;
 }

@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <future>
 #include <limits>
 #include <memory>
 #include <stdexcept>
@@ -76,6 +77,12 @@ struct EngineBase {
 
 static inline unsigned nblk(long n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// Status of a save's file writing (rw_save, RW_OPT_ASYNC_SAVE).
+struct SaveResult {
+  int rc;
+  std::string msg;
+};
+
 template <class T> struct Engine final : EngineBase {
   Params<T> P{};
   DevState<T> S{};
@@ -104,10 +111,15 @@ template <class T> struct Engine final : EngineBase {
   // Step graphs captured with conditional nodes (gated()); st_body captures their bodies.
   bool allow_cond = false;
   bool graph_gates = true;  // RW_OPT_GRAPH_GATES
+  // RW_OPT_ASYNC_SAVE: the files of a save are formatted and written by a background
+  // task (at most one in flight) instead of by rw_save itself
+  bool async_save = false;
+  std::future<SaveResult> pending_save;
   bool graph_cond = false;  // the instantiated step graph has the gates
   cudaStream_t st_body = nullptr;
 
   ~Engine() override {
+    wait_save();
     if (gexec) cudaGraphExecDestroy(gexec);
     if (st) cudaStreamSynchronize(st);
     for (void* p : allocs) cudaFree(p);
@@ -903,6 +915,7 @@ template <class T> struct Engine final : EngineBase {
 
   int sync() override {
     RW_CU(cudaStreamSynchronize(st));
+    if (int rc = wait_save()) return rc;  // a save written in the background
     Dyn<T> d = dyn_host();
     if (d.err) {
       err = "device error word " + std::to_string(d.err);
@@ -982,6 +995,9 @@ template <class T> struct Engine final : EngineBase {
       strict_fp = v != 0.0;
     } else if (opt == RW_OPT_GRAPH_GATES) {
       graph_gates = v != 0.0;
+    } else if (opt == RW_OPT_ASYNC_SAVE) {
+      if (int rc = wait_save()) return rc;
+      async_save = v != 0.0;
     } else if (opt == RW_OPT_CLOSURE_MAX_ERR) {
       if (!(v >= 0.0)) {
         err = "closure error bound must be >= 0";
@@ -1246,6 +1262,7 @@ template <class T> struct Engine final : EngineBase {
   // Saving (src/loquat.cu:439-482): output_N.xml + particles with the Shepard-smoothed
   // stress (StressSavingRegularization, src/field_smoothing.cu:103-111) + time history.
   void save(const char* outdir) override {
+    if (int rc = wait_save()) throw Fail(rc, "the previous save: " + err);
     std::string dir = outdir ? outdir : ".";
     ::mkdir(dir.c_str(), 0755);
     Dyn<T> d = dyn_host();
@@ -1286,34 +1303,61 @@ template <class T> struct Engine final : EngineBase {
     // (src/loquat.cu:533-537); every later Saving increments first (src/loquat.cu:456).
     const bool initial = saves++ == 0;
     if (!initial) output_number++;
-    const std::string xmlp = dir + "/output_" + std::to_string(output_number) + ".xml";
+    const int onum = output_number;
     // The time written is the reference's par_host->time: that of the last step begun
     // (StepCalculation, src/loquat.cu:366-374), the case's time before any step.
     // and the time step is the parameter file's until StepCalculation first sets it.
     const double dt_out = initial && d.step == 0 ? (double)(T)cparams.dt : (double)P.dt;
-    int rc = write_output_xml(xmlp, cparams, P.np, P.npb, d.npm, (double)d.time_f, dt_out, output_number);
-    if (rc) throw Fail(rc, "cannot write " + xmlp);
-    if (P.output_format == 1) rc = write_frame_dat(dir + "/" + std::to_string(output_number) + ".dat", f);
-    else rc = write_frame_vtu(dir, output_number, f);
-    if (rc) throw Fail(rc, "cannot write particle output in " + dir);
-    if (initial) return;
-    {  // stress_zz<N>.txt: depth, then the three bands (GetValuesAlongLine, src/utilities.cu:324-367)
-      const int nb = (int)(T(1.0f) / P.dr);
-      std::vector<double> prof(4 * (size_t)std::max(nb, 1));
+    const double time_out = (double)d.time_f;
+    // stress_zz<N>.txt and the time history need the device: computed here, written below
+    std::vector<double> prof;
+    double wf[3] = {0.0, 0.0, 0.0};
+    const int nb = (int)(T(1.0f) / P.dr);
+    if (!initial) {
+      prof.assign(4 * (size_t)std::max(nb, 1), 0.0);
       const double nan = std::numeric_limits<double>::quiet_NaN();
       wall_profile(nan, nan, nan, nb, prof.data());
-      std::FILE* fz = std::fopen((dir + "/stress_zz" + std::to_string(output_number) + ".txt").c_str(), "w");
-      if (!fz) throw Fail(RW_EIO, "cannot write stress_zz file");
-      for (int b = 0; b < nb; ++b)
-        std::fprintf(fz, "%g %g %g %g\n", prof[4 * b], prof[4 * b + 1], prof[4 * b + 2], prof[4 * b + 3]);
-      std::fclose(fz);
+      wall_force(1, 10, nullptr, wf);
     }
-    double wf[3];
-    wall_force(1, 10, nullptr, wf);
-    std::FILE* th = std::fopen((dir + "/time_history.txt").c_str(), "a");
-    if (!th) throw Fail(RW_EIO, "cannot write time_history.txt");
-    std::fprintf(th, "%g %g\n", (double)d.time_f, 0.001 * wf[0]);  // ostream's default 6 digits
-    std::fclose(th);
+    // The files: formatted and written here, or by a background task with
+    // RW_OPT_ASYNC_SAVE (one in flight; the next save, rw_synchronize or the context's
+    // end waits for it and reports its status).
+    auto job = [dir, onum, dt_out, time_out, initial, nb, fmt = P.output_format, cp = cparams, np = P.np,
+                npb = P.npb, npm = d.npm, f = std::move(f), prof = std::move(prof), wfx = wf[0]]() -> SaveResult {
+      const std::string xmlp = dir + "/output_" + std::to_string(onum) + ".xml";
+      int rc = write_output_xml(xmlp, cp, np, npb, npm, time_out, dt_out, onum);
+      if (rc) return {rc, "cannot write " + xmlp};
+      if (fmt == 1) rc = write_frame_dat(dir + "/" + std::to_string(onum) + ".dat", f);
+      else rc = write_frame_vtu(dir, onum, f);
+      if (rc) return {rc, "cannot write particle output in " + dir};
+      if (initial) return {RW_OK, ""};
+      {  // stress_zz<N>.txt: depth, then the three bands (GetValuesAlongLine, src/utilities.cu:324-367)
+        std::FILE* fz = std::fopen((dir + "/stress_zz" + std::to_string(onum) + ".txt").c_str(), "w");
+        if (!fz) return {RW_EIO, "cannot write stress_zz file"};
+        for (int b = 0; b < nb; ++b)
+          std::fprintf(fz, "%g %g %g %g\n", prof[4 * b], prof[4 * b + 1], prof[4 * b + 2], prof[4 * b + 3]);
+        std::fclose(fz);
+      }
+      std::FILE* th = std::fopen((dir + "/time_history.txt").c_str(), "a");
+      if (!th) return {RW_EIO, "cannot write time_history.txt"};
+      std::fprintf(th, "%g %g\n", time_out, 0.001 * wfx);  // ostream's default 6 digits
+      std::fclose(th);
+      return {RW_OK, ""};
+    };
+    if (async_save) {
+      pending_save = std::async(std::launch::async, std::move(job));
+    } else {
+      const SaveResult r = job();
+      if (r.rc) throw Fail(r.rc, r.msg);
+    }
+  }
+
+  // Waits for a save being written in the background; its status, and its message in err.
+  int wait_save() {
+    if (!pending_save.valid()) return RW_OK;
+    const SaveResult r = pending_save.get();
+    if (r.rc) err = r.msg;
+    return r.rc;
   }
   void get6_cache(std::vector<T>& o) {
     const size_t n = P.np;

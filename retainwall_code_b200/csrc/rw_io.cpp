@@ -17,6 +17,41 @@
 
 namespace rw {
 
+namespace {
+// A real as an ostream prints it by default (printf's %g, six significant digits): the
+// format of the reference's output writer.
+inline void put_g(std::string& o, double v) {
+  char buf[40];
+  auto r = std::to_chars(buf, buf + sizeof(buf), v, std::chars_format::general, 6);
+  o.append(buf, r.ptr);
+}
+inline void put_i(std::string& o, long long v) {
+  char buf[24];
+  auto r = std::to_chars(buf, buf + sizeof(buf), v);
+  o.append(buf, r.ptr);
+}
+int io_threads() { return (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency())); }
+// Rows [0, n) formatted by fn(row, out) on several host threads, each into its own
+// buffer, then written to f in order.
+template <class Fn> bool put_rows(std::FILE* f, size_t n, size_t bytes_per_row, Fn fn) {
+  const int nth = n < 8192 ? 1 : io_threads();
+  std::vector<std::string> part(nth);
+  auto run = [&](int t) {
+    const size_t lo = n * t / nth, hi = n * (t + 1) / nth;
+    part[t].reserve((hi - lo) * bytes_per_row);
+    for (size_t q = lo; q < hi; ++q) fn(q, part[t]);
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nth; ++t) th.emplace_back(run, t);
+  run(0);
+  for (auto& x : th) x.join();
+  bool ok = true;
+  for (auto& s : part) ok = ok && std::fwrite(s.data(), 1, s.size(), f) == s.size();
+  return ok;
+}
+inline bool put_text(std::FILE* f, const std::string& s) { return std::fwrite(s.data(), 1, s.size(), f) == s.size(); }
+}  // namespace
+
 rw_case HostCase::view() const {
   rw_case c;
   c.params = params;
@@ -343,27 +378,41 @@ int write_output_xml(const std::string& path, const rw_case_params& p, int np, i
 // particle (boundary and soil) carries four normal columns, deleted particles do not and
 // end with a space.  The reference prints normal_m[i] for live soil rows too, reading
 // past its npb-entry normal array (src/loquat_io.cu:216,449); those columns are 0 here.
+// Rows are formatted by several host threads and written in order.
 int write_frame_dat(const std::string& path, const Frame& f) {
-  std::ofstream o(path);
+  std::FILE* o = std::fopen(path.c_str(), "wb");
   if (!o) return RW_EIO;
   const int live = f.npb + f.npm;
-  for (int i = 0; i < f.np; ++i) {
+  auto row = [&](size_t q, std::string& s) {
+    const int i = (int)q;
     const int32_t* c = &f.codes[4 * i];
-    o << c[0] << " " << c[1] << " " << c[2] << " " << c[3];
-    for (int k = 0; k < 4; ++k) o << " " << f.pos[4 * i + k];
-    for (int k = 0; k < 4; ++k) o << " " << f.vel[4 * i + k];
-    o << " " << f.idm[4 * i + 0] << " " << f.idm[4 * i + 1] << " " << f.idm[4 * i + 3];
-    for (int k = 0; k < 6; ++k) o << " " << f.str[6 * i + k];
-    for (int k = 0; k < 6; ++k) o << " " << f.stn[6 * i + k];
+    put_i(s, c[0]);
+    for (int k = 1; k < 4; ++k) {
+      s.push_back(' ');
+      put_i(s, c[k]);
+    }
+    auto g = [&](double v) {
+      s.push_back(' ');
+      put_g(s, v);
+    };
+    for (int k = 0; k < 4; ++k) g(f.pos[4 * i + k]);
+    for (int k = 0; k < 4; ++k) g(f.vel[4 * i + k]);
+    g(f.idm[4 * i + 0]);
+    g(f.idm[4 * i + 1]);
+    g(f.idm[4 * i + 3]);
+    for (int k = 0; k < 6; ++k) g(f.str[6 * i + k]);
+    for (int k = 0; k < 6; ++k) g(f.stn[6 * i + k]);
     if (i < f.npb)
-      for (int k = 0; k < 4; ++k) o << " " << f.normal[4 * i + k];
+      for (int k = 0; k < 4; ++k) g(f.normal[4 * i + k]);
     else if (i < live)
-      o << " 0 0 0 0";
+      s.append(" 0 0 0 0");
     else
-      o << " ";
-    o << "\n";
-  }
-  return o ? RW_OK : RW_EIO;
+      s.push_back(' ');
+    s.push_back('\n');
+  };
+  bool ok = put_rows(o, (size_t)f.np, 300, row);
+  ok = std::fclose(o) == 0 && ok;
+  return ok ? RW_OK : RW_EIO;
 }
 
 int write_frame_vtu(const std::string& dir, int output_number, const Frame& f) {
@@ -377,51 +426,76 @@ int write_frame_vtu(const std::string& dir, int output_number, const Frame& f) {
     size_t e = s;
     while (e < idx.size() && (int)f.idm[4 * idx[e]] == id) ++e;
     const size_t n = e - s;
-    std::ofstream o(dir + "/" + std::to_string(id) + "_" + std::to_string(output_number) + ".vtu");
+    const std::string path = dir + "/" + std::to_string(id) + "_" + std::to_string(output_number) + ".vtu";
+    std::FILE* o = std::fopen(path.c_str(), "wb");
     if (!o) return RW_EIO;
-    o << "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\" "
-         "compressor=\"vtkZLibDataCompressor\">\n  <UnstructuredGrid GhostLevel=\"0\">\n";
-    o << "    <Piece NumberOfPoints=\"" << n << "\" NumberOfCells=\"" << n << "\" Name=\"" << id << "\">\n      <PointData>\n";
+    bool ok = put_text(o, "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" "
+                          "byte_order=\"LittleEndian\" compressor=\"vtkZLibDataCompressor\">\n  <UnstructuredGrid "
+                          "GhostLevel=\"0\">\n");
+    ok = ok && put_text(o, "    <Piece NumberOfPoints=\"" + std::to_string(n) + "\" NumberOfCells=\"" +
+                               std::to_string(n) + "\" Name=\"" + std::to_string(id) + "\">\n      <PointData>\n");
+    // one DataArray: the block's rows formatted by several threads, each row by fn(i, out)
     auto arr = [&](const char* name, int ncomp, auto fn) {
-      o << "        <DataArray type=\"Float64\" Name=\"" << name << "\"";
-      if (ncomp > 1) o << " NumberOfComponents=\"" << ncomp << "\"";
-      o << ">\n";
-      for (size_t q = s; q < e; ++q) fn(idx[q]);
-      o << "</DataArray>\n";
+      std::string h = std::string("        <DataArray type=\"Float64\" Name=\"") + name + "\"";
+      if (ncomp > 1) h += " NumberOfComponents=\"" + std::to_string(ncomp) + "\"";
+      h += ">\n";
+      ok = ok && put_text(o, h);
+      ok = ok && put_rows(o, n, 16 * (size_t)ncomp, [&](size_t q, std::string& t) { fn(idx[s + q], t); });
+      ok = ok && put_text(o, "</DataArray>\n");
     };
-    arr("Material", 1, [&](int i) { o << f.codes[4 * i + 3] << " "; });
-    arr("Ori_ID", 1, [&](int i) { o << f.idm[4 * i + 3] << " "; });
-    arr("Velocity", 3, [&](int i) { o << f.vel[4 * i] << " " << f.vel[4 * i + 1] << " " << f.vel[4 * i + 2] << " "; });
-    arr("Acceleration", 3, [&](int i) { o << f.acc[4 * i] << " " << f.acc[4 * i + 1] << " " << f.acc[4 * i + 2] << " "; });
-    arr("Density", 1, [&](int i) { o << f.vel[4 * i + 3] << " "; });
-    arr("Mass", 1, [&](int i) { o << f.idm[4 * i + 1] << " "; });
+    auto g = [](std::string& t, double v) {
+      put_g(t, v);
+      t.push_back(' ');
+    };
+    arr("Material", 1, [&](int i, std::string& t) {
+      put_i(t, f.codes[4 * i + 3]);
+      t.push_back(' ');
+    });
+    arr("Ori_ID", 1, [&](int i, std::string& t) { g(t, f.idm[4 * i + 3]); });
+    arr("Velocity", 3, [&](int i, std::string& t) {
+      for (int k = 0; k < 3; ++k) g(t, f.vel[4 * i + k]);
+    });
+    arr("Acceleration", 3, [&](int i, std::string& t) {
+      for (int k = 0; k < 3; ++k) g(t, f.acc[4 * i + k]);
+    });
+    arr("Density", 1, [&](int i, std::string& t) { g(t, f.vel[4 * i + 3]); });
+    arr("Mass", 1, [&](int i, std::string& t) { g(t, f.idm[4 * i + 1]); });
     if (id < 100)
-      arr("Normal", 3, [&](int i) {
-        if (i < f.npb) o << f.normal[4 * i] << " " << f.normal[4 * i + 1] << " " << f.normal[4 * i + 2] << " ";
-        else o << "0 0 0 ";
+      arr("Normal", 3, [&](int i, std::string& t) {
+        if (i < f.npb)
+          for (int k = 0; k < 3; ++k) g(t, f.normal[4 * i + k]);
+        else
+          t.append("0 0 0 ");
       });
-    arr("Stress", 6, [&](int i) {
-      const double* t = &f.str[6 * i];
-      o << t[0] << " " << t[1] << " " << t[2] << " " << t[3] << " " << t[5] << " " << t[4] << " ";
+    // six components in the order xx yy zz xy yz xz
+    auto six = [&](const std::vector<double>& a, int i, std::string& t) {
+      const double* v = &a[6 * (size_t)i];
+      for (int k : {0, 1, 2, 3, 5, 4}) g(t, v[k]);
+    };
+    arr("Stress", 6, [&](int i, std::string& t) { six(f.str, i, t); });
+    arr("Strain", 6, [&](int i, std::string& t) { six(f.stn, i, t); });
+    ok = ok && put_text(o, "      </PointData>\n      <CellData>\n      </CellData>\n      <Points>\n"
+                           "        <DataArray type=\"Float64\" Name=\"Points\" NumberOfComponents=\"3\">\n");
+    ok = ok && put_rows(o, n, 48, [&](size_t q, std::string& t) {
+      const int i = idx[s + q];
+      for (int k = 0; k < 3; ++k) g(t, f.pos[4 * i + k]);
     });
-    arr("Strain", 6, [&](int i) {
-      const double* t = &f.stn[6 * i];
-      o << t[0] << " " << t[1] << " " << t[2] << " " << t[3] << " " << t[5] << " " << t[4] << " ";
+    ok = ok && put_text(o, "</DataArray>\n      </Points>\n      <Cells>\n        <DataArray type=\"Int64\" "
+                           "Name=\"connectivity\" format=\"ascii\">\n");
+    ok = ok && put_rows(o, n, 8, [&](size_t q, std::string& t) {
+      put_i(t, (long long)q);
+      t.push_back(' ');
     });
-    o << "      </PointData>\n      <CellData>\n      </CellData>\n      <Points>\n"
-         "        <DataArray type=\"Float64\" Name=\"Points\" NumberOfComponents=\"3\">\n";
-    for (size_t q = s; q < e; ++q) {
-      int i = idx[q];
-      o << f.pos[4 * i] << " " << f.pos[4 * i + 1] << " " << f.pos[4 * i + 2] << " ";
-    }
-    o << "</DataArray>\n      </Points>\n      <Cells>\n        <DataArray type=\"Int64\" Name=\"connectivity\" format=\"ascii\">\n";
-    for (size_t q = 0; q < n; ++q) o << q << " ";
-    o << "</DataArray>\n        <DataArray type=\"Int64\" Name=\"offsets\" format=\"ascii\"> \n";
-    for (size_t q = 0; q < n; ++q) o << q + 1 << " ";
-    o << "</DataArray>\n        <DataArray type=\"Int64\" Name=\"types\" format=\"ascii\">\n";
-    for (size_t q = 0; q < n; ++q) o << 1 << " ";
-    o << "</DataArray>\n      </Cells>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>\n";
-    if (!o) return RW_EIO;
+    ok = ok && put_text(o, "</DataArray>\n        <DataArray type=\"Int64\" Name=\"offsets\" format=\"ascii\"> \n");
+    ok = ok && put_rows(o, n, 8, [&](size_t q, std::string& t) {
+      put_i(t, (long long)q + 1);
+      t.push_back(' ');
+    });
+    ok = ok && put_text(o, "</DataArray>\n        <DataArray type=\"Int64\" Name=\"types\" format=\"ascii\">\n");
+    ok = ok && put_rows(o, n, 2, [&](size_t, std::string& t) { t.append("1 "); });
+    ok = ok && put_text(o, "</DataArray>\n      </Cells>\n    </Piece>\n  </UnstructuredGrid>\n</VTKFile>\n");
+    ok = std::fclose(o) == 0 && ok;
+    if (!ok) return RW_EIO;
     s = e;
   }
   return RW_OK;

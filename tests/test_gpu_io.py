@@ -124,3 +124,31 @@ def test_case_ingest_matches_host_conversion():
     assert np.all(idx[:c.npb] < c.npb)  # boundary rows stay in front
     np.testing.assert_array_equal(s.get("normal_m"), c.normal.astype(f32)[idx[:c.npb]].astype(np.float64))
     assert s.info().device_err == 0
+
+
+def test_async_save_writes_the_same_files(tmp_path):
+    """RW_OPT_ASYNC_SAVE: rw_save returns while a background task writes the files; the
+    next save or rw_synchronize waits for it.  The files equal those of synchronous saves
+    byte for byte (both formats), and a write that fails is reported by rw_synchronize."""
+    from retainwall_code_b200 import _abi
+
+    for fmt in (1, 2):
+        case = _wall_case()
+        case.params["output_format"] = fmt
+        a, b = LoquatSph(case=case), LoquatSph(case=case)
+        b.set_option(_abi.OPT_ASYNC_SAVE, 1)
+        da, db = str(tmp_path / f"sync{fmt}"), str(tmp_path / f"async{fmt}")
+        for s, d in ((a, da), (b, db)):
+            s.save(d)
+            for _ in range(3):
+                s.step(4)
+                s.save(d)
+            s.synchronize()
+        assert sorted(os.listdir(da)) == sorted(os.listdir(db))
+        for name in os.listdir(da):
+            assert open(os.path.join(da, name), "rb").read() == open(os.path.join(db, name), "rb").read(), name
+    c = LoquatSph(case=_wall_case())
+    c.set_option(_abi.OPT_ASYNC_SAVE, 1)
+    c.save("/proc/no_such_dir/out")  # the directory cannot be made: the background write fails
+    with pytest.raises(RuntimeError):
+        c.synchronize()
