@@ -10,6 +10,7 @@
 #include <stdexcept>
 #include <string>
 #include <sys/stat.h>
+#include <thread>
 #include <vector>
 
 #include "../../include/retainwall.h"
@@ -115,11 +116,14 @@ template <class T> struct Engine final : EngineBase {
   // task (at most one in flight) instead of by rw_save itself
   bool async_save = false;
   std::future<SaveResult> pending_save;
+  unsigned char* stage_h = nullptr;  // page-locked staging of a save's arrays
+  size_t stage_bytes = 0;
   bool graph_cond = false;  // the instantiated step graph has the gates
   cudaStream_t st_body = nullptr;
 
   ~Engine() override {
     wait_save();
+    if (stage_h) cudaFreeHost(stage_h);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (st) cudaStreamSynchronize(st);
     for (void* p : allocs) cudaFree(p);
@@ -1275,30 +1279,106 @@ template <class T> struct Engine final : EngineBase {
       k_shepard<T><<<nblk(P.npm0, 128), 128, 0, st>>>(P, S, d_dyn, 0);
       check_launch();
     }
-    Frame f;
-    f.np = P.np;
-    f.npb = P.npb;
-    f.npm = d.npm;
-    auto conv4 = [&](int which, std::vector<double>& o, size_t nrow) {
-      std::vector<T> h(4 * nrow);
-      if (nrow) {
-        int rc = get_array(which, h.data(), h.size() * sizeof(T));
-        if (rc) throw Fail(rc, "save: array export failed");
-      }
-      o.assign(h.begin(), h.end());
+    // The arrays a save writes, copied into one page-locked staging block with
+    // asynchronous copies and one wait; the conversion to the output values (absolute
+    // positions formed in the context's precision, as rw_get_array forms them) is done
+    // by the writing task, on several host threads.  The block stays in use until that
+    // task ends; the next save waits for it first.
+    const size_t npb = P.npb, n4 = sizeof(V4<T>), n2 = sizeof(V2<T>);
+    size_t off = 0;
+    auto take = [&](size_t b) {
+      const size_t o = off;
+      off += (b + 255) & ~(size_t)255;
+      return o;
     };
-    f.codes.resize(4 * np);
-    if (get_array(RW_ARR_CODES, f.codes.data(), 16 * np)) throw Fail(RW_ECUDA, "save: codes");
-    conv4(RW_ARR_POS_ABS, f.pos, np);
-    conv4(RW_ARR_VELRHOP, f.vel, np);
-    conv4(RW_ARR_ACCAD, f.acc, np);
-    conv4(RW_ARR_IDMASSIDX, f.idm, np);
-    conv4(RW_ARR_NORMAL, f.normal, P.npb);
-    std::vector<T> h6(6 * np);
-    get6_cache(h6);
-    f.str.assign(h6.begin(), h6.end());
-    if (get_array(RW_ARR_STN, h6.data(), h6.size() * sizeof(T))) throw Fail(RW_ECUDA, "save: stn");
-    f.stn.assign(h6.begin(), h6.end());
+    const size_t o_codes = take(np * 16), o_pos = take(np * n4), o_cell = take(np * 16), o_vel = take(np * n4),
+                 o_acc = take(np * n4), o_idm = take(np * n4), o_nrm = take(npb * n4), o_ta = take(np * n4),
+                 o_tb = take(np * n2), o_sa = take(np * n4), o_sb = take(np * n2);
+    if (off > stage_bytes) {
+      if (stage_h) cudaFreeHost(stage_h);
+      stage_h = nullptr;
+      stage_bytes = 0;
+      RW_CU(cudaMallocHost(reinterpret_cast<void**>(&stage_h), off));
+      stage_bytes = off;
+    }
+    auto get = [&](size_t o, const void* src, size_t b) {
+      if (b) RW_CU(cudaMemcpyAsync(stage_h + o, src, b, cudaMemcpyDeviceToHost, st));
+    };
+    get(o_codes, S.codes[c], np * 16);
+    get(o_pos, S.pos[c], np * n4);
+    get(o_cell, S.cellpos[c], np * 16);
+    get(o_vel, S.vel[c], np * n4);
+    get(o_acc, S.accad, np * n4);
+    get(o_idm, S.idm[c], np * n4);
+    get(o_nrm, S.normal[d.cur_nrm], npb * n4);
+    get(o_ta, S.tc_a, np * n4);
+    get(o_tb, S.tc_b, np * n2);
+    get(o_sa, S.stn_a[c], np * n4);
+    get(o_sb, S.stn_b[c], np * n2);
+    RW_CU(cudaStreamSynchronize(st));
+    const unsigned char* sh = stage_h;
+    const T two_h = P.two_h;
+    const int npm_now = d.npm;
+    auto make_frame = [=]() {
+      Frame f;
+      f.np = (int)np;
+      f.npb = (int)npb;
+      f.npm = npm_now;
+      f.codes.resize(4 * np);
+      f.pos.resize(4 * np);
+      f.vel.resize(4 * np);
+      f.acc.resize(4 * np);
+      f.idm.resize(4 * np);
+      f.normal.resize(4 * npb);
+      f.str.resize(6 * np);
+      f.stn.resize(6 * np);
+      const auto* codes = reinterpret_cast<const int32_t*>(sh + o_codes);
+      const auto* pos = reinterpret_cast<const V4<T>*>(sh + o_pos);
+      const auto* cell = reinterpret_cast<const int4*>(sh + o_cell);
+      const auto* vel = reinterpret_cast<const V4<T>*>(sh + o_vel);
+      const auto* acc = reinterpret_cast<const V4<T>*>(sh + o_acc);
+      const auto* idm = reinterpret_cast<const V4<T>*>(sh + o_idm);
+      const auto* nrm = reinterpret_cast<const V4<T>*>(sh + o_nrm);
+      const auto* ta = reinterpret_cast<const V4<T>*>(sh + o_ta);
+      const auto* tb = reinterpret_cast<const V2<T>*>(sh + o_tb);
+      const auto* sa = reinterpret_cast<const V4<T>*>(sh + o_sa);
+      const auto* sb = reinterpret_cast<const V2<T>*>(sh + o_sb);
+      auto put4 = [](double* o, const V4<T>& v) {
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+      };
+      auto put6 = [](double* o, const V4<T>& a, const V2<T>& b) {
+        o[0] = a.x;
+        o[1] = a.y;
+        o[2] = a.z;
+        o[3] = a.w;
+        o[4] = b.x;
+        o[5] = b.y;
+      };
+      auto rows = [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+          std::memcpy(&f.codes[4 * i], codes + 4 * i, 16);
+          const V4<T> p = pos[i];
+          const int4 cc = cell[i];
+          const V4<T> pa{p.x + (T)cc.x * two_h, p.y + (T)cc.y * two_h, p.z + (T)cc.z * two_h, p.w};
+          put4(&f.pos[4 * i], pa);
+          put4(&f.vel[4 * i], vel[i]);
+          put4(&f.acc[4 * i], acc[i]);
+          put4(&f.idm[4 * i], idm[i]);
+          if (i < npb) put4(&f.normal[4 * i], nrm[i]);
+          put6(&f.str[6 * i], ta[i], tb[i]);
+          put6(&f.stn[6 * i], sa[i], sb[i]);
+        }
+      };
+      const int nth = np < 65536 ? 1 : (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+      std::vector<std::thread> th;
+      for (int t = 1; t < nth; ++t) th.emplace_back(rows, np * t / nth, np * (t + 1) / nth);
+      rows(0, np / nth);
+      for (auto& x : th) x.join();
+      return f;
+    };
     // RunSimulation writes the initial configuration with the case's output number
     // (src/loquat.cu:533-537); every later Saving increments first (src/loquat.cu:456).
     const bool initial = saves++ == 0;
@@ -1323,7 +1403,9 @@ template <class T> struct Engine final : EngineBase {
     // RW_OPT_ASYNC_SAVE (one in flight; the next save, rw_synchronize or the context's
     // end waits for it and reports its status).
     auto job = [dir, onum, dt_out, time_out, initial, nb, fmt = P.output_format, cp = cparams, np = P.np,
-                npb = P.npb, npm = d.npm, f = std::move(f), prof = std::move(prof), wfx = wf[0]]() -> SaveResult {
+                npb = P.npb, npm = d.npm, mk = std::move(make_frame), prof = std::move(prof),
+                wfx = wf[0]]() -> SaveResult {
+      const Frame f = mk();
       const std::string xmlp = dir + "/output_" + std::to_string(onum) + ".xml";
       int rc = write_output_xml(xmlp, cp, np, npb, npm, time_out, dt_out, onum);
       if (rc) return {rc, "cannot write " + xmlp};
