@@ -234,11 +234,19 @@ int read_project(const std::string& project, HostCase* hc, std::string* msg) {
     *msg = "number-of-motion out of range";
     return RW_EFORMAT;
   }
-  // .dat (src/loquat_io.cu:222-264)
-  std::ifstream dat(project + ".dat");
-  if (!dat) {
+  // .dat (src/loquat_io.cu:222-264): one particle per line, read whole, the lines
+  // parsed by several host threads (strtol / strtod, as a line-by-line read would)
+  std::FILE* df = std::fopen((project + ".dat").c_str(), "rb");
+  if (!df) {
     *msg = "Error! Cannot open " + project + ".dat !";
     return RW_ENOENT;
+  }
+  std::string buf;
+  {
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = std::fread(chunk, 1, sizeof(chunk), df)) > 0) buf.append(chunk, got);
+    std::fclose(df);
   }
   const size_t np = (size_t)p.np, npb = (size_t)p.npb;
   hc->codes.assign(4 * np, 0);
@@ -248,17 +256,41 @@ int read_project(const std::string& project, HostCase* hc, std::string* msg) {
   hc->stress.assign(6 * np, 0.0);
   hc->strain.assign(6 * np, 0.0);
   hc->normal.assign(4 * npb, 0.0);
-  std::string line;
+  // the first np lines, each ended by a terminator in place of its newline
+  std::vector<size_t> start(np);
+  size_t at = 0;
   for (size_t i = 0; i < np; ++i) {
-    if (!std::getline(dat, line)) {
+    if (at >= buf.size()) {
       *msg = "Error! " + project + ".dat ends before particle " + std::to_string(i);
       return RW_EFORMAT;
     }
-    const char* c = line.c_str();
-    char* e = nullptr;
-    auto nextl = [&]() { long v = std::strtol(c, &e, 10); if (e == c) throw 1; c = e; return (int32_t)v; };
-    auto nextd = [&]() { double v = std::strtod(c, &e); if (e == c) throw 1; c = e; return v; };
-    try {
+    start[i] = at;
+    const size_t nl = buf.find('\n', at);
+    if (nl == std::string::npos) {
+      at = buf.size();
+    } else {
+      buf[nl] = '\0';
+      at = nl + 1;
+    }
+  }
+  std::vector<size_t> bad_line(io_threads(), np);  // per thread: first malformed line
+  auto parse = [&](int t, size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) {
+      const char* c = buf.c_str() + start[i];
+      char* e = nullptr;
+      bool ok = true;
+      auto nextl = [&]() {
+        long v = std::strtol(c, &e, 10);
+        ok = ok && e != c;
+        c = e;
+        return (int32_t)v;
+      };
+      auto nextd = [&]() {
+        double v = std::strtod(c, &e);
+        ok = ok && e != c;
+        c = e;
+        return v;
+      };
       for (int k = 0; k < 4; ++k) hc->codes[4 * i + k] = nextl();
       for (int k = 0; k < 4; ++k) hc->pospres[4 * i + k] = nextd();
       for (int k = 0; k < 4; ++k) hc->velrhop[4 * i + k] = nextd();
@@ -270,10 +302,23 @@ int read_project(const std::string& project, HostCase* hc, std::string* msg) {
       for (int k = 0; k < 6; ++k) hc->strain[6 * i + k] = nextd();
       if (i < npb)
         for (int k = 0; k < 4; ++k) hc->normal[4 * i + k] = nextd();
-    } catch (int) {
-      *msg = "Error! malformed particle line " + std::to_string(i) + " in " + project + ".dat";
-      return RW_EFORMAT;
+      if (!ok) {
+        bad_line[t] = i;
+        return;
+      }
     }
+  };
+  {
+    const int nth = np < 8192 ? 1 : (int)bad_line.size();
+    std::vector<std::thread> th;
+    for (int t = 1; t < nth; ++t) th.emplace_back(parse, t, np * t / nth, np * (t + 1) / nth);
+    parse(0, 0, np / nth);
+    for (auto& x : th) x.join();
+  }
+  const size_t bad = *std::min_element(bad_line.begin(), bad_line.end());
+  if (bad < np) {
+    *msg = "Error! malformed particle line " + std::to_string(bad) + " in " + project + ".dat";
+    return RW_EFORMAT;
   }
   // .motion (src/loquat_io.cu:266-311)
   if (p.n_motion > 0) {

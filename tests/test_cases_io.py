@@ -84,3 +84,31 @@ def test_native_dat_writer_matches_python(tmp_path):
         assert filecmp.cmp(a + ".dat", n + ".dat", shallow=False)
         r = C.read_case(n)
         np.testing.assert_array_equal(r.pospres.astype(np.float32), c.pospres.astype(np.float32))
+
+
+def test_project_reader_reports_malformed_and_short_particle_files(tmp_path):
+    """rw_create reads <project>.dat (src/loquat_io.cu:222-264) on several host threads
+    before it touches the GPU: a malformed line deep in a large file is reported with
+    its index, as a line-by-line read would, and so is a file that ends early."""
+    import ctypes as ct
+
+    from retainwall_code_b200 import _lib, cases as C
+
+    case = C.column_collapse()  # 27,648 soil particles: the reader splits the file across threads
+    proj = str(tmp_path / "col")
+    C.write_case(case, proj)
+    lines = open(proj + ".dat").read().split("\n")
+    L = _lib.lib()
+
+    def create_error():
+        ctx = ct.c_void_p()
+        st = L.rw_create(proj.encode(), 0, 4, ct.byref(ctx))
+        assert st != 0
+        return L.rw_last_error(None).decode()
+
+    bad = list(lines)
+    bad[20000] = bad[20000].split(" ")[0] + " 1 2 x"
+    open(proj + ".dat", "w").write("\n".join(bad))
+    assert "malformed particle line 20000" in create_error()
+    open(proj + ".dat", "w").write("\n".join(lines[:30000]) + "\n")
+    assert "ends before particle 30000" in create_error()
