@@ -1376,17 +1376,17 @@ template <bool Strict, class T> RWD void ix_finish(const Params<T>& P, const Dev
 
 // Candidate lists of the live soil particles: the 27 cells in the scan's order (cz,
 // cy, cx; boundary range before material range; ascending j), every candidate within
-// the list radius, written column-major to HBM.  Mode 0 builds every list and starts
-// the displacement bounds; mode 2 (list update) rebuilds only the lists of particles
-// next to a marked cell and carries the others through the section's permutation, the
-// bounds running on from the last full build (a list built since then moved no more
-// than its particle's bound).  A list longer than IX_CAP is marked -1 and counted
-// (n_spill): the scan launch then takes that particle.  Light (no pair arithmetic, no
-// shared-memory list), so it runs at full occupancy; the walk kernel then evaluates
-// the lists with the same pairs in the same order as a scan.  One thread per particle,
-// boundary rows first: in an update after a permutation the boundary rows carry their
-// Adami lists too (the Adami kernel, which holds many registers and runs few warps,
-// only rebuilds the ones next to a marked cell).
+// the list radius, written column-major to HBM.  Mode 0 builds every soil list here and
+// starts the displacement bounds (the Adami kernel builds the boundary lists).  Mode 2
+// (list update) queues the lists of particles next to a marked cell, soil and boundary
+// rows alike, for k_rebuild_lists, and carries the others through the section's
+// permutation; the bounds run on from the last full build (a list built since then
+// moved no more than its particle's bound).  A list longer than IX_CAP is marked -1 and
+// counted (n_spill): the scan launch then takes that particle.  Light (no pair
+// arithmetic, no shared-memory list), so it runs at full occupancy; the walk kernel
+// then evaluates the lists with the same pairs in the same order as a scan.  One thread
+// per particle, boundary rows first, so that in an update the Adami kernel (many
+// registers, few warps per SM) only walks lists.
 template <class T> __global__ void __launch_bounds__(256) k_build_lists(const Params<T> P, DevState<T> S, Dyn<T>* dyn) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   const int mode = dyn->ix_mode;
