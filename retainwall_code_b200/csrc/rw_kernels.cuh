@@ -2269,7 +2269,7 @@ template <class T> __global__ void __launch_bounds__(WF_THREADS) k_wall_force(co
                                                                              const Dyn<T>* dyn, int cpar, int mode,
                                                                              int wall_id, double xmax, double zmin,
                                                                              double zmax) {
-  __shared__ double red[3][WF_THREADS];
+  __shared__ double red[3][WF_THREADS / 32];
   const int npm = dyn->npm, c = dyn->cur_main;
   double a[3] = {0.0, 0.0, 0.0};
   for (int t = blockIdx.x * WF_THREADS + threadIdx.x; t < npm; t += gridDim.x * WF_THREADS) {
@@ -2292,15 +2292,21 @@ template <class T> __global__ void __launch_bounds__(WF_THREADS) k_wall_force(co
       a[2] += (double)f.z;
     }
   }
-  for (int k = 0; k < 3; ++k) red[k][threadIdx.x] = a[k];
+  // warp-shuffle butterfly, then the warps' partials in warp order: a fixed order, so
+  // the resultant does not change from run to run
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; ++k) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; ++k) red[k][warp] = a[k];
   __syncthreads();
-  for (int s = WF_THREADS / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-      for (int k = 0; k < 3; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + s];
-    __syncthreads();
-  }
   if (threadIdx.x == 0)
-    for (int k = 0; k < 3; ++k) S.wsum[3 * blockIdx.x + k] = red[k][0];
+    for (int k = 0; k < 3; ++k) {
+      double v = 0.0;
+      for (int w = 0; w < WF_THREADS / 32; ++w) v += red[k][w];
+      S.wsum[3 * blockIdx.x + k] = v;
+    }
 }
 
 static __global__ void k_wall_force_final(double* wsum, int nblocks) {
